@@ -1,0 +1,97 @@
+"""Generate the golden fixtures in tests/golden from the reference's own solver.
+
+Run from the repository root after ``make -C oracle ref`` (which compiles the
+reference's lbm.cpp / System.cpp / mpi_view_transfer.cpp from the reference
+tree against oracle/refshim):
+
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+
+Each fixture records the inputs (the nine input.in numbers, the step count,
+the sphere's `ran` field) and the reference's outputs after that many steps:
+interior u, v, w, p (x fastest), a SHA-256 of the padded distribution array
+f (population fastest, exactly as the reference stores it) and of the solid
+mask.  The three input.in files the reference ships are recorded with the
+parameters System derives from them, and one Tecplot file written by the
+reference's MPIoutput is recorded by digest and header bytes.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle.bindings import Reference, run_reference_case  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# (name, case, rho0, R, Re, u0, nx, ny, nz, steps)
+CASES = [
+    ("tgv_8x8x8_s10", "tgv", 1.0, 0.1, 100, 0.05, 8, 8, 8, 10),
+    ("tgv_10x12x9_s7", "tgv", 1.0, 0.1, 1600, 0.05, 10, 12, 9, 7),
+    ("cavity_8x8x8_s20", "cavity", 1.0, 8.0, 100, 0.1, 8, 8, 8, 20),
+    ("cavity_9x11x10_s12", "cavity", 1.0, 10.0, 50, 0.1, 9, 11, 10, 12),
+    ("sphere_72x12x12_s4", "sphere", 1.0, 2.0, 100, 0.1, 72, 12, 12, 4),
+]
+
+# the three input.in files of the reference tree, as (case, nine numbers)
+SHIPPED = {
+    "tgv": "tgv/input.in",
+    "cavity": "lid_driven_cavity/input.in",
+    "sphere": "sphere/input.in",
+}
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main(refroot: str = "/root/reference"):
+    manifest = {}
+    for name, case, rho0, R, Re, u0, nx, ny, nz, steps in CASES:
+        r = run_reference_case(case, rho0, R, Re, u0, nx, ny, nz, steps, warmup=20)
+        s = r["system"]
+        arrays = dict(u=r["u"], v=r["v"], w=r["w"], p=r["p"])
+        if case == "sphere":
+            arrays["ran"] = r["ran"].astype(np.uint8)
+        np.savez_compressed(os.path.join(OUT, f"ref_{name}.npz"), **arrays)
+        manifest[name] = dict(case=case, rho0=rho0, R=R, Re=Re, u0=u0, nx=nx, ny=ny, nz=nz, steps=steps,
+                              tau=s["tau"], f_sha256=sha(r["f"]), usr_sha256=sha(r["usr"]),
+                              solid_cells=int((r["usr"][3:-3, 3:-3, 3:-3] == 0).sum()) if case == "sphere" else 0)
+        print(name, "ok")
+
+    systems = {}
+    for case, rel in SHIPPED.items():
+        src = os.path.join(refroot, rel)
+        with open(src) as fh:
+            nums = fh.read().split()[:9]
+        d = tempfile.mkdtemp(prefix="imexlb_sys_")
+        with open(os.path.join(d, "input.in"), "w") as fh:
+            fh.write(f"{nums[0]} {nums[1]} {nums[2]}\n{nums[3]} {nums[4]} {nums[5]}\n{nums[6]} {nums[7]} {nums[8]}\n")
+        systems[case] = dict(input=nums, derived=Reference(case).system(d))
+    manifest["shipped_input_in"] = systems
+
+    # Tecplot output of the cavity driver: MPIoutput(0) and every 5 steps
+    d = tempfile.mkdtemp(prefix="imexlb_plt_")
+    run_reference_case("cavity", 1.0, 8.0, 100, 0.1, 8, 8, 8, 10, out_every=5, want_f=False, workdir=d)
+    plt = {}
+    for n in (0, 1, 2):
+        with open(os.path.join(d, f"output{n}.plt"), "rb") as fh:
+            data = fh.read()
+        plt[f"output{n}.plt"] = dict(size=len(data), sha256=hashlib.sha256(data).hexdigest(),
+                                     header_hex=data[:332].hex())
+    manifest["tecplot_cavity_8x8x8"] = dict(rho0=1.0, R=8.0, Re=100, u0=0.1, nx=8, ny=8, nz=8, steps=10,
+                                            out_every=5, files=plt)
+
+    with open(os.path.join(OUT, "manifest.json"), "w") as fh:
+        json.dump(manifest, fh, indent=1, sort_keys=True)
+    print("wrote", os.path.join(OUT, "manifest.json"))
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])
