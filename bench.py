@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the fused D3Q27 step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: the lid-driven cavity, plain FP64, 128^3 lattice, halfway
+bounce-back on five walls and a lid moving at u_w = (0.1, 0, 0) with the
+-2 w_i rho (c_i . u_w)/cs^2 correction, Re = 1000 (nu = 0.1*128/1000,
+tau = 0.5 + 3 nu).  A "step" is one lattice time step over the whole box.
+Metric: MLUPS (million lattice-cell updates per second), whole job.
+
+* value     device-resident throughput: K steps on the lattice's stream timed
+            with CUDA events (barrier + synchronize on both sides, max over
+            ranks); the two 470 MB distribution buffers exceed the 126 MB L2,
+            so no flush is needed between steps.
+* e2e       the same solve through the public C ABI from host memory: create
+            (host set-up + upload), K steps with the u, v, w, p fields read
+            into pinned host buffers every K/10 steps (the reference driver's
+            output cadence, Time/inter = 10), host wall clock.
+* roofline  the fused step kernel: 432 algorithmic bytes per cell update
+            (27 FP64 loads + 27 FP64 stores) x cells / mean launch duration
+            (per-launch CUDA events on the launching stream), against the
+            measured HBM copy bandwidth of MEASURED_PEAKS.json.
+* cpu_baseline  the reference's own solver (oracle/_ref) on the host cores,
+            rank 0, a bounded sample of full-size steps (subprocess).
+--impl reference runs only that CPU measurement (rank 0) and prints its line.
+With --gpus N (torchrun, one rank per GPU) every rank advances its own
+replica of the workload: the path has no exchange step ("replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # BASELINE configuration: lid-driven cavity, plain FP64, 128^3, Re 1000
+    "cavity128-f64": dict(case="cavity", bc="standard", storage="f64", arith="fast", n=(128, 128, 128), Re=1000,
+                          u0=0.1, R=128.0, lid_u=0.1),
+    "cavity128-f64-exact": dict(case="cavity", bc="standard", storage="f64", arith="exact", n=(128, 128, 128),
+                                Re=1000, u0=0.1, R=128.0, lid_u=0.1),
+    # the reference's own boundary passes (bit-exact drop-in)
+    "cavity128-f64-refbc": dict(case="cavity", bc="reference", storage="f64", arith="exact", n=(128, 128, 128),
+                                Re=1000, u0=0.1, R=128.0, lid_u=0.1),
+    "tgv64-f64": dict(case="tgv", bc="reference", storage="f64", arith="exact", n=(64, 64, 64), Re=100, u0=0.05,
+                      R=0.1, lid_u=0.0),
+    "tgv256-f64": dict(case="tgv", bc="reference", storage="f64", arith="fast", n=(256, 256, 256), Re=1600,
+                       u0=0.05, R=0.1, lid_u=0.0),
+    "cavity128-f16": dict(case="cavity", bc="standard", storage="f16", arith="fast", n=(128, 128, 128), Re=1000,
+                          u0=0.1, R=128.0, lid_u=0.1),
+    "cavity128-f32": dict(case="cavity", bc="standard", storage="f32", arith="fast", n=(128, 128, 128), Re=1000,
+                          u0=0.1, R=128.0, lid_u=0.1),
+}
+DEFAULT_WORKLOAD = "cavity128-f64"
+
+
+def tau_of(w) -> float:
+    """tau0 = 3 nu: System::tau of the reference (tgv/src/System.cpp:21,
+    lid_driven_cavity/src/System.cpp:19)."""
+    cs2 = 1.0 / 3.0
+    if w["case"] == "tgv":
+        return w["u0"] * w["n"][0] / w["Re"] / cs2 / 2 / 3.1415926
+    return w["u0"] * w["R"] / w["Re"] / cs2
+
+
+def dtype_of(w) -> str:
+    return {"f64": "f64", "f32": "f32 (fp32 collide)", "f16": "f16 storage / fp32 collide",
+            "bf16": "bf16 storage / fp32 collide"}[w["storage"]]
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=6650.0, source="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(0.25)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"], samples=0)
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(smax) if smax else None,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+def run_cpu_baseline(w, seconds: float, max_steps: int | None = None) -> dict:
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+    env["OMP_PROC_BIND"] = "false"
+    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--case", w["case"], "--n", *map(str, w["n"]),
+           "--R", repr(w["R"]), "--Re", str(w["Re"]), "--u0", repr(w["u0"]), "--seconds", str(seconds)]
+    if max_steps:
+        cmd += ["--max-steps", str(max_steps)]
+    out = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=900)
+    if out.returncode != 0:
+        return dict(value=None, unit="MLUPS", cores=None, kind=None, sample="failed: " + out.stderr[-300:])
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    return dict(value=res["mlups"], unit="MLUPS", cores=res["cores"], kind=res["kind"], sample=res["sample"],
+                seconds=res["seconds"])
+
+
+def config_of(w, name, n_gpus) -> dict:
+    nx, ny, nz = w["n"]
+    return {"workload": name, "case": w["case"], "boundary": w["bc"], "storage": w["storage"],
+            "arith": w["arith"], "lattice": f"{nx}x{ny}x{nz}", "Re": w["Re"], "tau": 0.5 + tau_of(w),
+            "lid_u": w["lid_u"], "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
+            "l2": "inputs larger than L2 (two distribution buffers of "
+                  f"{27 * nx * ny * nz * (8 if w['storage'] == 'f64' else 4 if w['storage'] == 'f32' else 2) / 1e6:.0f} MB)"}
+
+
+def reference_arm(args, w, name, rank, world):
+    if rank != 0:
+        return 0
+    # each reference "step" is one full-size lattice step; the sample is
+    # bounded so that the whole run ends within minutes
+    cb = run_cpu_baseline(w, seconds=min(60.0, 5.0 + 0.5 * args.steps), max_steps=args.steps)
+    line = {"impl": "reference", "metric": "D3Q27 MLUPS", "value": cb["value"], "unit": "MLUPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (1e3 * cb["seconds"] / max(1, int(cb["sample"].split()[0]))) if cb["value"] else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic initial and boundary conditions of the case)",
+            "config": config_of(w, name, 1),
+            "cpu_baseline": {"value": cb["value"], "unit": "MLUPS", "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args(argv)
+    w = WORKLOADS[args.workload]
+    name = args.workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return reference_arm(args, w, name, rank, world)
+
+    # CPU baseline first, in a subprocess, before this process touches CUDA
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_baseline(w, args.cpu_seconds)
+
+    import numpy as np
+    import torch
+
+    from imexlb_b200 import api
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    nx, ny, nz = w["n"]
+    cells = nx * ny * nz
+    tau = tau_of(w)
+    kw = dict(bc=w["bc"], storage=w["storage"], arith=w["arith"], lid_u=w["lid_u"])
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        lbm = api.LBM(w["case"], nx, ny, nz, tau, 1.0, w["u0"], stream=stream.cuda_stream, **kw)
+        lbm.step(args.warmup)
+        barrier()
+        sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+        if sampler:
+            sampler.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lbm.profile(True)
+        barrier()
+        ev0.record(stream)
+        lbm.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        kt = lbm.profile_read()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        elapsed_ms = ev0.elapsed_time(ev1)
+        resid = lbm.reduce("umax")
+        lbm.close()
+
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * cells * args.steps / (max_ms * 1e-3) / 1e6
+
+    # ---- end to end through the public API, host memory in and out
+    outputs = 10
+    chunk = max(1, args.steps // outputs)
+    pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
+    barrier()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        lbm2 = api.LBM(w["case"], nx, ny, nz, tau, 1.0, w["u0"], stream=stream.cuda_stream, **kw)
+        done = 0
+        nout = 0
+        while done < args.steps:
+            s = min(chunk, args.steps - done)
+            lbm2.step(s)
+            done += s
+            lbm2.fields(out=pinned)
+            nout += 1
+        lbm2.close()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    e2e = world * cells * args.steps / e2e_s / 1e6
+    h2d = 4 * 8 * cells / args.steps  # the initial u, v, w, p fields uploaded at create
+    d2h = nout * 4 * 8 * cells / args.steps
+
+    if rank == 0:
+        peaks = load_peaks()
+        bpv = api.BYTES_PER_VALUE[w["storage"]]
+        alg_bytes = 2 * 27 * bpv * cells
+        step_ms = kt["step_ms"] / max(1, kt["step_launches"])
+        achieved = alg_bytes / (step_ms * 1e-3) / 1e9
+        dominant = "step_kernel (fused pull/moments/collide)"
+        launches = kt["step_launches"] + kt["ghost_launches"]
+        line = {
+            "metric": "D3Q27 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
+            "data": "synthetic (analytic initial and boundary conditions of the case)",
+            "config": config_of(w, name, world),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic": None, "bytes_per_cell_update": 2 * 27 * bpv,
+                         "mean_launch_ms": step_ms,
+                         "ghost_gather_ms_per_step": kt["ghost_ms"] / max(1, kt["ghost_launches"])
+                         if kt["ghost_launches"] else 0.0},
+            "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds": e2e_s, "outputs": nout},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": ({"value": cpu["value"], "unit": "MLUPS", "cores": cpu["cores"], "kind": cpu["kind"],
+                              "sample": cpu["sample"]} if cpu else None),
+            "check": {"max_speed_after_run": resid},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

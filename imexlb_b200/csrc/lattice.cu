@@ -1,0 +1,732 @@
+// Host runtime behind the C ABI (include/imexlb.h): parameter parsing,
+// case set-up, device buffers, the step loop and the output paths.
+//
+// Case set-up follows the reference's Initialize (tgv/src/lbm.cpp:195-218,
+// lid_driven_cavity/src/lbm.cpp:191-210, sphere/src/lbm.cpp:221-254): the
+// macroscopic fields are computed here in FP64 with the same expressions (and
+// the same libm), then the device writes f = feq into both buffers.  Host code
+// in this file is compiled with -ffp-contract=off so every operation rounds
+// as written.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/imexlb.h"
+#include "lattice.h"
+
+using namespace imx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define IMX_CUDA(call)                                                                             \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(IMEXLB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));               \
+  } while (0)
+
+constexpr double PI_REF = 3.1415926;  // tgv/src/lbm.cpp:5, tgv/src/System.cpp:20-21
+
+// splitmix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): the sphere's `ran` field when the caller gives
+// none.  ran(i, j, k) = mix(seed ^ index) % 100, independent of thread order.
+uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+template <class T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevArray() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    reset();
+    n = count;
+    return count ? cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)) : cudaSuccess;
+  }
+};
+
+}  // namespace
+
+namespace imx {
+Layout make_layout(int nx, int ny, int nz, int g, int elem) {
+  Layout L;
+  L.nx = nx;
+  L.ny = ny;
+  L.nz = nz;
+  L.g = g;
+  L.elem = elem;
+  L.ex = nx + 2 * g;
+  L.ey = ny + 2 * g;
+  L.ez = nz + 2 * g;
+  const int64_t line = 128 / elem;  // elements per 128-byte line
+  L.xoff = (line - (g % line)) % line;
+  L.pitch = ((L.xoff + L.ex + line - 1) / line) * line;
+  L.sz = L.pitch * L.ey;
+  L.sq = L.sz * L.ez;
+  return L;
+}
+}  // namespace imx
+
+struct imexlb_lattice {
+  imexlb_params P{};
+  Layout L;
+  LaunchCfg cfg{};
+  DevArray<unsigned char> buf[2];
+  int cur = 0;
+  int64_t ncell = 0;
+  DevArray<double> mom;       // u, v, w, p (4 * ncell)
+  DevArray<double> prev_mom;  // u, v, w of the last residual call
+  bool have_prev = false;
+  DevArray<uint8_t> usr;      // interior mask (sphere)
+  DevArray<double> inlet;     // reference sphere inlet profile per z
+  DevArray<int64_t> gtgt, gsrc;
+  int64_t gn = 0;
+  DevArray<double> red;       // reduction partials + result
+  cudaStream_t stream = nullptr;
+  int64_t steps = 0;
+  std::vector<int32_t> usr_padded;  // host copy, padded box (reference sphere)
+  std::vector<int32_t> ran;
+  Encoding enc{};
+  double p_shift = 0;
+  StepArgs base_args;
+  // per-launch timing: (start, end, kind) with kind 0 = step, 1 = ghost gather
+  bool profiling = false;
+  struct Timed {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+  ~imexlb_lattice() {
+    std::vector<cudaEvent_t> all(event_pool);
+    for (auto& t : timed) {
+      if (std::find(all.begin(), all.end(), t.a) == all.end()) all.push_back(t.a);
+      if (std::find(all.begin(), all.end(), t.b) == all.end()) all.push_back(t.b);
+    }
+    for (auto e : all) cudaEventDestroy(e);
+  }
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+
+namespace {
+
+bool is_float_store(imexlb_storage s) { return s != IMEXLB_F64; }
+
+// Macroscopic initial fields over the box the layout stores (padded box for
+// reference boundaries, interior otherwise), x fastest.
+void init_fields(imexlb_lattice* h, std::vector<double>& U, std::vector<double>& V, std::vector<double>& W,
+                 std::vector<double>& Pf) {
+  const Layout& L = h->L;
+  const imexlb_params& P = h->P;
+  const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
+  U.assign(n, 0.0);
+  V.assign(n, 0.0);
+  W.assign(n, 0.0);
+  Pf.assign(n, 0.0);
+  const int g = L.g;
+  const int glx = P.nx, gly = P.ny, glz = P.nz;
+  auto at = [&](int i, int j, int k) { return static_cast<size_t>(i) + L.ex * (static_cast<size_t>(j) + L.ey * k); };
+  if (P.kase == IMEXLB_TGV) {
+    // tgv/src/lbm.cpp:195-206 (cs2 = 1/3)
+    const double u0 = P.u0, rho0 = P.rho0, cs2 = 1.0 / 3.0;
+    for (int k = 0; k < L.ez; ++k)
+      for (int j = 0; j < L.ey; ++j)
+        for (int i = 0; i < L.ex; ++i) {
+          const double X = static_cast<double>(i - g) / static_cast<double>(glx) * 2.0 * PI_REF;
+          const double Y = static_cast<double>(j - g) / static_cast<double>(gly) * 2.0 * PI_REF;
+          const double Z = static_cast<double>(k - g) / static_cast<double>(glz) * 2.0 * PI_REF;
+          const size_t c = at(i, j, k);
+          U[c] = u0 * std::sin(X) * std::cos(Y) * std::cos(Z);
+          V[c] = -u0 * std::cos(X) * std::sin(Y) * std::cos(Z);
+          W[c] = 0;
+          Pf[c] = rho0 * cs2 + rho0 * u0 * u0 / 16.0 * (std::cos(X * 2.0) + std::cos(Y * 2.0)) *
+                                   (std::cos(Z * 2.0) + 2.0);
+        }
+  } else if (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE) {
+    // sphere/src/lbm.cpp:231-242 over the padded box, with `ran` given
+    const double u0 = P.u0;
+    const int c8 = (glx - 1) / 8;
+    const double r = (glx - 1) / 64.0;
+    for (int k = 0; k < L.ez; ++k)
+      for (int j = 0; j < L.ey; ++j)
+        for (int i = 0; i < L.ex; ++i) {
+          const size_t c = at(i, j, k);
+          const int dx = i - GHOST - c8, dy = j - GHOST - c8, dz = k - GHOST - c8;
+          const double d2 = static_cast<double>(dx) * dx + static_cast<double>(dy) * dy + static_cast<double>(dz) * dz;
+          const int s = (d2 <= r * r) ? 0 : 1;
+          h->usr_padded[c] = s;
+          U[c] = (u0 * 4.0 * (k - GHOST) * (glz - 1 - (k - GHOST)) / (static_cast<double>(glz - 1) * (glz - 1))) * s *
+                 (1.0 + h->ran[c] * 0.001);
+        }
+  } else if (P.kase == IMEXLB_SPHERE) {
+    // standard channel: uniform inlet velocity in the fluid at rest pressure
+    const double ui = P.inlet_u;
+    for (int k = 0; k < L.ez; ++k)
+      for (int j = 0; j < L.ey; ++j)
+        for (int i = 0; i < L.ex; ++i) {
+          const size_t c = at(i, j, k);
+          const double dx = i - P.sphere_c[0], dy = j - P.sphere_c[1], dz = k - P.sphere_c[2];
+          const bool solid = dx * dx + dy * dy + dz * dz <= 0.25 * P.sphere_d * P.sphere_d;
+          h->usr_padded[c] = solid ? 0 : 1;
+          U[c] = solid ? 0.0 : ui;
+        }
+  }
+  // cavity (both boundary kinds): u = p = 0 (lid_driven_cavity/src/lbm.cpp:191-198)
+}
+
+int upload_case(imexlb_lattice* h) {
+  const Layout& L = h->L;
+  std::vector<double> U, V, W, Pf;
+  init_fields(h, U, V, W, Pf);
+  const size_t n = U.size();
+  DevArray<double> tmp;
+  IMX_CUDA(tmp.alloc(4 * n));
+  IMX_CUDA(cudaMemcpyAsync(tmp.p, U.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(tmp.p + n, V.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(tmp.p + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(tmp.p + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
+  IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
+  IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, tmp.p, tmp.p + n, tmp.p + 2 * n, tmp.p + 3 * n,
+                         h->p_shift, h->enc, h->stream));
+  // the views after Initialize: interior moments
+  std::vector<double> mom(4 * static_cast<size_t>(h->ncell));
+  for (int k = 0; k < L.nz; ++k)
+    for (int j = 0; j < L.ny; ++j)
+      for (int i = 0; i < L.nx; ++i) {
+        const size_t d = i + static_cast<size_t>(L.nx) * (j + static_cast<size_t>(L.ny) * k);
+        const size_t c = (i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g));
+        mom[d] = U[c];
+        mom[h->ncell + d] = V[c];
+        mom[2 * h->ncell + d] = W[c];
+        mom[3 * h->ncell + d] = Pf[c];
+      }
+  IMX_CUDA(cudaMemcpyAsync(h->mom.p, mom.data(), mom.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  // reference boundaries: the first step's passes act on the initial state
+  if (h->gn)
+    IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[0].p, h->buf[1].p, h->gtgt.p, h->gsrc.p, h->gn, L.sq, h->enc,
+                                 h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  h->cur = 0;
+  h->steps = 0;
+  h->have_prev = false;
+  return IMEXLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void imexlb_params_default(imexlb_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->kase = IMEXLB_TGV;
+  p->bc = IMEXLB_BC_REFERENCE;
+  p->storage = IMEXLB_F64;
+  p->arith = IMEXLB_ARITH_EXACT;
+  p->rho0 = 1.0;
+  p->u0 = 0.05;
+  p->seed = 5374857ULL;
+}
+
+int imexlb_system_read(const char* path, imexlb_case kase, imexlb_system* out) {
+  if (!path || !out) return fail(IMEXLB_E_ARG, "null argument");
+  std::ifstream in(path);
+  if (!in) return fail(IMEXLB_E_IO, std::string("cannot open ") + path);
+  imexlb_system s{};
+  s.cs2 = 1.0 / 3.0;
+  s.cs = std::sqrt(s.cs2);
+  // tgv/src/System.cpp:12-15: three lines of whitespace-separated numbers;
+  // Re, Time, inter, sx, sy, sz are integers
+  in >> s.rho0 >> s.R >> s.Re;
+  in >> s.u0 >> s.Time >> s.inter;
+  in >> s.sx >> s.sy >> s.sz;
+  if (!in) return fail(IMEXLB_E_IO, std::string("malformed input.in: ") + path);
+  s.Ma = s.u0 / s.cs;
+  if (kase == IMEXLB_TGV) {  // tgv/src/System.cpp:17-21
+    s.Time = 100;
+    s.inter = 10;
+    s.miu = s.rho0 * s.u0 * s.sx / 2 / 3.1415926 / s.Re;
+    s.tau = s.u0 * s.sx / s.Re / s.cs2 / 2 / 3.1415926;
+  } else {  // lid_driven_cavity/src/System.cpp:17-19
+    s.miu = s.rho0 * s.u0 * s.R / s.Re;
+    s.tau = s.u0 * s.R / s.Re / s.cs2;
+    if (kase == IMEXLB_SPHERE) {  // sphere/src/System.cpp:21-22
+      s.Time = static_cast<int>(std::pow(2 * s.R, 2) / s.miu);
+      s.inter = 1;
+    }
+  }
+  *out = s;
+  return IMEXLB_OK;
+}
+
+int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
+  if (!pin || !out) return fail(IMEXLB_E_ARG, "null argument");
+  *out = nullptr;
+  imexlb_params P = *pin;
+  if (P.kase < IMEXLB_TGV || P.kase > IMEXLB_SPHERE) return fail(IMEXLB_E_ARG, "unknown case");
+  if (P.bc != IMEXLB_BC_REFERENCE && P.bc != IMEXLB_BC_STANDARD) return fail(IMEXLB_E_ARG, "unknown boundary kind");
+  if (P.storage < IMEXLB_F64 || P.storage > IMEXLB_BF16) return fail(IMEXLB_E_ARG, "unknown storage");
+  if (P.nx < 2 || P.ny < 2 || P.nz < 2) return fail(IMEXLB_E_ARG, "lattice extents must be >= 2");
+  if (P.nz > 65535) return fail(IMEXLB_E_ARG, "nz above 65535");
+  if (!(P.tau0 > 0.0) || !std::isfinite(P.tau0)) return fail(IMEXLB_E_ARG, "tau0 must be positive");
+  const bool ref_sphere = P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE;
+  if (ref_sphere && (P.nx - 1) / 8 + (P.nx - 1) / 64.0 + 2 >= std::min(P.ny, P.nz))
+    return fail(IMEXLB_E_ARG, "reference sphere (centre (nx-1)/8 on every axis) does not fit in ny, nz");
+  if (P.kase == IMEXLB_CAVITY && P.bc == IMEXLB_BC_STANDARD && P.lid_u == 0.0) P.lid_u = P.u0;
+  if (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_STANDARD) {
+    if (P.inlet_u == 0.0) P.inlet_u = P.u0;
+    if (P.sphere_d == 0.0) P.sphere_d = P.nx / 24.0;
+    if (P.sphere_c[0] == 0.0 && P.sphere_c[1] == 0.0 && P.sphere_c[2] == 0.0) {
+      P.sphere_c[0] = P.nx / 4.0;
+      P.sphere_c[1] = P.ny / 2.0;
+      P.sphere_c[2] = P.nz / 2.0;
+    }
+  }
+
+  std::unique_ptr<imexlb_lattice> h(new imexlb_lattice);
+  h->P = P;
+  h->P.ran = nullptr;
+  h->stream = static_cast<cudaStream_t>(P.stream);
+  const bool ghost = P.bc == IMEXLB_BC_REFERENCE && P.kase != IMEXLB_TGV;
+  h->cfg.bc = P.kase == IMEXLB_TGV ? Bc::Periodic : (ghost ? Bc::Ghost : Bc::Standard);
+  h->cfg.store = static_cast<Store>(P.storage);
+  h->cfg.exact = P.storage == IMEXLB_F64 && P.arith == IMEXLB_ARITH_EXACT;
+  if (P.kase == IMEXLB_TGV)
+    h->cfg.rule = CaseRule::None;
+  else if (P.kase == IMEXLB_CAVITY)
+    h->cfg.rule = ghost ? CaseRule::CavityRef : CaseRule::CavityStd;
+  else
+    h->cfg.rule = ghost ? CaseRule::SphereRef : CaseRule::SphereStd;
+  const int elem = P.storage == IMEXLB_F64 ? 8 : (P.storage == IMEXLB_F32 ? 4 : 2);
+  h->L = make_layout(P.nx, P.ny, P.nz, ghost ? GHOST : 0, elem);
+  const Layout& L = h->L;
+  h->ncell = static_cast<int64_t>(P.nx) * P.ny * P.nz;
+
+  // reduced precision: deviations from the rest state, scaled per population
+  const double p_rest = P.kase == IMEXLB_TGV ? P.rho0 / 3.0 : 0.0;
+  h->p_shift = is_float_store(P.storage) ? p_rest : 0.0;
+  for (int q = 0; q < Q; ++q) {
+    const double t = weight_of_class(D3Q27::wclass[q]);
+    const double sc = P.storage == IMEXLB_F16 ? 16384.0 / t : (P.storage == IMEXLB_BF16 ? 1.0 / t : 1.0);
+    h->enc.scale[q] = static_cast<float>(sc);
+    h->enc.inv_scale[q] = static_cast<float>(1.0 / sc);
+  }
+
+  const size_t padded = static_cast<size_t>(L.ex) * L.ey * L.ez;
+  if (P.kase == IMEXLB_SPHERE) {
+    h->usr_padded.assign(padded, 1);
+    if (ref_sphere) {
+      h->ran.resize(padded);
+      if (pin->ran) {
+        std::memcpy(h->ran.data(), pin->ran, padded * sizeof(int32_t));
+      } else {
+        for (size_t c = 0; c < padded; ++c) h->ran[c] = static_cast<int32_t>(splitmix64(P.seed ^ c) % 100);
+      }
+    }
+  }
+
+  IMX_CUDA(h->buf[0].alloc(L.bytes()));
+  IMX_CUDA(h->buf[1].alloc(L.bytes()));
+  IMX_CUDA(h->mom.alloc(4 * static_cast<size_t>(h->ncell)));
+  IMX_CUDA(h->red.alloc(reduce_blocks() + 8));
+
+  // base step arguments
+  StepArgs& a = h->base_args;
+  a.nx = P.nx;
+  a.ny = P.ny;
+  a.nz = P.nz;
+  a.sq = L.sq;
+  a.sz = L.sz;
+  a.pitch = L.pitch;
+  a.base = L.idx(0, L.g, L.g, L.g);
+  for (int q = 0; q < Q; ++q)
+    a.off[q] = q * L.sq - (D3Q27::ez[q] * L.sz + D3Q27::ey[q] * L.pitch + D3Q27::ex[q]);
+  a.tau_half = P.tau0 + 0.5;
+  a.omega = 1.0 / (P.tau0 + 0.5);
+  a.mu = h->mom.p;
+  a.mv = h->mom.p + h->ncell;
+  a.mw = h->mom.p + 2 * h->ncell;
+  a.mp = h->mom.p + 3 * h->ncell;
+  a.lid_u = h->cfg.rule == CaseRule::CavityRef ? 0.1 : P.lid_u;  // reference lid: literal 0.1
+  a.rho_w = P.rho0;
+  a.inlet_u = P.inlet_u;
+  a.p_shift = h->p_shift;
+  a.enc = h->enc;
+
+  // initial fields need usr_padded before the mask goes to the device
+  if (P.kase == IMEXLB_SPHERE) {
+    std::vector<double> U, V, W, Pf;
+    init_fields(h.get(), U, V, W, Pf);  // fills usr_padded
+    std::vector<uint8_t> m(static_cast<size_t>(h->ncell));
+    for (int k = 0; k < P.nz; ++k)
+      for (int j = 0; j < P.ny; ++j)
+        for (int i = 0; i < P.nx; ++i)
+          m[i + static_cast<size_t>(P.nx) * (j + static_cast<size_t>(P.ny) * k)] = static_cast<uint8_t>(
+              h->usr_padded[(i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g))]);
+    IMX_CUDA(h->usr.alloc(m.size()));
+    IMX_CUDA(cudaMemcpy(h->usr.p, m.data(), m.size(), cudaMemcpyHostToDevice));
+    a.usr = h->usr.p;
+    if (ref_sphere) {
+      std::vector<double> prof(P.nz);
+      const int glz = P.nz;
+      for (int k = 0; k < P.nz; ++k)  // sphere/src/lbm.cpp:405
+        prof[k] = P.u0 * 4.0 * k * (glz - 1 - k) / std::pow(static_cast<double>(glz - 1), 2);
+      IMX_CUDA(h->inlet.alloc(prof.size()));
+      IMX_CUDA(cudaMemcpy(h->inlet.p, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
+      a.inlet = h->inlet.p;
+    } else {
+      // equilibrium populations of the inlet (deviation form)
+      const double ui = P.inlet_u;
+      for (int q = 0; q < Q; ++q) {
+        const double t = weight_of_class(D3Q27::wclass[q]);
+        const double e = D3Q27::ex[q] * ui;
+        a.feq_in[q] = t * (3.0 * (0.0 - h->p_shift) + 3.0 * e + 4.5 * e * e - 1.5 * ui * ui);
+      }
+    }
+  }
+
+  if (ghost) {
+    GhostPlan plan;
+    std::string err;
+    if (!build_ghost_plan_keys(static_cast<int>(P.kase), P.nx, P.ny, P.nz,
+                               P.kase == IMEXLB_SPHERE ? h->usr_padded.data() : nullptr, &plan, &err))
+      return fail(IMEXLB_E_UNSUPPORTED, err);
+    const int lx = P.nx + 2 * GHOST, ly = P.ny + 2 * GHOST;
+    auto to_dev = [&](int64_t key) {
+      const int q = static_cast<int>(key % Q);
+      int64_t c = key / Q;
+      const int i = static_cast<int>(c % lx);
+      c /= lx;
+      const int j = static_cast<int>(c % ly);
+      const int k = static_cast<int>(c / ly);
+      return L.idx(q, i, j, k);
+    };
+    std::vector<int64_t> t(plan.tgt.size()), s(plan.src.size());
+    for (size_t n = 0; n < t.size(); ++n) {
+      t[n] = to_dev(plan.tgt[n]);
+      const int64_t src = plan.src[n];
+      s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
+    }
+    h->gn = static_cast<int64_t>(t.size());
+    IMX_CUDA(h->gtgt.alloc(t.size()));
+    IMX_CUDA(h->gsrc.alloc(s.size()));
+    IMX_CUDA(cudaMemcpy(h->gtgt.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
+    IMX_CUDA(cudaMemcpy(h->gsrc.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice));
+  }
+
+  const int rc = upload_case(h.get());
+  if (rc) return rc;
+  *out = h.release();
+  return IMEXLB_OK;
+}
+
+int imexlb_initialize(imexlb_lattice* h) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  return upload_case(h);
+}
+
+int imexlb_step(imexlb_lattice* h, int nsteps) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (nsteps < 0) return fail(IMEXLB_E_ARG, "negative step count");
+  StepArgs a = h->base_args;
+  for (int s = 0; s < nsteps; ++s) {
+    a.src = h->buf[h->cur].p;
+    a.dst = h->buf[1 - h->cur].p;
+    a.store = s == nsteps - 1;
+    imexlb_lattice::Timed t0{nullptr, nullptr, 0}, t1{nullptr, nullptr, 1};
+    if (h->profiling) {
+      t0.a = h->take_event();
+      t0.b = h->take_event();
+      IMX_CUDA(cudaEventRecord(t0.a, h->stream));
+    }
+    IMX_CUDA(launch_step(h->cfg, a, h->stream));
+    if (h->profiling) {
+      IMX_CUDA(cudaEventRecord(t0.b, h->stream));
+      h->timed.push_back(t0);
+    }
+    if (h->gn) {
+      if (h->profiling) {
+        t1.a = t0.b;
+        t1.b = h->take_event();
+      }
+      IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[1 - h->cur].p, h->buf[h->cur].p, h->gtgt.p, h->gsrc.p, h->gn,
+                                   h->L.sq, h->enc, h->stream));
+      if (h->profiling) {
+        IMX_CUDA(cudaEventRecord(t1.b, h->stream));
+        h->timed.push_back(t1);
+      }
+    }
+    h->cur = 1 - h->cur;
+    ++h->steps;
+  }
+  return IMEXLB_OK;
+}
+
+int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double* p) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  double* dst[4] = {u, v, w, p};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c])
+      IMX_CUDA(cudaMemcpyAsync(dst[c], h->mom.p + c * h->ncell, h->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  return IMEXLB_OK;
+}
+
+int imexlb_get_mask(imexlb_lattice* h, int32_t* usr) {
+  if (!h || !usr) return fail(IMEXLB_E_ARG, "null argument");
+  const Layout& L = h->L;
+  for (int k = 0; k < L.nz; ++k)
+    for (int j = 0; j < L.ny; ++j)
+      for (int i = 0; i < L.nx; ++i) {
+        const size_t d = i + static_cast<size_t>(L.nx) * (j + static_cast<size_t>(L.ny) * k);
+        usr[d] = h->usr_padded.empty()
+                     ? 1
+                     : h->usr_padded[(i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g))];
+      }
+  return IMEXLB_OK;
+}
+
+int imexlb_write_tecplot(imexlb_lattice* h, const char* path, int n) {
+  if (!h || !path) return fail(IMEXLB_E_ARG, "null argument");
+  const int64_t N = h->ncell;
+  std::vector<double> f(4 * static_cast<size_t>(N));
+  const int rc = imexlb_get_fields(h, f.data(), f.data() + N, f.data() + 2 * N, f.data() + 3 * N);
+  if (rc) return rc;
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(IMEXLB_E_IO, std::string("cannot open ") + path);
+  std::vector<unsigned char> hdr;
+  auto put = [&](const void* x, size_t nb) {
+    const unsigned char* c = static_cast<const unsigned char*>(x);
+    hdr.insert(hdr.end(), c, c + nb);
+  };
+  auto I = [&](int32_t x) { put(&x, 4); };
+  auto F = [&](float x) { put(&x, 4); };
+  auto D = [&](double x) { put(&x, 8); };
+  // header of tgv/src/lbm.cpp:467-647: magic, byte order, file type, title,
+  // 7 variable names, zone "ZONE 001", solution time, ordered zone extents,
+  // data section with FP64 variables and their min/max
+  put("#!TDV112", 8);
+  I(1);
+  I(0);
+  I(0);
+  I(7);
+  for (char c : std::string("xyzuvwp")) {
+    I(c);
+    I(0);
+  }
+  F(299.0f);
+  for (char c : std::string("ZONE 001")) I(c);
+  I(0);
+  I(-1);
+  D(static_cast<double>(n));
+  I(0);
+  I(-1);
+  I(0);
+  I(0);
+  I(0);
+  I(0);
+  I(h->P.nx);
+  I(h->P.ny);
+  I(h->P.nz);
+  I(0);
+  F(357.0f);
+  F(299.0f);
+  for (int c = 0; c < 7; ++c) I(2);
+  I(0);
+  I(0);
+  I(-1);
+  for (int c = 0; c < 3; ++c) {
+    D(0.0);
+    D(1.0);
+  }
+  for (int c = 0; c < 4; ++c) {
+    const double* a = f.data() + c * N;
+    double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
+    for (int64_t e = 0; e < N; ++e) {
+      if (a[e] > mx) mx = a[e];
+      if (a[e] < mn) mn = a[e];
+    }
+    D(mn);
+    D(mx);
+  }
+  bool ok = std::fwrite(hdr.data(), 1, hdr.size(), fp) == hdr.size();
+  std::vector<double> coord(static_cast<size_t>(N));
+  const int ext[3] = {h->P.nx, h->P.ny, h->P.nz};
+  for (int axis = 0; axis < 3 && ok; ++axis) {
+    for (int k = 0; k < h->P.nz; ++k)
+      for (int j = 0; j < h->P.ny; ++j)
+        for (int i = 0; i < h->P.nx; ++i) {
+          const int c = axis == 0 ? i : (axis == 1 ? j : k);
+          coord[i + static_cast<size_t>(h->P.nx) * (j + static_cast<size_t>(h->P.ny) * k)] =
+              static_cast<double>(c) / (ext[axis] - 1);
+        }
+    ok = std::fwrite(coord.data(), 8, N, fp) == static_cast<size_t>(N);
+  }
+  if (ok) ok = std::fwrite(f.data(), 8, 4 * N, fp) == static_cast<size_t>(4 * N);
+  if (std::fclose(fp) != 0 || !ok) return fail(IMEXLB_E_IO, std::string("write failed: ") + path);
+  return IMEXLB_OK;
+}
+
+int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
+  if (!h || !out) return fail(IMEXLB_E_ARG, "null argument");
+  const int64_t N = h->ncell;
+  const double* u = h->mom.p;
+  const double* v = u + N;
+  const double* w = u + 2 * N;
+  const double* p = u + 3 * N;
+  double* part = h->red.p;
+  double* res = h->red.p + reduce_blocks();
+  switch (kind) {
+    case IMEXLB_REDUCE_MASS:
+      IMX_CUDA(launch_reduce(RedKind::Mass, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_KINETIC:
+      IMX_CUDA(launch_reduce(RedKind::Kinetic, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_UMAX:
+      IMX_CUDA(launch_reduce(RedKind::UMax, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_RESIDUAL: {
+      if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N)));
+      double num = 0, den = 0;
+      if (h->have_prev) {
+        IMX_CUDA(launch_reduce(RedKind::DiffSq, u, v, w, p, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N,
+                               part, res, h->stream));
+        IMX_CUDA(cudaMemcpyAsync(&num, res, 8, cudaMemcpyDeviceToHost, h->stream));
+        IMX_CUDA(launch_reduce(RedKind::NormSq, u, v, w, p, nullptr, nullptr, nullptr, N, part, res + 1, h->stream));
+        IMX_CUDA(cudaMemcpyAsync(&den, res + 1, 8, cudaMemcpyDeviceToHost, h->stream));
+      }
+      IMX_CUDA(cudaMemcpyAsync(h->prev_mom.p, u, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      IMX_CUDA(cudaStreamSynchronize(h->stream));
+      const bool first = !h->have_prev;
+      h->have_prev = true;
+      *out = first ? INFINITY : (den > 0 ? std::sqrt(num / den) : (num > 0 ? INFINITY : 0.0));
+      if (!std::isfinite(num) || !std::isfinite(den))
+        return fail(IMEXLB_E_STATE, "lattice is not finite (NaN/Inf in the velocity field)");
+      return IMEXLB_OK;
+    }
+    default:
+      return fail(IMEXLB_E_ARG, "unknown or unsupported reduction");
+  }
+  IMX_CUDA(cudaMemcpyAsync(out, res, 8, cudaMemcpyDeviceToHost, h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  if (!std::isfinite(*out)) return fail(IMEXLB_E_STATE, "lattice is not finite (NaN/Inf in the moments)");
+  return IMEXLB_OK;
+}
+
+int imexlb_steps_taken(const imexlb_lattice* h, int64_t* steps) {
+  if (!h || !steps) return fail(IMEXLB_E_ARG, "null argument");
+  *steps = h->steps;
+  return IMEXLB_OK;
+}
+
+int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* bytes_per_cell_update) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (device_bytes)
+    *device_bytes = h->buf[0].n + h->buf[1].n + h->mom.n * 8 + h->prev_mom.n * 8 + h->usr.n + h->inlet.n * 8 +
+                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->red.n * 8;
+  if (bytes_per_cell_update) *bytes_per_cell_update = 2.0 * Q * h->L.elem;
+  return IMEXLB_OK;
+}
+
+int imexlb_ghost_plan(imexlb_case kase, int nx, int ny, int nz, const int32_t* usr_padded, int64_t* tgt,
+                      int64_t* src, int64_t* n) {
+  if (!n) return fail(IMEXLB_E_ARG, "null count");
+  if (nx < 2 || ny < 2 || nz < 2) return fail(IMEXLB_E_ARG, "lattice extents must be >= 2");
+  GhostPlan plan;
+  std::string err;
+  if (!build_ghost_plan_keys(static_cast<int>(kase), nx, ny, nz, usr_padded, &plan, &err))
+    return fail(IMEXLB_E_UNSUPPORTED, err);
+  const int64_t m = static_cast<int64_t>(plan.tgt.size());
+  if (tgt && src) {
+    if (*n < m) return fail(IMEXLB_E_ARG, "output arrays too small");
+    std::memcpy(tgt, plan.tgt.data(), m * sizeof(int64_t));
+    std::memcpy(src, plan.src.data(), m * sizeof(int64_t));
+  }
+  *n = m;
+  return IMEXLB_OK;
+}
+
+int imexlb_profile(imexlb_lattice* h, int enable) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  h->profiling = enable != 0;
+  return IMEXLB_OK;
+}
+
+int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out) {
+  if (!h || !out) return fail(IMEXLB_E_ARG, "null argument");
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  *out = imexlb_kernel_times{0.0, 0.0, 0, 0};
+  std::vector<cudaEvent_t> done;
+  for (auto& t : h->timed) {
+    float ms = 0.f;
+    IMX_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+    if (t.kind == 0) {
+      out->step_ms += ms;
+      ++out->step_launches;
+    } else {
+      out->ghost_ms += ms;
+      ++out->ghost_launches;
+    }
+  }
+  // a gather's start event is its step's end event: release each event once
+  for (auto& t : h->timed) {
+    if (std::find(done.begin(), done.end(), t.a) == done.end()) done.push_back(t.a);
+    if (std::find(done.begin(), done.end(), t.b) == done.end()) done.push_back(t.b);
+  }
+  h->event_pool.insert(h->event_pool.end(), done.begin(), done.end());
+  h->timed.clear();
+  h->profiling = false;
+  return IMEXLB_OK;
+}
+
+int imexlb_synchronize(imexlb_lattice* h) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  return IMEXLB_OK;
+}
+
+void imexlb_destroy(imexlb_lattice* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->stream);
+  delete h;
+}
+
+const char* imexlb_last_error(void) { return g_last_error.c_str(); }
+
+const char* imexlb_version(void) { return "imexlb-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

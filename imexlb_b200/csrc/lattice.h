@@ -1,0 +1,115 @@
+// Internal declarations shared by the host runtime (lattice.cu) and the
+// device kernels (kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "d3q27.cuh"
+
+namespace imx {
+
+enum class Bc : int { Periodic = 0, Ghost = 1, Standard = 2 };
+enum class Store : int { F64 = 0, F32 = 1, F16 = 2, BF16 = 3 };
+// Which per-cell rules the step applies after the moments.
+enum class CaseRule : int {
+  None = 0,         // TGV
+  CavityRef = 1,    // lid velocity forced on the top plane (Update)
+  SphereRef = 2,    // solid mask times moments, inlet profile, outlet p = 0
+  CavityStd = 3,    // moving-lid halfway bounce-back
+  SphereStd = 4     // channel: equilibrium inlet, zero-gradient outlet, solid sphere
+};
+
+// Storage layout of one distribution buffer: 27 population planes, each a
+// (z, y, x) box of stored extents (n + 2g) with x fastest.  Stored x = 0 sits
+// `xoff` elements into its row so that interior x = 0 starts on a 128-byte
+// boundary; rows, planes and populations are padded to 128 bytes.
+struct Layout {
+  int nx = 0, ny = 0, nz = 0;  // interior
+  int g = 0;                   // stored ghost width (3 for reference boundaries)
+  int ex = 0, ey = 0, ez = 0;  // stored extents
+  int64_t xoff = 0, pitch = 0, sz = 0, sq = 0;
+  int elem = 8;  // bytes per stored value
+  IMX_HD int64_t idx(int q, int i, int j, int k) const {  // stored coordinates
+    return q * sq + k * sz + j * pitch + xoff + i;
+  }
+  IMX_HD int64_t interior(int q, int i, int j, int k) const { return idx(q, i + g, j + g, k + g); }
+  size_t bytes() const { return static_cast<size_t>(sq) * Q * elem; }
+};
+Layout make_layout(int nx, int ny, int nz, int g, int elem);
+
+// Per-population scaling of reduced-precision storage:
+// stored = d_q * scale[q], d_q = stored * inv_scale[q], where d_q is the
+// deviation f_q - 3 w_q p_shift.
+struct Encoding {
+  float scale[Q];
+  float inv_scale[Q];
+};
+
+struct StepArgs {
+  const void* src = nullptr;
+  void* dst = nullptr;
+  const void* prev = nullptr;  // ghost gather: buffer of the previous step
+  int nx = 0, ny = 0, nz = 0;
+  int64_t sq = 0, sz = 0, pitch = 0;
+  int64_t base = 0;    // stored index of interior cell (0,0,0), population 0
+  int64_t off[Q] = {}; // pull offset of population q relative to a cell's base index
+  double tau_half = 1; // tau0 + 0.5
+  double omega = 1;    // 1 / (tau0 + 0.5)
+  double* mu = nullptr;
+  double* mv = nullptr;
+  double* mw = nullptr;
+  double* mp = nullptr;
+  int store = 0;  // write moments this step
+  const uint8_t* usr = nullptr;  // interior mask, 1 = fluid (sphere)
+  const double* inlet = nullptr; // per interior z: reference inlet velocity
+  double lid_u = 0;       // standard cavity lid speed; reference lid value
+  double rho_w = 1;       // wall density of the moving-wall term
+  double inlet_u = 0;     // standard sphere inlet velocity
+  double feq_in[Q] = {};  // standard sphere: inlet equilibrium (deviation form)
+  double p_shift = 0;     // rest pressure removed from stored values (0 for FP64)
+  Encoding enc;
+};
+
+// Ghost-slot plan for reference boundaries: after each step, slot tgt[n] of
+// the new buffer receives the value named by src[n]:
+//   src >= 0       the new buffer at index src (this step's post-collision)
+//   src == -1      zero
+//   src <= -2      the previous buffer at index (-src - 2)
+struct GhostPlan {
+  std::vector<int64_t> tgt, src;
+};
+
+// Build the plan in reference slot keys: key = q + 27*(i + lx*(j + ly*k)) over
+// the padded box (lx = nx + 6).  Same encoding of src as GhostPlan.
+// usr_padded: solid mask over the padded box (sphere), may be null.
+// Returns false and sets *err if the passes would race.
+bool build_ghost_plan_keys(int kase, int nx, int ny, int nz, const int32_t* usr_padded, GhostPlan* out,
+                           std::string* err);
+
+// ---------------------------------------------------------------- launchers
+struct LaunchCfg {
+  Bc bc;
+  Store store;
+  CaseRule rule;
+  bool exact;
+};
+
+cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void* buf1, const double* u,
+                          const double* v, const double* w, const double* p, double p_shift, const Encoding& enc,
+                          cudaStream_t s);
+cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s);
+cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
+                                int64_t n, int64_t sq, const Encoding& enc, cudaStream_t s);
+// Deterministic FP64 sums over n values: out[c] = sum of comp(c) over cells
+// for the requested quantity; partial sums of `blocks` blocks go to scratch.
+enum class RedKind : int { Mass = 0, Kinetic = 1, DiffSq = 2, NormSq = 3, UMax = 4 };
+int reduce_blocks();
+cudaError_t launch_reduce(RedKind k, const double* u, const double* v, const double* w, const double* p,
+                          const double* u2, const double* v2, const double* w2, int64_t n, double* scratch,
+                          double* out, cudaStream_t s);
+
+}  // namespace imx

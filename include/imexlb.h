@@ -1,0 +1,193 @@
+/* imexlb-b200: C ABI of the B200 (sm_100a) D3Q27 lattice-Boltzmann step.
+ *
+ * This is the drop-in boundary for the imexlb proxy apps' solver.  The
+ * reference has no library interface: its "API" is the System class (input.in
+ * parsing, tgv/src/System.hpp) and the LBM struct's member functions
+ * (tgv/src/lbm.hpp:238-251) called by each case's main().  Every entry point
+ * below names the reference function it replaces.
+ *
+ * Conventions: every function returns 0 on success and a nonzero IMEXLB_E_*
+ * code on failure (no exception crosses the ABI); imexlb_last_error() gives
+ * the message of the calling thread's last failure.  The library owns all
+ * device memory; callers own host buffers.  A lattice handle belongs to one
+ * host thread at a time.  Host arrays are interior fields with x fastest:
+ * index i + nx*(j + ny*k), the Fortran order MPIoutput writes
+ * (tgv/src/lbm.cpp:361-377).
+ */
+#ifndef IMEXLB_H
+#define IMEXLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IMEXLB_Q 27
+
+enum {
+  IMEXLB_OK = 0,
+  IMEXLB_E_ARG = 1,      /* invalid argument */
+  IMEXLB_E_CUDA = 2,     /* CUDA runtime error (message has the CUDA text) */
+  IMEXLB_E_IO = 3,       /* file error */
+  IMEXLB_E_NOMEM = 4,    /* device or host allocation failed */
+  IMEXLB_E_STATE = 5,    /* call out of order, or the lattice went non-finite */
+  IMEXLB_E_UNSUPPORTED = 6
+};
+
+/* The three proxy apps (tgv/, lid_driven_cavity/, sphere/). */
+typedef enum imexlb_case { IMEXLB_TGV = 0, IMEXLB_CAVITY = 1, IMEXLB_SPHERE = 2 } imexlb_case;
+
+/* Boundary treatment.
+ * IMEXLB_BC_REFERENCE: the reference's own boundary passes, bit for bit,
+ *   including their ghost-slot chains (lid_driven_cavity/src/lbm.cpp:231-317,
+ *   sphere/src/lbm.cpp:274-371) and forced moments (Update).  TGV is
+ *   periodic either way.
+ * IMEXLB_BC_STANDARD: halfway bounce-back with the moving-wall correction
+ *   -2 w_i rho (c_i . u_w)/cs^2 on the cavity lid; for the sphere a periodic
+ *   channel with an equilibrium inlet, a zero-gradient outlet and halfway
+ *   bounce-back on a voxelised sphere (momentum-exchange drag available). */
+typedef enum imexlb_bc { IMEXLB_BC_REFERENCE = 0, IMEXLB_BC_STANDARD = 1 } imexlb_bc;
+
+/* Storage of the distributions in HBM.  F64 stores f_i; F32/F16/BF16 store
+ * the deviation f_i - w_i * 3 p_ref scaled per population, and collide in FP32. */
+typedef enum imexlb_storage {
+  IMEXLB_F64 = 0,
+  IMEXLB_F32 = 1,
+  IMEXLB_F16 = 2,
+  IMEXLB_BF16 = 3
+} imexlb_storage;
+
+/* FP64 arithmetic mode.  EXACT keeps the reference's operation order with
+ * one rounding per operation (bit-identical to the reference); FAST lets
+ * multiply-adds fuse and divides by constants become multiplies (agrees with
+ * the reference to ~1e-15 relative). */
+typedef enum imexlb_arith { IMEXLB_ARITH_EXACT = 0, IMEXLB_ARITH_FAST = 1 } imexlb_arith;
+
+/* System (tgv/src/System.hpp:9-15): the nine input.in numbers and what the
+ * constructor derives from them. */
+typedef struct imexlb_system {
+  double rho0, R;
+  int Re;
+  double u0;
+  int Time, inter;
+  int sx, sy, sz;
+  double miu, tau, Ma, cs2, cs;
+} imexlb_system;
+
+typedef struct imexlb_params {
+  imexlb_case kase;
+  imexlb_bc bc;
+  imexlb_storage storage;
+  imexlb_arith arith;   /* FP64 storage only */
+  int nx, ny, nz;       /* interior lattice (glx, gly, glz) */
+  double tau0;          /* 3 nu: System::tau; the relaxation time is tau0 + 0.5 */
+  double rho0, u0;      /* LBM::rho0, LBM::u0 */
+  /* Sphere, reference boundaries: padded (nx+6)(ny+6)(nz+6) integer field
+   * `ran` (x fastest) of sphere/src/lbm.cpp:221-229; NULL = derive it from
+   * `seed` with this library's generator. */
+  const int32_t* ran;
+  uint64_t seed;
+  /* Standard boundaries: lid velocity (cavity, along +x), inlet velocity,
+   * sphere diameter and centre (sphere channel).  Zero = BASELINE defaults. */
+  double lid_u;
+  double inlet_u;
+  double sphere_d;
+  double sphere_c[3];
+  void* stream; /* cudaStream_t to run on; NULL = the legacy default stream */
+} imexlb_params;
+
+typedef struct imexlb_lattice imexlb_lattice;
+
+/* Fill *p with defaults (FP64, EXACT, reference boundaries). */
+void imexlb_params_default(imexlb_params* p);
+
+/* System::System (tgv/src/System.cpp:5-24, lid_driven_cavity/src/System.cpp:5-20,
+ * sphere/src/System.cpp:5-23): parse `path` (an input.in) for `kase`,
+ * including the per-case overrides of Time and inter. */
+int imexlb_system_read(const char* path, imexlb_case kase, imexlb_system* out);
+
+/* LBM::LBM + LBM::Initialize (tgv/src/lbm.hpp:161-236, tgv/src/lbm.cpp:7-221):
+ * allocate the lattice on the current CUDA device and set the initial state. */
+int imexlb_create(const imexlb_params* p, imexlb_lattice** out);
+
+/* LBM::Initialize again (tgv/main.cpp:68): reset to the initial state. */
+int imexlb_initialize(imexlb_lattice* h);
+
+/* nsteps x { Collision; pack; exchange; unpack; Streaming; Update }
+ * (tgv/main.cpp:70-134, lid_driven_cavity/main.cpp:67-83), fused into one
+ * kernel per step (plus one small ghost-slot kernel for reference
+ * boundaries).  Asynchronous on the lattice's stream. */
+int imexlb_step(imexlb_lattice* h, int nsteps);
+
+/* The ua, va, wa, p views after the last step (interior, x fastest; any
+ * pointer may be NULL).  Synchronises the lattice's stream. */
+int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double* p);
+
+/* The usr view (sphere solid mask, 1 = fluid; interior, x fastest). */
+int imexlb_get_mask(imexlb_lattice* h, int32_t* usr);
+
+/* LBM::MPIoutput(n) at one rank (tgv/src/lbm.cpp:335-669): the 332-byte
+ * #!TDV112 header and x, y, z, u, v, w, p as FP64, written to `path`. */
+int imexlb_write_tecplot(imexlb_lattice* h, const char* path, int n);
+
+/* FP64 reductions over the interior after the last step. */
+enum {
+  IMEXLB_REDUCE_MASS = 0,     /* sum of 3p                          */
+  IMEXLB_REDUCE_KINETIC = 1,  /* sum of (u^2+v^2+w^2)/2              */
+  IMEXLB_REDUCE_RESIDUAL = 2, /* sqrt(sum|u-u_prev|^2 / sum|u|^2) between the
+                                 last two calls of this reduction     */
+  IMEXLB_REDUCE_DRAG = 3,     /* momentum-exchange force on the sphere at the
+                                 last step, out[0..2] (standard sphere) */
+  IMEXLB_REDUCE_UMAX = 4      /* max |u|                             */
+};
+int imexlb_reduce(imexlb_lattice* h, int kind, double* out);
+
+/* Number of steps taken since the last (re)initialisation. */
+int imexlb_steps_taken(const imexlb_lattice* h, int64_t* steps);
+
+/* Device bytes the lattice holds, and HBM bytes one step moves by design. */
+int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* bytes_per_cell_update);
+
+/* Host-only: the ghost-slot plan that reference boundaries apply after every
+ * step (the reference's unpack + boundary passes at one rank, resolved into
+ * one copy per slot; lid_driven_cavity/src/lbm.cpp:231-301,
+ * sphere/src/lbm.cpp:274-356).  Slots are keyed as the reference stores f:
+ * key = q + 27*(i + lx*(j + ly*k)) over the padded box, lx = nx + 6.  After a
+ * step, slot tgt[n] takes: src[n] >= 0 -> that slot of this step's
+ * post-collision state; src[n] == -1 -> zero; src[n] <= -2 -> slot
+ * (-src[n] - 2) as it stood after the previous step.  usr_padded is the
+ * sphere's padded solid mask (NULL for the cavity).  Call with tgt = src =
+ * NULL to get the count in *n. */
+int imexlb_ghost_plan(imexlb_case kase, int nx, int ny, int nz, const int32_t* usr_padded, int64_t* tgt,
+                      int64_t* src, int64_t* n);
+
+/* Per-launch device timing (CUDA events on the lattice's stream around each
+ * kernel launch), for roofline measurement.  imexlb_profile(h, 1) starts
+ * recording, imexlb_profile_read() waits, sums the durations since the start
+ * and stops recording.  No counterpart in the reference (it times phases
+ * with MPI_Wtime, tgv/main.cpp:74-119). */
+typedef struct imexlb_kernel_times {
+  double step_ms;  /* fused step kernels */
+  double ghost_ms; /* ghost-slot gathers (reference boundaries) */
+  int64_t step_launches, ghost_launches;
+} imexlb_kernel_times;
+int imexlb_profile(imexlb_lattice* h, int enable);
+int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out);
+
+/* Wait for all work queued on the lattice's stream. */
+int imexlb_synchronize(imexlb_lattice* h);
+
+void imexlb_destroy(imexlb_lattice* h);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* imexlb_last_error(void);
+
+/* Library version string. */
+const char* imexlb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMEXLB_H */

@@ -144,15 +144,16 @@ class RefSystem(ctypes.Structure):
                 ("cs2", ctypes.c_double), ("cs", ctypes.c_double)]
 
 
-def reference_available(case: str) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{case}.so"))
+def reference_available(case: str, fast: bool = False) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_{case}{'_fast' if fast else ''}.so"))
 
 
 class Reference:
-    """The reference's own solver (oracle/_ref) for one case."""
+    """The reference's own solver (oracle/_ref) for one case.  fast=True loads
+    the build without the stand-in's view bounds checks (for timing)."""
 
-    def __init__(self, case: str):
-        path = os.path.join(HERE, "_ref", f"libref_{case}.so")
+    def __init__(self, case: str, fast: bool = False):
+        path = os.path.join(HERE, "_ref", f"libref_{case}{'_fast' if fast else ''}.so")
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.case = case

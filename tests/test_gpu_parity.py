@@ -1,0 +1,123 @@
+"""GPU parity: the fused sm_100a step against the oracle and the reference fixtures.
+
+Bars (each written in the test):
+* FP64 EXACT arithmetic: bit-identical u, v, w, p to the oracle (which is
+  itself bit-identical to the reference's own solver build).
+* FP64 FAST arithmetic: max |diff| <= 1e-12 * max |reference| per field.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.bindings import Oracle, oracle_system
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["tgv_8x8x8_s10", "tgv_10x12x9_s7", "cavity_8x8x8_s20", "cavity_9x11x10_s12", "sphere_72x12x12_s4"]
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    from imexlb_b200 import api as a
+
+    return a
+
+
+def _rel(got, want):
+    scale = max(np.abs(want).max(), 1e-300)
+    return np.abs(got - want).max() / scale
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_exact_matches_reference_fixture(api, golden_dir, name):
+    m = json.load(open(os.path.join(golden_dir, "manifest.json")))[name]
+    data = np.load(os.path.join(golden_dir, f"ref_{name}.npz"))
+    ran = data["ran"].astype(np.int32) if "ran" in data else None
+    with api.LBM(m["case"], m["nx"], m["ny"], m["nz"], m["tau"], m["rho0"], m["u0"], ran=ran) as lbm:
+        lbm.step(m["steps"])
+        got = lbm.fields()
+    for k in "uvwp":
+        assert np.array_equal(got[k], data[k]), f"{k}: max |diff| {np.abs(got[k] - data[k]).max()}"
+
+
+PARITY = [
+    ("tgv", 1.0, 0.1, 100, 0.05, 32, 32, 32, 40),
+    ("tgv", 1.0, 0.1, 1600, 0.05, 24, 20, 28, 25),
+    ("cavity", 1.0, 16.0, 100, 0.1, 16, 16, 16, 60),
+    ("cavity", 1.0, 20.0, 400, 0.1, 20, 18, 22, 33),
+    ("sphere", 1.0, 3.0, 100, 0.1, 96, 20, 20, 12),
+]
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("case,rho0,R,Re,u0,nx,ny,nz,steps", PARITY)
+def test_fp64_matches_oracle(api, case, rho0, R, Re, u0, nx, ny, nz, steps, arith):
+    tau = oracle_system(case, rho0, R, Re, u0, steps, 1, nx)["tau"]
+    ran = None
+    if case == "sphere":
+        ran = np.random.default_rng(11).integers(0, 100, size=(nz + 6) * (ny + 6) * (nx + 6), dtype=np.int32)
+    o = Oracle(case, nx, ny, nz, tau, rho0, u0, ran)
+    o.initialize()
+    o.step(steps)
+    want = dict(zip("uvwp", o.moments()))
+    with api.LBM(case, nx, ny, nz, tau, rho0, u0, ran=ran, arith=arith) as lbm:
+        lbm.step(steps)
+        got = lbm.fields()
+    for k in "uvwp":
+        if arith == "exact":
+            assert np.array_equal(got[k], want[k]), f"{k}: max |diff| {np.abs(got[k] - want[k]).max()}"
+        else:
+            assert _rel(got[k], want[k]) <= 1e-12, f"{k}: rel {_rel(got[k], want[k])}"
+
+
+def test_split_calls_equal_one_call(api):
+    """step(a); step(b) == step(a + b), and Initialize() resets."""
+    tau = oracle_system("cavity", 1.0, 12.0, 100, 0.1, 1, 1, 12)["tau"]
+    with api.LBM("cavity", 12, 12, 12, tau, 1.0, 0.1) as lbm:
+        lbm.step(7)
+        lbm.step(5)
+        a = lbm.fields()
+        lbm.Initialize()
+        lbm.step(12)
+        b = lbm.fields()
+        assert lbm.steps_taken() == 12
+    for k in "uvwp":
+        assert np.array_equal(a[k], b[k])
+
+
+def test_initial_fields_are_initialize_views(api):
+    """Before any step the fields are the views Initialize sets."""
+    o = Oracle("tgv", 16, 16, 16, 0.01, 1.0, 0.05)
+    o.initialize()
+    want = dict(zip("uvwp", o.moments()))
+    with api.LBM("tgv", 16, 16, 16, 0.01, 1.0, 0.05) as lbm:
+        got = lbm.fields()
+    for k in "uvwp":
+        assert np.array_equal(got[k], want[k])
+
+
+def test_tecplot_matches_oracle_bytes(api, tmp_path):
+    tau = oracle_system("cavity", 1.0, 8.0, 100, 0.1, 1, 1, 8)["tau"]
+    o = Oracle("cavity", 8, 8, 8, tau, 1.0, 0.1)
+    o.initialize()
+    o.step(10)
+    o.write_tecplot(str(tmp_path / "want.plt"), 2)
+    with api.LBM("cavity", 8, 8, 8, tau, 1.0, 0.1) as lbm:
+        lbm.step(10)
+        path = lbm.MPIoutput(2, str(tmp_path))
+    assert open(path, "rb").read() == open(tmp_path / "want.plt", "rb").read()
+
+
+def test_mass_conserved_tgv(api):
+    with api.LBM("tgv", 24, 24, 24, 0.02, 1.0, 0.05) as lbm:
+        lbm.step(1)
+        m0 = lbm.reduce("mass")
+        lbm.step(200)
+        m1 = lbm.reduce("mass")
+    assert abs(m1 - m0) <= 1e-10 * abs(m0)
