@@ -57,6 +57,14 @@ WORKLOADS = {
                        u0=0.05, R=0.1, lid_u=0.0),
     "cavity128-f16": dict(case="cavity", bc="standard", storage="f16", arith="fast", n=(128, 128, 128), Re=1000,
                           u0=0.1, R=128.0, lid_u=0.1),
+    "cavity128-f64-refbc-fast": dict(case="cavity", bc="reference", storage="f64", arith="fast", n=(128, 128, 128),
+                                     Re=1000, u0=0.1, R=128.0, lid_u=0.1),
+    "cavity128-bf16": dict(case="cavity", bc="standard", storage="bf16", arith="fast", n=(128, 128, 128), Re=1000,
+                           u0=0.1, R=128.0, lid_u=0.1),
+    "cavity256-f64": dict(case="cavity", bc="standard", storage="f64", arith="fast", n=(256, 256, 256), Re=1000,
+                          u0=0.1, R=256.0, lid_u=0.1),
+    "cavity256-f16": dict(case="cavity", bc="standard", storage="f16", arith="fast", n=(256, 256, 256), Re=1000,
+                          u0=0.1, R=256.0, lid_u=0.1),
     "cavity128-f32": dict(case="cavity", bc="standard", storage="f32", arith="fast", n=(128, 128, 128), Re=1000,
                           u0=0.1, R=128.0, lid_u=0.1),
 }

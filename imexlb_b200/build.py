@@ -68,8 +68,9 @@ def build(verbose: bool = False, ptxas: bool = False, force: bool = False) -> st
         if not os.path.exists(src):
             continue
         if force or _stale(exe, [src, LIB, os.path.join(CSRC, "apps", "driver.h")]):
-            cmd = [cc, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", exe, src,
-                   "-L", HERE, "-limexlb", "-Xlinker", "-rpath,$ORIGIN/.."]
+            cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+            cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", exe, src,
+                   "-L", HERE, "-limexlb", "-Wl,-rpath,$ORIGIN/.."]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

@@ -27,6 +27,8 @@
 namespace imx {
 namespace {
 
+constexpr int RED_THREADS_DRAG = 256;
+
 template <int A, int B, class F>
 __device__ __forceinline__ void static_for(F&& f) {
   if constexpr (A < B) {
@@ -76,6 +78,22 @@ __device__ __forceinline__ R edu_of(R u, R v, R w) {
   return t;
 }
 
+// RN(x / 3) in three FP64 operations (Markstein's correction step: P.
+// Markstein, IBM J. Res. Dev. 34(1), 1990).  With z = RN(1/3):
+//   q0 = RN(x z) is within 1.75 ulp of x/3, so r = x - 3 q0 is a multiple of
+//   ulp(q0) of magnitude <= 5.25 ulp(q0): the fma computes it exactly;
+//   q1 = RN(q0 + r z) = RN(x/3 + eta) with |eta| < 2^-52 ulp.
+// x/3 is never within ulp/6 of a midpoint between doubles (a midpoint has an
+// odd 54-bit significand, 3 times it cannot equal the 53-bit x), so q1 is
+// exactly the correctly rounded quotient, as IEEE division gives.  Valid for
+// zero and every x whose quotient is normal (the lattice values are O(1)).
+__device__ __forceinline__ double div3_rn(double x) {
+  const double z = 0x1.5555555555555p-2;
+  const double q0 = __dmul_rn(x, z);
+  const double r = __fma_rn(-q0, 3.0, x);
+  return __fma_rn(r, z, q0);
+}
+
 template <class R>
 __device__ __forceinline__ R wgt(int cls) {
   return cls == 0 ? R(8.0 / 27.0) : (cls == 1 ? R(2.0 / 27.0) : (cls == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0)));
@@ -91,7 +109,7 @@ __device__ __forceinline__ void moments(const R (&f)[Q], R& u, R& v, R& w, R& p)
     double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      pm = A::add(pm, __ddiv_rn(f[q], 3.0));
+      pm = A::add(pm, div3_rn(f[q]));
       if constexpr (D3Q27::ex[q] == 1) um = A::add(um, f[q]);
       if constexpr (D3Q27::ex[q] == -1) um = A::sub(um, f[q]);
       if constexpr (D3Q27::ey[q] == 1) vm = A::add(vm, f[q]);
@@ -207,20 +225,36 @@ __global__ void init_f_kernel(Layout L, typename StoreT<S>::T* b0, typename Stor
 }
 
 // ------------------------------------------------------------ step
-template <Store S, Bc B, CaseRule RULE, bool EXACT>
-__global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
-  using T = typename StoreT<S>::T;
-  using R = typename StoreT<S>::R;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= a.nx || j >= a.ny) return;
-  const T* __restrict__ src = static_cast<const T*>(a.src);
-  T* __restrict__ dst = static_cast<T*>(a.dst);
-  const int64_t b = a.base + k * a.sz + j * a.pitch + i;
-  const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+// The step is split into a load phase (pull the 27 populations of a cell,
+// applying the boundary rule of each link) and a compute phase (moments,
+// case rules, collision, stores).  A thread handles CPT cells stacked along
+// y and issues the loads of all of them before any arithmetic, so enough
+// bytes are in flight per thread for the narrow storage formats.  Every
+// boundary rule is expressed as a per-link choice of source address, never
+// as divergent control flow: a warp always issues its loads back to back.
 
-  R f[Q];
+// Cell flags for the standard boundaries: which walls the cell touches
+// (bit 0..5: x-, x+, y-, y+, z-, z+) -- the lid is z+.
+__device__ __forceinline__ unsigned wall_flags(const StepArgs& a, int i, int j, int k) {
+  return (i == 0 ? 1u : 0u) | (i == a.nx - 1 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == a.ny - 1 ? 8u : 0u) |
+         (k == 0 ? 16u : 0u) | (k == a.nz - 1 ? 32u : 0u);
+}
+// the link of population q leaves the box through a wall the cell touches
+template <int q>
+__device__ __forceinline__ bool leaves(unsigned w) {
+  constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+  constexpr unsigned m = (ex > 0 ? 1u : 0u) | (ex < 0 ? 2u : 0u) | (ey > 0 ? 4u : 0u) | (ey < 0 ? 8u : 0u) |
+                         (ez > 0 ? 16u : 0u) | (ez < 0 ? 32u : 0u);
+  return (w & m) != 0u;
+}
+
+template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG>
+__device__ __forceinline__ void load_cell(const StepArgs& a, const int i, const int j, const int k,
+                                          typename StoreT<S>::R (&f)[Q], double (&drag)[3]) {
+  using R = typename StoreT<S>::R;
+  using T = typename StoreT<S>::T;
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  const int64_t b = a.base + k * a.sz + j * a.pitch + i;
   if constexpr (B == Bc::Ghost) {
     // reference boundaries: the ghost slots the pull reaches were filled by
     // the ghost-slot gather after the previous step
@@ -235,81 +269,81 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
     const int64_t rz[3] = {km * a.sz, k * a.sz, kp * a.sz};
     const int64_t ry[3] = {jm * a.pitch, j * a.pitch, jp * a.pitch};
     const int64_t cx[3] = {im, i, ip};
-    const int64_t b0 = a.base;
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      const int64_t s =
-          b0 + q * a.sq + rz[1 - D3Q27::ez[q]] + ry[1 - D3Q27::ey[q]] + cx[1 - D3Q27::ex[q]];
+      const int64_t s = a.base + q * a.sq + rz[1 - D3Q27::ez[q]] + ry[1 - D3Q27::ey[q]] + cx[1 - D3Q27::ex[q]];
       f[q] = decode<S>(ldg_stream(src + s), q, a.enc);
     });
+  } else if constexpr (RULE == CaseRule::CavityStd) {
+    // halfway bounce-back on the six walls: a link leaving the box returns
+    // the cell's own opposite population; through the lid (z+) it gains
+    // -2 w rho_w (c_bb . u_w)/cs^2 = 6 w rho_w e_q.u_w
+    const unsigned wf = wall_flags(a, i, j, k);
+    const bool lid = (wf & 32u) != 0u;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q];
+      constexpr int exq = D3Q27::ex[q];
+      constexpr int cls = D3Q27::wclass[q];
+      const bool out = leaves<q>(wf);
+      const int64_t o = out ? static_cast<int64_t>(qb) * a.sq : a.off[q];
+      R val = decode<S>(ldg_stream(src + b + o), out ? qb : q, a.enc);
+      if constexpr (exq != 0 && D3Q27::ez[q] < 0) {
+        // ((6 rho_w u_w) w_q) e_q rounded on its own, then added (EXACT keeps
+        // the multiply and the add apart, as the specification does)
+        using A = Ar<R, EXACT>;
+        if (lid) val = A::add(val, A::mul(A::mul(R(6.0 * a.rho_w * a.lid_u), wgt<R>(cls)), R(exq)));
+      }
+      f[q] = val;
+    });
   } else {
-    static_assert(B == Bc::Standard, "boundary kind");
-    if constexpr (RULE == CaseRule::CavityStd) {
-      // halfway bounce-back on all six walls; the lid (z >= nz) moves
-      const bool edge = i == 0 || i == a.nx - 1 || j == 0 || j == a.ny - 1 || k == 0 || k == a.nz - 1;
-      if (!edge) {
-        static_for<0, Q>([&](auto qc) {
-          constexpr int q = decltype(qc)::value;
-          f[q] = decode<S>(ldg_stream(src + b + a.off[q]), q, a.enc);
-        });
-      } else {
-        static_for<0, Q>([&](auto qc) {
-          constexpr int q = decltype(qc)::value;
-          constexpr int qb = D3Q27::bb[q];
-          constexpr int exq = D3Q27::ex[q], eyq = D3Q27::ey[q], ezq = D3Q27::ez[q];
-          constexpr int cls = D3Q27::wclass[q];
-          const int si = i - exq, sj = j - eyq, sk = k - ezq;
-          const bool inside = si >= 0 && si < a.nx && sj >= 0 && sj < a.ny && sk >= 0 && sk < a.nz;
-          if (inside) {
-            f[q] = decode<S>(ldg_stream(src + b + a.off[q]), q, a.enc);
-          } else {
-            // f_q(x) = f*_bb(q)(x) - 2 w rho_w (c_bb(q) . u_w) / cs^2 with c_bb(q) = -e_q
-            R val = decode<S>(ldg_stream(src + b + qb * a.sq), qb, a.enc);
-            if constexpr (exq != 0) {
-              if (sk >= a.nz) val += R(6.0 * a.rho_w * a.lid_u) * wgt<R>(cls) * R(exq);
-            }
-            f[q] = val;
-          }
-        });
+    static_assert(RULE == CaseRule::SphereStd, "standard rule");
+    // channel periodic in y and z; x-: equilibrium inlet; x+: zero-gradient
+    // outlet (the link re-enters from the cell's own column); solid links
+    // (bit q of the cell's link mask) bounce back
+    const int jm = j == 0 ? a.ny - 1 : j - 1, jp = j == a.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1, kp = k == a.nz - 1 ? 0 : k + 1;
+    const int64_t rz[3] = {km * a.sz, k * a.sz, kp * a.sz};
+    const int64_t ry[3] = {jm * a.pitch, j * a.pitch, jp * a.pitch};
+    const bool inlet = i == 0, outlet = i == a.nx - 1;
+    const int64_t cx[3] = {i - 1, i, outlet ? i : i + 1};
+    const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+    const bool near = k >= a.near_lo[2] && k <= a.near_hi[2] && j >= a.near_lo[1] && j <= a.near_hi[1] &&
+                      i >= a.near_lo[0] && i <= a.near_hi[0];
+    const uint32_t links = near ? a.links[cell] : 0u;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q];
+      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+      [[maybe_unused]] constexpr int cls = D3Q27::wclass[q];
+      const bool solid = (links >> q) & 1u;
+      const int64_t s_pull = a.base + q * a.sq + rz[1 - ez] + ry[1 - ey] + cx[1 - ex];
+      const int64_t s_bb = b + static_cast<int64_t>(qb) * a.sq;
+      R val = decode<S>(ldg_stream(src + (solid ? s_bb : s_pull)), solid ? qb : q, a.enc);
+      if constexpr (ex > 0) {
+        if (inlet) val = R(a.feq_in[q]);
       }
-    } else {
-      static_assert(RULE == CaseRule::SphereStd, "standard rule");
-      // channel: periodic in y and z, equilibrium inlet at x < 0,
-      // zero-gradient outlet at x >= nx, halfway bounce-back on solid cells
-      if (!a.usr[cell]) {
-        if (a.store) {
-          a.mu[cell] = 0;
-          a.mv[cell] = 0;
-          a.mw[cell] = 0;
-          a.mp[cell] = a.p_shift;
+      if constexpr (DRAG) {
+        if (solid) {
+          const double fd = static_cast<double>(val) + (S == Store::F64 ? 0.0 : 3.0 * wgt<double>(cls) * a.p_shift);
+          if constexpr (ex != 0) drag[0] -= 2.0 * fd * ex;
+          if constexpr (ey != 0) drag[1] -= 2.0 * fd * ey;
+          if constexpr (ez != 0) drag[2] -= 2.0 * fd * ez;
         }
-        return;
       }
-      const int jm = j == 0 ? a.ny - 1 : j - 1, jp = j == a.ny - 1 ? 0 : j + 1;
-      const int km = k == 0 ? a.nz - 1 : k - 1, kp = k == a.nz - 1 ? 0 : k + 1;
-      const int jj[3] = {jm, j, jp}, kk[3] = {km, k, kp};
-      const int64_t nxy = static_cast<int64_t>(a.nx) * a.ny;
-      static_for<0, Q>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
-        constexpr int qb = D3Q27::bb[q];
-        const int si = i - ex;
-        const int sj = jj[1 - ey], sk = kk[1 - ez];
-        if (si < 0) {
-          f[q] = R(a.feq_in[q]);
-        } else {
-          const int sx = si >= a.nx ? a.nx - 1 : si;
-          const int64_t scell = sx + a.nx * static_cast<int64_t>(sj) + nxy * sk;
-          if (!a.usr[scell]) {
-            f[q] = decode<S>(ldg_stream(src + b + qb * a.sq), qb, a.enc);
-          } else {
-            const int64_t s = a.base + q * a.sq + sk * a.sz + sj * a.pitch + sx;
-            f[q] = decode<S>(ldg_stream(src + s), q, a.enc);
-          }
-        }
-      });
-    }
+      f[q] = val;
+    });
   }
+}
+
+template <Store S, CaseRule RULE, bool EXACT>
+__device__ __forceinline__ void compute_cell(const StepArgs& a, const int i, const int j, const int k,
+                                             typename StoreT<S>::R (&f)[Q]) {
+  using T = typename StoreT<S>::T;
+  using R = typename StoreT<S>::R;
+  T* __restrict__ dst = static_cast<T*>(a.dst);
+  const int64_t b = a.base + k * a.sz + j * a.pitch + i;
+  const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
 
   R u, v, w, p;
   moments<R, EXACT>(f, u, v, w, p);
@@ -355,6 +389,87 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
     }
     dst[b + q * a.sq] = encode<S>(fs, q, a.enc);
   });
+}
+
+template <Store S> struct CellsPerThread { static constexpr int value = 1; };
+template <> struct CellsPerThread<Store::F32> { static constexpr int value = 2; };
+template <> struct CellsPerThread<Store::F16> { static constexpr int value = 2; };
+template <> struct CellsPerThread<Store::BF16> { static constexpr int value = 2; };
+
+template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG>
+__global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
+  using R = typename StoreT<S>::R;
+  constexpr int CPT = CellsPerThread<S>::value;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * CPT;
+  const int k = blockIdx.z;
+  double drag[3] = {0.0, 0.0, 0.0};
+  R f[CPT][Q];
+  bool act[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int j = j0 + c;
+    act[c] = i < a.nx && j < a.ny;
+    if constexpr (RULE == CaseRule::SphereStd) {
+      // solid cells are not updated; they report zero moments
+      if (act[c]) {
+        const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+        if (!a.usr[cell]) {
+          if (a.store) {
+            a.mu[cell] = 0;
+            a.mv[cell] = 0;
+            a.mw[cell] = 0;
+            a.mp[cell] = a.p_shift;
+          }
+          act[c] = false;
+        }
+      }
+    }
+    if (act[c]) load_cell<S, B, RULE, EXACT, DRAG>(a, i, j, k, f[c], drag);
+  }
+#pragma unroll
+  for (int c = 0; c < CPT; ++c)
+    if (act[c]) compute_cell<S, RULE, EXACT>(a, i, j0 + c, k, f[c]);
+
+  if constexpr (DRAG) {
+    // every thread reaches the block reduction; the per-block partial sums
+    // are added in a fixed order afterwards, so the force is deterministic
+    __shared__ double sh[3][8];
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double x = drag[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[c][warp] = x;
+    }
+    __syncthreads();
+    if (t < 3) {
+      const int nw = (blockDim.x * blockDim.y + 31) / 32;
+      double x = 0.0;
+      for (int w = 0; w < nw; ++w) x += sh[t][w];
+      const int64_t blk = blockIdx.x + static_cast<int64_t>(gridDim.x) * (blockIdx.y + static_cast<int64_t>(gridDim.y) * blockIdx.z);
+      a.drag_part[3 * blk + t] = x;
+    }
+  }
+}
+
+// Sum the per-block drag partials (3 components, fixed order).
+__global__ void drag_sum_kernel(const double* part, int64_t nblk, double* out) {
+  const int c = blockIdx.x;  // component
+  double acc = 0.0;
+  for (int64_t b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[3 * b + c];
+  __shared__ double sh[RED_THREADS_DRAG / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0;
+    for (int w = 0; w < RED_THREADS_DRAG / 32; ++w) x += sh[w];
+    out[c] = x;
+  }
 }
 
 // ------------------------------------------------------------ ghost slots
@@ -440,16 +555,28 @@ __global__ void reduce_pass2(RedKind kind, const double* part, int nparts, doubl
   }
 }
 
+}  // namespace
+
 dim3 step_block(int nx) {
   if (nx >= 128) return dim3(128, 2, 1);
   if (nx >= 64) return dim3(64, 4, 1);
   return dim3(32, 8, 1);
 }
 
-}  // namespace
-
 // ------------------------------------------------------------ launchers
 int reduce_blocks() { return RED_BLOCKS; }
+
+int64_t step_grid_blocks(int nx, int ny, int nz, int storage) {
+  const dim3 b = step_block(nx);
+  const int cpt = storage == static_cast<int>(Store::F64) ? 1 : CellsPerThread<Store::F16>::value;
+  const int rows = b.y * cpt;
+  return static_cast<int64_t>((nx + b.x - 1) / b.x) * ((ny + rows - 1) / rows) * nz;
+}
+
+cudaError_t launch_drag_sum(const double* part, int64_t nblk, double* out, cudaStream_t s) {
+  drag_sum_kernel<<<3, RED_THREADS_DRAG, 0, s>>>(part, nblk, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_reduce(RedKind k, const double* u, const double* v, const double* w, const double* p,
                           const double* u2, const double* v2, const double* w2, int64_t n, double* scratch,
@@ -488,8 +615,15 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
   const dim3 block = step_block(a.nx);
-  const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + block.y - 1) / block.y, a.nz);
-  step_kernel<S, B, R, EXACT><<<grid, block, 0, s>>>(a);
+  const int rows = block.y * CellsPerThread<S>::value;
+  const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);
+  if constexpr (R == CaseRule::SphereStd) {
+    if (a.drag_part) {
+      step_kernel<S, B, R, EXACT, true><<<grid, block, 0, s>>>(a);
+      return cudaGetLastError();
+    }
+  }
+  step_kernel<S, B, R, EXACT, false><<<grid, block, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -101,10 +101,13 @@ struct imexlb_lattice {
   DevArray<double> prev_mom;  // u, v, w of the last residual call
   bool have_prev = false;
   DevArray<uint8_t> usr;      // interior mask (sphere)
+  DevArray<uint32_t> links;   // standard sphere: per-cell solid-link bits
   DevArray<double> inlet;     // reference sphere inlet profile per z
   DevArray<int64_t> gtgt, gsrc;
   int64_t gn = 0;
   DevArray<double> red;       // reduction partials + result
+  DevArray<double> drag_part; // standard sphere: per-block drag partials of the last step
+  int64_t drag_blocks = 0;
   cudaStream_t stream = nullptr;
   int64_t steps = 0;
   std::vector<int32_t> usr_padded;  // host copy, padded box (reference sphere)
@@ -407,6 +410,41 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       IMX_CUDA(cudaMemcpy(h->inlet.p, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
       a.inlet = h->inlet.p;
     } else {
+      // per-cell bit q: the cell's pull along -e_q starts in a solid cell
+      // (y and z periodic; the x ends are handled by the inlet/outlet rules)
+      std::vector<uint32_t> links(static_cast<size_t>(h->ncell), 0u);
+      int lo[3] = {P.nx, P.ny, P.nz}, hi[3] = {-1, -1, -1};
+      for (int k = 0; k < P.nz; ++k)
+        for (int j = 0; j < P.ny; ++j)
+          for (int i = 0; i < P.nx; ++i) {
+            const size_t c = i + static_cast<size_t>(P.nx) * (j + static_cast<size_t>(P.ny) * k);
+            if (!m[c]) continue;
+            uint32_t bits = 0;
+            for (int q = 0; q < Q; ++q) {
+              const int si = i - D3Q27::ex[q];
+              if (si < 0 || si >= P.nx) continue;
+              const int sj = (j - D3Q27::ey[q] + P.ny) % P.ny, sk = (k - D3Q27::ez[q] + P.nz) % P.nz;
+              if (!m[si + static_cast<size_t>(P.nx) * (sj + static_cast<size_t>(P.ny) * sk)]) bits |= 1u << q;
+            }
+            links[c] = bits;
+            if (bits) {
+              const int x[3] = {i, j, k};
+              for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], x[d]);
+                hi[d] = std::max(hi[d], x[d]);
+              }
+            }
+          }
+      IMX_CUDA(h->links.alloc(links.size()));
+      IMX_CUDA(cudaMemcpy(h->links.p, links.data(), links.size() * 4, cudaMemcpyHostToDevice));
+      a.links = h->links.p;
+      for (int d = 0; d < 3; ++d) {
+        a.near_lo[d] = lo[d];
+        a.near_hi[d] = hi[d];
+      }
+      h->drag_blocks = step_grid_blocks(P.nx, P.ny, P.nz, static_cast<int>(P.storage));
+      IMX_CUDA(h->drag_part.alloc(3 * static_cast<size_t>(h->drag_blocks)));
+      IMX_CUDA(cudaMemset(h->drag_part.p, 0, h->drag_part.n * sizeof(double)));
       // equilibrium populations of the inlet (deviation form)
       const double ui = P.inlet_u;
       for (int q = 0; q < Q; ++q) {
@@ -465,6 +503,7 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
     a.src = h->buf[h->cur].p;
     a.dst = h->buf[1 - h->cur].p;
     a.store = s == nsteps - 1;
+    a.drag_part = (a.store && h->drag_part.p) ? h->drag_part.p : nullptr;
     imexlb_lattice::Timed t0{nullptr, nullptr, 0}, t1{nullptr, nullptr, 1};
     if (h->profiling) {
       t0.a = h->take_event();
@@ -638,6 +677,15 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
         return fail(IMEXLB_E_STATE, "lattice is not finite (NaN/Inf in the velocity field)");
       return IMEXLB_OK;
     }
+    case IMEXLB_REDUCE_DRAG: {
+      if (!h->drag_part.p) return fail(IMEXLB_E_UNSUPPORTED, "drag needs the standard sphere channel");
+      IMX_CUDA(launch_drag_sum(h->drag_part.p, h->drag_blocks, res, h->stream));
+      IMX_CUDA(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      IMX_CUDA(cudaStreamSynchronize(h->stream));
+      if (!std::isfinite(out[0]) || !std::isfinite(out[1]) || !std::isfinite(out[2]))
+        return fail(IMEXLB_E_STATE, "drag is not finite");
+      return IMEXLB_OK;
+    }
     default:
       return fail(IMEXLB_E_ARG, "unknown or unsupported reduction");
   }
@@ -657,7 +705,7 @@ int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* byte
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
   if (device_bytes)
     *device_bytes = h->buf[0].n + h->buf[1].n + h->mom.n * 8 + h->prev_mom.n * 8 + h->usr.n + h->inlet.n * 8 +
-                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->red.n * 8;
+                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->red.n * 8 + h->drag_part.n * 8 + h->links.n * 4;
   if (bytes_per_cell_update) *bytes_per_cell_update = 2.0 * Q * h->L.elem;
   return IMEXLB_OK;
 }

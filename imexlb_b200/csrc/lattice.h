@@ -71,6 +71,10 @@ struct StepArgs {
   double inlet_u = 0;     // standard sphere inlet velocity
   double feq_in[Q] = {};  // standard sphere: inlet equilibrium (deviation form)
   double p_shift = 0;     // rest pressure removed from stored values (0 for FP64)
+  double* drag_part = nullptr;  // standard sphere: per-block momentum-exchange partials (3 per block), or null
+  const uint32_t* links = nullptr;  // standard sphere: per-cell bit q = the link along -e_q ends in the solid
+  int near_lo[3] = {0, 0, 0};       // box of cells that have solid links
+  int near_hi[3] = {-1, -1, -1};
   Encoding enc;
 };
 
@@ -104,6 +108,9 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
 cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s);
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
                                 int64_t n, int64_t sq, const Encoding& enc, cudaStream_t s);
+dim3 step_block(int nx);
+int64_t step_grid_blocks(int nx, int ny, int nz, int storage);
+cudaError_t launch_drag_sum(const double* part, int64_t nblk, double* out, cudaStream_t s);
 // Deterministic FP64 sums over n values: out[c] = sum of comp(c) over cells
 // for the requested quantity; partial sums of `blocks` blocks go to scratch.
 enum class RedKind : int { Mass = 0, Kinetic = 1, DiffSq = 2, NormSq = 3, UMax = 4 };

@@ -66,6 +66,16 @@ def oracle_lib():
         lib.oracle_write_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         lib.oracle_write_tecplot.restype = ctypes.c_int
         lib.oracle_threads.restype = ctypes.c_int
+        lib.oracle_check_div3.argtypes = [ctypes.c_long, ctypes.c_ulonglong, ctypes.c_int]
+        lib.oracle_check_div3.restype = ctypes.c_int
+        lib.oracle_std_create.restype = ctypes.c_void_p
+        lib.oracle_std_create.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 9
+        lib.oracle_std_destroy.argtypes = [ctypes.c_void_p]
+        lib.oracle_std_destroy.restype = None
+        lib.oracle_std_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.oracle_std_step.restype = None
+        lib.oracle_std_get_moments.argtypes = [ctypes.c_void_p] * 5
+        lib.oracle_std_drag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         _ORACLE_LIB = lib
     return _ORACLE_LIB
 
@@ -123,6 +133,41 @@ class Oracle:
         rc = self.lib.oracle_write_tecplot(self.h, path.encode(), n)
         if rc:
             raise OSError(f"oracle_write_tecplot failed for {path}")
+
+
+class OracleStd:
+    """The standard-boundary specification (moving-lid cavity, sphere channel)."""
+
+    def __init__(self, case: str, nx: int, ny: int, nz: int, tau0: float, rho0: float = 1.0, u0: float = 0.1,
+                 lid_u: float = 0.0, inlet_u: float = 0.0, sphere_d: float = 0.0, sphere_c=(0.0, 0.0, 0.0)):
+        self.lib = oracle_lib()
+        self.n = (nx, ny, nz)
+        self.h = self.lib.oracle_std_create(CASES[case], nx, ny, nz, tau0, rho0, u0, lid_u, inlet_u, sphere_d,
+                                            *sphere_c)
+        if not self.h:
+            raise ValueError("oracle_std_create failed")
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_std_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def step(self, n: int = 1):
+        self.lib.oracle_std_step(self.h, n)
+
+    def moments(self):
+        nx, ny, nz = self.n
+        out = [np.empty(nx * ny * nz) for _ in range(4)]
+        self.lib.oracle_std_get_moments(self.h, *[_ptr(a) for a in out])
+        return [a.reshape(nz, ny, nx) for a in out]
+
+    def drag(self):
+        f = [ctypes.c_double() for _ in range(3)]
+        self.lib.oracle_std_drag(self.h, *[ctypes.byref(x) for x in f])
+        return tuple(x.value for x in f)
 
 
 def oracle_system(case: str, rho0, R, Re, u0, time_in, inter_in, sx):

@@ -585,3 +585,218 @@ int oracle_write_tecplot(const oracle_lbm* o, const char* path, int n) {
   for (int a = 0; a < 4; ++a) free(fld[a]);
   return fclose(fp) == 0 ? 0 : 1;
 }
+
+/* ======================================================================
+ * Standard-boundary variants (see imexlb_oracle.h).  Interior-only storage,
+ * two buffers, the fused order pull -> moments -> collide, FP64 with the
+ * reference's expression order (the device's EXACT arithmetic).
+ * ====================================================================== */
+struct oracle_std {
+  int kase, nx, ny, nz;
+  double tau0, rho0, u0, lid_u, inlet_u;
+  double *A, *B; /* post-collision distributions, index q + Q*cell */
+  double *u, *v, *w, *p;
+  unsigned char* fluid;
+  double feq_in[Q];
+  double drag[3];
+};
+
+static inline size_t SC(const oracle_std* o, int i, int j, int k) {
+  return (size_t)i + (size_t)o->nx * ((size_t)j + (size_t)o->ny * (size_t)k);
+}
+
+/* the device's e.u with zero terms dropped (same value as the reference's
+ * (e0*u + e1*v) + e2*w) */
+static double std_edu(int q, double u, double v, double w) {
+  const int a = E_REF[q][0], b = E_REF[q][1], c = E_REF[q][2];
+  double t = 0.0;
+  int have = 0;
+  if (a) { t = a > 0 ? u : -u; have = 1; }
+  if (b) { t = have ? (b > 0 ? t + v : t - v) : (b > 0 ? v : -v); have = 1; }
+  if (c) { t = have ? (c > 0 ? t + w : t - w) : (c > 0 ? w : -w); }
+  return t;
+}
+
+static void std_collide(const oracle_std* o, const double* f, double u, double v, double w, double p, double* out) {
+  const double udu15 = 1.5 * ((u * u + v * v) + w * w);
+  for (int q = 0; q < Q; ++q) {
+    const double t = W_REF[q];
+    const double e = std_edu(q, u, v, w);
+    const double feq = (t * p) * 3.0 + t * (((3.0 * e) + (4.5 * (e * e))) - udu15);
+    out[q] = f[q] - ((f[q] - feq) / (o->tau0 + 0.5));
+  }
+}
+
+oracle_std* oracle_std_create(int kase, int nx, int ny, int nz, double tau0, double rho0, double u0,
+                              double lid_u, double inlet_u, double sphere_d, double cx, double cy, double cz) {
+  if ((kase != ORACLE_CAVITY && kase != ORACLE_SPHERE) || nx < 2 || ny < 2 || nz < 2) return NULL;
+  oracle_std* o = (oracle_std*)calloc(1, sizeof(oracle_std));
+  o->kase = kase;
+  o->nx = nx;
+  o->ny = ny;
+  o->nz = nz;
+  o->tau0 = tau0;
+  o->rho0 = rho0;
+  o->u0 = u0;
+  o->lid_u = lid_u;
+  o->inlet_u = inlet_u;
+  const size_t n = (size_t)nx * ny * nz;
+  o->A = (double*)calloc(n * Q, sizeof(double));
+  o->B = (double*)calloc(n * Q, sizeof(double));
+  o->u = (double*)calloc(n, sizeof(double));
+  o->v = (double*)calloc(n, sizeof(double));
+  o->w = (double*)calloc(n, sizeof(double));
+  o->p = (double*)calloc(n, sizeof(double));
+  o->fluid = (unsigned char*)malloc(n);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t c = SC(o, i, j, k);
+        int solid = 0;
+        if (kase == ORACLE_SPHERE) {
+          const double dx = i - cx, dy = j - cy, dz = k - cz;
+          solid = dx * dx + dy * dy + dz * dz <= 0.25 * sphere_d * sphere_d;
+        }
+        o->fluid[c] = (unsigned char)!solid;
+        o->u[c] = (kase == ORACLE_SPHERE && !solid) ? inlet_u : 0.0;
+      }
+  for (int q = 0; q < Q; ++q) {
+    const double t = W_REF[q];
+    const double e = E_REF[q][0] * inlet_u;
+    o->feq_in[q] = t * (3.0 * (0.0 - 0.0) + 3.0 * e + 4.5 * e * e - 1.5 * inlet_u * inlet_u);
+  }
+  /* f = feq of the initial fields; the first collision leaves it unchanged */
+  for (size_t c = 0; c < n; ++c) {
+    const double uu = o->u[c], vv = o->v[c], ww = o->w[c], pp = o->p[c];
+    const double udu15 = 1.5 * ((uu * uu + vv * vv) + ww * ww);
+    for (int q = 0; q < Q; ++q) {
+      const double t = W_REF[q];
+      const double e = std_edu(q, uu, vv, ww);
+      o->A[q + Q * c] = (t * pp) * 3.0 + t * (((3.0 * e) + (4.5 * (e * e))) - udu15);
+    }
+  }
+  return o;
+}
+
+void oracle_std_destroy(oracle_std* o) {
+  if (!o) return;
+  free(o->A);
+  free(o->B);
+  free(o->u);
+  free(o->v);
+  free(o->w);
+  free(o->p);
+  free(o->fluid);
+  free(o);
+}
+
+void oracle_std_step(oracle_std* o, int nsteps) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int s = 0; s < nsteps; ++s) {
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : fx, fy, fz)
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const size_t c = SC(o, i, j, k);
+          double f[Q];
+          if (o->kase == ORACLE_SPHERE && !o->fluid[c]) {
+            o->u[c] = o->v[c] = o->w[c] = o->p[c] = 0.0;
+            continue;
+          }
+          for (int q = 0; q < Q; ++q) {
+            const int ex = E_REF[q][0], ey = E_REF[q][1], ez = E_REF[q][2];
+            int si = i - ex, sj = j - ey, sk = k - ez;
+            if (o->kase == ORACLE_CAVITY) {
+              if (si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz) {
+                f[q] = o->A[q + Q * SC(o, si, sj, sk)];
+              } else {
+                double val = o->A[BB_REF[q] + Q * c];
+                if (ex != 0 && sk >= nz) val += ((6.0 * o->rho0) * o->lid_u) * W_REF[q] * (double)ex;
+                f[q] = val;
+              }
+            } else {
+              sj = (sj + ny) % ny;
+              sk = (sk + nz) % nz;
+              if (si < 0) {
+                f[q] = o->feq_in[q];
+              } else {
+                if (si >= nx) si = nx - 1;
+                const size_t sc = SC(o, si, sj, sk);
+                if (!o->fluid[sc]) {
+                  f[q] = o->A[BB_REF[q] + Q * c];
+                  fx += -2.0 * f[q] * ex;
+                  fy += -2.0 * f[q] * ey;
+                  fz += -2.0 * f[q] * ez;
+                } else {
+                  f[q] = o->A[q + Q * sc];
+                }
+              }
+            }
+          }
+          double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
+          for (int q = 0; q < Q; ++q) {
+            pm = pm + f[q] / 3.0;
+            if (E_REF[q][0]) um = E_REF[q][0] > 0 ? um + f[q] : um - f[q];
+            if (E_REF[q][1]) vm = E_REF[q][1] > 0 ? vm + f[q] : vm - f[q];
+            if (E_REF[q][2]) wm = E_REF[q][2] > 0 ? wm + f[q] : wm - f[q];
+          }
+          o->u[c] = um;
+          o->v[c] = vm;
+          o->w[c] = wm;
+          o->p[c] = pm;
+          std_collide(o, f, um, vm, wm, pm, &o->B[Q * c]);
+        }
+    double* t = o->A;
+    o->A = o->B;
+    o->B = t;
+    o->drag[0] = fx;
+    o->drag[1] = fy;
+    o->drag[2] = fz;
+  }
+}
+
+void oracle_std_get_moments(const oracle_std* o, double* u, double* v, double* w, double* p) {
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
+  if (u) memcpy(u, o->u, n * sizeof(double));
+  if (v) memcpy(v, o->v, n * sizeof(double));
+  if (w) memcpy(w, o->w, n * sizeof(double));
+  if (p) memcpy(p, o->p, n * sizeof(double));
+}
+
+void oracle_std_drag(const oracle_std* o, double* fx, double* fy, double* fz) {
+  *fx = o->drag[0];
+  *fy = o->drag[1];
+  *fz = o->drag[2];
+}
+
+/* Check of the three-operation correctly rounded division by 3 the device's
+ * EXACT mode uses for the moments: returns how many of n random doubles
+ * (random signs, exponents in [-200, 200] around 1, random significands)
+ * give a quotient different from IEEE division.  planted = 1 drops the
+ * correction step (q0 = x * RN(1/3) alone), a known-wrong variant that shows
+ * the check can fail. */
+int oracle_check_div3(long n, unsigned long long seed, int planted) {
+  const double z = 0x1.5555555555555p-2;
+  int bad = 0;
+  unsigned long long s = seed ? seed : 88172645463325252ULL;
+  for (long t = 0; t < n; ++t) {
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    const unsigned long long mant = s & 0xFFFFFFFFFFFFFULL;
+    const long e = (long)((s >> 52) % 401) - 200;
+    const unsigned long long sign = (s >> 63) << 63;
+    union {
+      unsigned long long u;
+      double d;
+    } v;
+    v.u = sign | ((unsigned long long)(1023 + e) << 52) | mant;
+    const double x = v.d;
+    const double q0 = x * z;
+    const double r = fma(-q0, 3.0, x);
+    const double q1 = planted ? q0 : fma(r, z, q0);
+    if (q1 != x / 3.0) ++bad;
+  }
+  return bad;
+}

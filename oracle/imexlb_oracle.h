@@ -56,8 +56,38 @@ void oracle_system(int kase, double rho0, double R, int Re, double u0, int time_
 /* Tecplot binary writer of LBM::MPIoutput at one rank (tgv/src/lbm.cpp:335-669) */
 int oracle_write_tecplot(const oracle_lbm* o, const char* path, int n);
 
+/* Mismatches of the device's three-operation x/3 against IEEE division over n
+ * random doubles (test of the EXACT-mode moment arithmetic). */
+int oracle_check_div3(long n, unsigned long long seed, int planted);
+
 /* Number of OpenMP threads the oracle will use (for the CPU baseline). */
 int oracle_threads(void);
+
+/* ------------------------------------------------------------------------
+ * Standard-boundary variants (the BASELINE configurations; no reference
+ * code exists for them, so this is the specification the device path is
+ * checked against):
+ *   ORACLE_CAVITY: fluid box [0,n)^3, halfway bounce-back on all six walls,
+ *     the lid (z >= nz) moving along +x at lid_u:
+ *       f_q(x) = f*_bb(q)(x) + 6 w_q rho0 (e_q . u_w)   when x - e_q is a wall
+ *   ORACLE_SPHERE: channel periodic in y and z, equilibrium inlet
+ *     feq(p = 0, u = (inlet_u, 0, 0)) for populations entering at x = 0,
+ *     zero-gradient outlet (a population entering at x = nx-1 is pulled
+ *     from x = nx-1 instead of x = nx), halfway bounce-back on the voxelised
+ *     sphere |x - c|^2 <= d^2/4; solid cells are not updated and report
+ *     zero moments.  Drag = sum over links of -2 f_q(x) e_q.
+ * Both use the reference's p-based equilibrium and collision, FP64, with
+ * the same operation order as the device's EXACT mode.
+ * ------------------------------------------------------------------------ */
+typedef struct oracle_std oracle_std;
+oracle_std* oracle_std_create(int kase, int nx, int ny, int nz, double tau0, double rho0, double u0,
+                              double lid_u, double inlet_u, double sphere_d, double cx, double cy, double cz);
+void oracle_std_destroy(oracle_std* o);
+void oracle_std_step(oracle_std* o, int nsteps);
+void oracle_std_get_moments(const oracle_std* o, double* u, double* v, double* w, double* p);
+/* momentum-exchange force of the last step (sphere channel) */
+void oracle_std_drag(const oracle_std* o, double* fx, double* fy, double* fz);
+
 
 #ifdef __cplusplus
 }

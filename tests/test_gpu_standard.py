@@ -1,0 +1,100 @@
+"""GPU checks of the standard-boundary variants and reduced-precision storage.
+
+* Standard boundaries (moving-lid cavity, sphere channel) against the C
+  specification in oracle/imexlb_oracle.c (oracle_std_*): EXACT arithmetic
+  bit-identical moments; FAST within 1e-12 of the largest value; the
+  momentum-exchange drag within 1e-10 relative (the CPU sums in another order).
+* Reduced-precision storage against this library's own FP64 run of the same
+  case: relative velocity L2 error
+      ||u - u64||_2 / ||u64||_2   (all three components)
+  under the bound written in each case.
+"""
+import numpy as np
+import pytest
+
+from oracle.bindings import OracleStd
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    from imexlb_b200 import api as a
+
+    return a
+
+
+def rel_l2(a, b):
+    num = sum(np.sum((a[k] - b[k]) ** 2) for k in "uvw")
+    den = sum(np.sum(b[k] ** 2) for k in "uvw")
+    return float(np.sqrt(num / den))
+
+
+STD = [
+    ("cavity", (16, 16, 16), 0.0384, dict(lid_u=0.1), 120),
+    ("cavity", (20, 14, 18), 0.03, dict(lid_u=0.08), 75),
+    ("sphere", (48, 16, 16), 0.015, dict(inlet_u=0.05, sphere_d=6.0, sphere_c=(12.0, 8.0, 8.0)), 90),
+    ("sphere", (40, 12, 14), 0.02, dict(inlet_u=0.04, sphere_d=5.0, sphere_c=(10.0, 6.0, 7.0)), 33),
+]
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("case,n,tau,kw,steps", STD)
+def test_standard_boundaries_match_spec(api, case, n, tau, kw, steps, arith):
+    o = OracleStd(case, *n, tau, 1.0, 0.1, **kw)
+    o.step(steps)
+    want = dict(zip("uvwp", o.moments()))
+    with api.LBM(case, *n, tau, 1.0, 0.1, bc="standard", arith=arith, **kw) as lbm:
+        lbm.step(steps)
+        got = lbm.fields()
+        drag = lbm.reduce("drag") if case == "sphere" else None
+    for k in "uvwp":
+        if arith == "exact":
+            assert np.array_equal(got[k], want[k]), f"{k}: max |diff| {np.abs(got[k] - want[k]).max()}"
+        else:
+            scale = max(np.abs(want[k]).max(), 1e-30)
+            assert np.abs(got[k] - want[k]).max() <= 1e-12 * scale, k
+    if drag is not None:
+        wd = o.drag()
+        assert abs(drag[0] - wd[0]) <= 1e-10 * abs(wd[0]), (drag, wd)
+        for c in (1, 2):
+            assert abs(drag[c] - wd[c]) <= 1e-10 * abs(wd[0])
+
+
+def test_cavity_lid_drives_flow(api):
+    with api.LBM("cavity", 32, 32, 32, 0.0384, 1.0, 0.1, bc="standard", lid_u=0.1) as lbm:
+        lbm.step(400)
+        f = lbm.fields()
+    top = f["u"][-1].mean()
+    assert 0.02 < top < 0.1  # the top plane follows the lid
+    assert f["u"][: 16].mean() < 0.0  # the return flow in the lower half
+
+
+# (case, storage, n, steps, bound on the relative velocity L2 error vs FP64)
+PRECISION = [
+    ("tgv", "f32", (32, 32, 32), 200, 1e-5),
+    ("tgv", "f16", (32, 32, 32), 200, 1e-3),
+    ("tgv", "bf16", (32, 32, 32), 200, 3e-2),
+    ("cavity", "f32", (32, 32, 32), 300, 1e-5),
+    ("cavity", "f16", (32, 32, 32), 300, 1e-3),
+    ("cavity", "bf16", (32, 32, 32), 300, 3e-2),
+]
+
+
+@pytest.mark.parametrize("case,storage,n,steps,bound", PRECISION)
+def test_reduced_precision_error(api, case, storage, n, steps, bound):
+    tau = 0.02
+    bc = "standard" if case == "cavity" else "reference"
+    kw = dict(lid_u=0.1) if case == "cavity" else {}
+    with api.LBM(case, *n, tau, 1.0, 0.1 if case == "cavity" else 0.05, bc=bc, arith="fast", **kw) as ref:
+        ref.step(steps)
+        want = ref.fields()
+    with api.LBM(case, *n, tau, 1.0, 0.1 if case == "cavity" else 0.05, bc=bc, storage=storage, **kw) as lbm:
+        lbm.step(steps)
+        got = lbm.fields()
+    err = rel_l2(got, want)
+    assert err <= bound, f"{storage} {case}: relative velocity L2 error {err:.3e} > {bound:.1e}"
