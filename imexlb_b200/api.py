@@ -64,7 +64,8 @@ class ParamsStruct(ctypes.Structure):
 
 # Every symbol include/imexlb.h declares (tests check the library exports them).
 EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imexlb_initialize", "imexlb_step",
-           "imexlb_get_fields", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce", "imexlb_steps_taken",
+           "imexlb_get_fields", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
+           "imexlb_reduce_fields_noalloc", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
            "imexlb_version"]
 
@@ -90,6 +91,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_get_mask.argtypes = [vp, vp]
     lib.imexlb_write_tecplot.argtypes = [vp, ctypes.c_char_p, i]
     lib.imexlb_reduce.argtypes = [vp, i, ctypes.POINTER(d)]
+    lib.imexlb_reduce_fields_noalloc.argtypes = [i, vp, vp, vp, vp, ctypes.c_int64, vp, vp]
     lib.imexlb_steps_taken.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.imexlb_footprint.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(d)]
     lib.imexlb_ghost_plan.argtypes = [i, i, i, i, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]

@@ -71,6 +71,8 @@ struct DevArray {
 }  // namespace
 
 namespace imx {
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
 Layout make_layout(int nx, int ny, int nz, int g, int elem) {
   Layout L;
   L.nx = nx;

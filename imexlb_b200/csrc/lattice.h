@@ -94,6 +94,10 @@ struct GhostPlan {
 bool build_ghost_plan_keys(int kase, int nx, int ny, int nz, const int32_t* usr_padded, GhostPlan* out,
                            std::string* err);
 
+// Record the calling thread's last error message (imexlb_last_error) and
+// return `code`.
+int set_last_error(int code, const std::string& msg);
+
 // ---------------------------------------------------------------- launchers
 struct LaunchCfg {
   Bc bc;

@@ -144,6 +144,25 @@ enum {
 };
 int imexlb_reduce(imexlb_lattice* h, int kind, double* out);
 
+/* The MASS, KINETIC and UMAX reductions over caller-provided device fields
+ * (u, v, w, p, n values each; a field the reduction does not read may be
+ * NULL), writing the result to the device address `out`, asynchronously on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).  No counterpart in
+ * the reference.  It allocates nothing: for callers that may not allocate
+ * device memory (an application that reserves all device memory up front, a
+ * plugin inside a framework that owns every allocation, code that must avoid
+ * cudaMalloc's implicit synchronisation), its partial sums live in a fixed
+ * 32 KiB array inside the library that every GPU using the library holds
+ * until exit.  n is limited to 268435456 cells; larger n is rejected with
+ * IMEXLB_E_ARG.  The first call on a device looks up that array's device
+ * address and must come before any stream capture on that device.  All
+ * calls on a device share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.
+ * Nothing in the array needs to start at zero: each call overwrites every
+ * partial it reads. */
+int imexlb_reduce_fields_noalloc(int kind, const double* u, const double* v, const double* w, const double* p,
+                                 int64_t n, double* out, void* stream);
+
 /* Number of steps taken since the last (re)initialisation. */
 int imexlb_steps_taken(const imexlb_lattice* h, int64_t* steps);
 
