@@ -62,12 +62,26 @@ class ParamsStruct(ctypes.Structure):
                 ("sphere_c", ctypes.c_double * 3), ("stream", ctypes.c_void_p)]
 
 
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [("kase", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("tau0", ctypes.c_double), ("rho0", ctypes.c_double), ("u0", ctypes.c_double),
+                ("lid_u", ctypes.c_double), ("inlet_u", ctypes.c_double), ("sphere_d", ctypes.c_double),
+                ("sphere_c", ctypes.c_double * 3), ("tile_bx", ctypes.c_int)]
+
+
+class EngineStats(ctypes.Structure):
+    _fields_ = [("instances", ctypes.c_int), ("cells", ctypes.c_int64), ("budget_bytes", ctypes.c_size_t),
+                ("used_bytes", ctypes.c_size_t), ("tiles", ctypes.c_int64), ("steps", ctypes.c_int64)]
+
+
 # Every symbol include/imexlb.h declares (tests check the library exports them).
 EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imexlb_initialize", "imexlb_step",
            "imexlb_get_fields", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
            "imexlb_reduce_fields_noalloc", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
-           "imexlb_version"]
+           "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_remove",
+           "imexlb_engine_step", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
+           "imexlb_engine_instance_bytes", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
 
 _LIB = None
 
@@ -102,6 +116,17 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_destroy.restype = None
     lib.imexlb_last_error.restype = ctypes.c_char_p
     lib.imexlb_version.restype = ctypes.c_char_p
+    lib.imexlb_engine_create.argtypes = [i, i, ctypes.c_size_t, i, vp, ctypes.POINTER(vp)]
+    lib.imexlb_engine_add.argtypes = [vp, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_int)]
+    lib.imexlb_engine_remove.argtypes = [vp, i]
+    lib.imexlb_engine_step.argtypes = [vp, i]
+    lib.imexlb_engine_fields.argtypes = [vp, i, vp, vp, vp, vp]
+    lib.imexlb_engine_residuals.argtypes = [vp, vp, i]
+    lib.imexlb_engine_info.argtypes = [vp, ctypes.POINTER(EngineStats)]
+    lib.imexlb_engine_instance_bytes.argtypes = [i, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_size_t)]
+    lib.imexlb_engine_synchronize.argtypes = [vp]
+    lib.imexlb_engine_destroy.argtypes = [vp]
+    lib.imexlb_engine_destroy.restype = None
     _LIB = lib
     return lib
 
@@ -235,3 +260,94 @@ class LBM:
         per = ctypes.c_double()
         _check(self.lib.imexlb_footprint(self.h, ctypes.byref(b), ctypes.byref(per)))
         return b.value, per.value
+
+
+def instance_desc(case: str, nx: int, ny: int, nz: int, tau: float, rho0: float = 1.0, u0: float = 0.05, *,
+                  lid_u: float = 0.0, inlet_u: float = 0.0, sphere_d: float = 0.0, sphere_c=(0.0, 0.0, 0.0),
+                  tile_bx: int = 0) -> InstanceDesc:
+    d = InstanceDesc()
+    d.kase, d.nx, d.ny, d.nz = CASES[case], nx, ny, nz
+    d.tau0, d.rho0, d.u0 = tau, rho0, u0
+    d.lid_u, d.inlet_u, d.sphere_d = lid_u, inlet_u, sphere_d
+    d.sphere_c[0], d.sphere_c[1], d.sphere_c[2] = sphere_c
+    d.tile_bx = tile_bx
+    return d
+
+
+def instance_bytes(storage: str, desc: InstanceDesc) -> int:
+    b = ctypes.c_size_t()
+    _check(load_library().imexlb_engine_instance_bytes(STORAGES[storage], ctypes.byref(desc), ctypes.byref(b)))
+    return b.value
+
+
+class Engine:
+    """Many independent lattices on one GPU, advanced together (C ABI engine)."""
+
+    def __init__(self, storage: str = "f64", arith: str = "fast", budget_bytes: int = 1 << 30,
+                 max_instances: int = 1024, stream: int | None = None):
+        self.lib = load_library()
+        self.storage = storage
+        self.max_instances = max_instances
+        h = ctypes.c_void_p()
+        _check(self.lib.imexlb_engine_create(STORAGES[storage], ARITHS[arith], budget_bytes, max_instances, stream,
+                                             ctypes.byref(h)))
+        self.h = h
+        self.shapes: dict[int, tuple] = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.imexlb_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, desc: InstanceDesc) -> int:
+        """Admit an instance; raises ImexlbError (code 4) when over budget."""
+        slot = ctypes.c_int()
+        _check(self.lib.imexlb_engine_add(self.h, ctypes.byref(desc), ctypes.byref(slot)))
+        self.shapes[slot.value] = (desc.nx, desc.ny, desc.nz)
+        return slot.value
+
+    def try_add(self, desc: InstanceDesc):
+        """Admit an instance, or return None if it does not fit now."""
+        slot = ctypes.c_int()
+        rc = self.lib.imexlb_engine_add(self.h, ctypes.byref(desc), ctypes.byref(slot))
+        if rc == 4:
+            return None
+        _check(rc)
+        self.shapes[slot.value] = (desc.nx, desc.ny, desc.nz)
+        return slot.value
+
+    def remove(self, slot: int):
+        _check(self.lib.imexlb_engine_remove(self.h, slot))
+        self.shapes.pop(slot, None)
+
+    def step(self, n: int = 1):
+        _check(self.lib.imexlb_engine_step(self.h, n))
+
+    def synchronize(self):
+        _check(self.lib.imexlb_engine_synchronize(self.h))
+
+    def fields(self, slot: int) -> dict:
+        nx, ny, nz = self.shapes[slot]
+        out = {k: np.empty((nz, ny, nx)) for k in ("u", "v", "w", "p")}
+        _check(self.lib.imexlb_engine_fields(self.h, slot, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]),
+                                             _ptr(out["p"])))
+        return out
+
+    def residuals(self) -> np.ndarray:
+        out = np.empty(self.max_instances)
+        _check(self.lib.imexlb_engine_residuals(self.h, _ptr(out), self.max_instances))
+        return out
+
+    def stats(self) -> dict:
+        st = EngineStats()
+        _check(self.lib.imexlb_engine_info(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in EngineStats._fields_}

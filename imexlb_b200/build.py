@@ -23,7 +23,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libimexlb.so")
 BIN = os.path.join(HERE, "bin")
 
-SOURCES = ["kernels.cu", "lattice.cu", "ghost_plan.cpp", "noalloc.cu"]
+SOURCES = ["kernels.cu", "lattice.cu", "ghost_plan.cpp", "noalloc.cu", "engine.cu"]
 APPS = ["tgv", "cavity", "sphere"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

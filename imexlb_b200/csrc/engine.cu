@@ -1,0 +1,689 @@
+// Engine: many independent lattices ("instances") of uneven sizes on one GPU,
+// all advanced one time step per persistent kernel launch.
+//
+// Batched solves and the served request stream (no counterpart in the
+// reference, which runs one lattice per process) need many small and medium
+// lattices to share the GPU.  A launch per lattice per step would leave most
+// of the 148 SMs idle on small lattices and pay a launch each; instead the
+// engine keeps a device-side work list of (instance, tile) items covering
+// every active instance, and one persistent launch per step walks it: block b
+// takes items b, b + grid, b + 2 grid, ...  A tile is 256 threads' worth of
+// cells of one instance (bx cells along x by 256/bx rows, times the cells per
+// thread of the storage format); its tile width bx is chosen per instance
+// (autotuned per size and storage).  A block copies the instance's arguments
+// into shared memory once per change of instance and runs exactly the
+// per-cell code of the single-lattice kernels (step_core.cuh).
+//
+// Instances live in one device arena reserved at creation: admission fails
+// (IMEXLB_E_NOMEM) when an instance does not fit the arena's budget, which
+// is how a server admits requests against an HBM budget.  Each instance keeps
+// its own buffer parity, so instances join and leave between any two steps.
+// Two consecutive steps are captured as a CUDA graph and replayed while the
+// set of instances does not change.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/imexlb.h"
+#include "lattice.h"
+#include "step_core.cuh"
+
+namespace imx {
+namespace {
+
+using namespace core;
+
+struct __align__(16) EngInst {
+  StepArgs a;
+  void* buf[2];
+  double* prev;  // u, v, w at the last residual check (3 n values)
+  int rule;      // CaseRule
+  int bx_log2;   // tile width 2^bx_log2 threads along x
+  int parity0;   // engine step parity at admission
+  int pad;
+};
+
+struct Tile {
+  int32_t slot, i0, j0, k;
+};
+
+struct EngArgs {
+  const EngInst* inst;
+  const Tile* tiles;
+  int ntiles;
+  int parity;
+  int store;
+};
+
+// Population planes of one instance: plane q starts q * sq elements into the
+// buffer (27 sq < 2^31 for every engine instance).
+template <class T>
+struct FlatPlanes {
+  const T* src;
+  T* dst;
+  int32_t sq;
+  __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(src + (q * sq + idx)); }
+  __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dst[q * sq + idx] = v; }
+};
+
+template <Store S, bool EXACT>
+__global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea) {
+  using T = typename StoreT<S>::T;
+  constexpr int CPT = CellsPerThread<S>::value;
+  __shared__ EngInst sh;
+  int loaded = -1;  // same tile sequence in every thread: a block-uniform value
+  for (int t = blockIdx.x; t < ea.ntiles; t += gridDim.x) {
+    const Tile tile = ea.tiles[t];
+    if (tile.slot != loaded) {
+      __syncthreads();
+      const int4* from = reinterpret_cast<const int4*>(ea.inst + tile.slot);
+      int4* to = reinterpret_cast<int4*>(&sh);
+      for (int w = threadIdx.x; w < static_cast<int>(sizeof(EngInst) / 16); w += blockDim.x) to[w] = from[w];
+      __syncthreads();
+      if (threadIdx.x == 0) sh.a.store = ea.store;
+      __syncthreads();
+      loaded = tile.slot;
+    }
+    const int cur = (ea.parity ^ sh.parity0) & 1;
+    const FlatPlanes<T> pl{static_cast<const T*>(sh.buf[cur]), static_cast<T*>(sh.buf[1 - cur]),
+                           static_cast<int32_t>(sh.a.sq)};
+    const int bxl = sh.bx_log2;
+    const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
+    const int i = tile.i0 + tx, j0 = tile.j0 + ty * CPT, k = tile.k;
+    double drag[3] = {0.0, 0.0, 0.0};
+    switch (sh.rule) {
+      case static_cast<int>(CaseRule::None):
+        step_cells<S, Bc::Periodic, CaseRule::None, EXACT, false>(sh.a, pl, i, j0, k, drag);
+        break;
+      case static_cast<int>(CaseRule::CavityStd):
+        step_cells<S, Bc::Standard, CaseRule::CavityStd, EXACT, false>(sh.a, pl, i, j0, k, drag);
+        break;
+      default:
+        step_cells<S, Bc::Standard, CaseRule::SphereStd, EXACT, false>(sh.a, pl, i, j0, k, drag);
+        break;
+    }
+  }
+}
+
+// Residual partial sums per tile: sum |u - u_prev|^2 and sum |u|^2 over the
+// tile's cells, then u_prev = u.  Deterministic: per-tile partials are added
+// in tile order per instance afterwards.
+template <int CPT>
+__global__ void engine_resid_kernel(const EngArgs ea, double* part) {
+  __shared__ double sh[2][8];
+  for (int t = blockIdx.x; t < ea.ntiles; t += gridDim.x) {
+    const Tile tile = ea.tiles[t];
+    const EngInst& in = ea.inst[tile.slot];
+    const int bxl = in.bx_log2;
+    const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
+    const int i = tile.i0 + tx, k = tile.k;
+    const int nx = in.a.nx, ny = in.a.ny;
+    const int64_t n = static_cast<int64_t>(nx) * ny * in.a.nz;
+    double d2 = 0.0, n2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int j = tile.j0 + ty * CPT + c;
+      if (i < nx && j < ny) {
+        const int64_t cell = i + static_cast<int64_t>(nx) * (j + static_cast<int64_t>(ny) * k);
+        const double u = in.a.mu[cell], v = in.a.mv[cell], w = in.a.mw[cell];
+        double* pu = in.prev + cell;
+        double* pv = in.prev + n + cell;
+        double* pw = in.prev + 2 * n + cell;
+        const double du = u - *pu, dv = v - *pv, dw = w - *pw;
+        d2 += du * du + dv * dv + dw * dw;
+        n2 += u * u + v * v + w * w;
+        *pu = u;
+        *pv = v;
+        *pw = w;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+      n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+      sh[0][warp] = d2;
+      sh[1][warp] = n2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      double x = 0.0;
+      for (int w = 0; w < 8; ++w) x += sh[threadIdx.x][w];
+      part[2 * static_cast<int64_t>(t) + threadIdx.x] = x;
+    }
+  }
+}
+
+// One block per listed instance: add its tiles' partials in order.
+__global__ void engine_resid_reduce(const int* seg_begin, const int* seg_end, const double* part, double* out) {
+  const int s = blockIdx.x;
+  double d2 = 0.0, n2 = 0.0;
+  for (int t = seg_begin[s] + threadIdx.x; t < seg_end[s]; t += blockDim.x) {
+    d2 += part[2 * static_cast<int64_t>(t)];
+    n2 += part[2 * static_cast<int64_t>(t) + 1];
+  }
+  __shared__ double sh[2][8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+    n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = d2;
+    sh[1][threadIdx.x >> 5] = n2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double x = 0.0;
+    for (int w = 0; w < 8; ++w) x += sh[threadIdx.x][w];
+    out[2 * s + threadIdx.x] = x;
+  }
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t reserve(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    const size_t want = std::max(n, cap + cap / 2);
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), want * sizeof(T));
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+};
+
+// First-fit arena over one device allocation, 512-byte granules, with
+// coalescing of freed neighbours.
+class Arena {
+ public:
+  char* base = nullptr;
+  size_t size = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+  size_t used = 0;
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 511) & ~static_cast<size_t>(511);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      *off = it->first;
+      const size_t rest = it->second - bytes;
+      const size_t o = it->first;
+      free_.erase(it);
+      if (rest) free_[o + bytes] = rest;
+      used += bytes;
+      return true;
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 511) & ~static_cast<size_t>(511);
+    used -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct Slot {
+  bool used = false;
+  imexlb_instance_desc d{};
+  Layout L;
+  size_t off = 0, bytes = 0;
+  int64_t ncell = 0;
+  int64_t steps = 0;
+  bool have_prev = false;
+  int bx_log2 = 5;
+  int seg = -1;  // index into the segment table of the current work list
+};
+
+int bx_log2_for(int nx, int tile_bx) {
+  int bx = tile_bx;
+  if (bx <= 0) {
+    bx = 16;
+    while (bx < nx && bx < 128) bx *= 2;
+  }
+  int l = 0;
+  while ((1 << l) < bx) ++l;
+  return std::min(std::max(l, 3), 8);
+}
+
+}  // namespace
+}  // namespace imx
+
+using namespace imx;
+
+struct imexlb_engine {
+  imexlb_storage storage = IMEXLB_F64;
+  bool exact = false;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Arena arena;
+  std::vector<Slot> slots;
+  std::vector<EngInst> h_inst;
+  DevBuf<EngInst> d_inst;
+  DevBuf<Tile> d_tiles;
+  std::vector<Tile> h_tiles;
+  DevBuf<double> d_part;
+  DevBuf<int> d_seg;  // begin[nseg], end[nseg]
+  DevBuf<double> d_res;
+  std::vector<int> seg_slots;
+  bool dirty = true;
+  int64_t gstep = 0;
+  int grid = 296;
+  cudaGraphExec_t graph = nullptr;
+  int graph_tiles = -1;
+  bool use_graph = true;
+  ~imexlb_engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (arena.base) cudaFree(arena.base);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int efail(int code, const std::string& msg) { return imx::set_last_error(code, msg); }
+
+#define IMX_ECUDA(call)                                                                        \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return efail(IMEXLB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int cpt_of(imexlb_storage s) { return s == IMEXLB_F64 ? 1 : 2; }
+
+int rebuild_tiles(imexlb_engine* e) {
+  if (!e->dirty) return IMEXLB_OK;
+  e->h_tiles.clear();
+  e->seg_slots.clear();
+  std::vector<int> sb, se;
+  const int cpt = cpt_of(e->storage);
+  for (int s = 0; s < static_cast<int>(e->slots.size()); ++s) {
+    Slot& sl = e->slots[s];
+    if (!sl.used) continue;
+    sl.seg = static_cast<int>(e->seg_slots.size());
+    e->seg_slots.push_back(s);
+    sb.push_back(static_cast<int>(e->h_tiles.size()));
+    const int bx = 1 << sl.bx_log2;
+    const int rows = (256 / bx) * cpt;
+    for (int k = 0; k < sl.L.nz; ++k)
+      for (int j0 = 0; j0 < sl.L.ny; j0 += rows)
+        for (int i0 = 0; i0 < sl.L.nx; i0 += bx) e->h_tiles.push_back(Tile{s, i0, j0, k});
+    se.push_back(static_cast<int>(e->h_tiles.size()));
+  }
+  const size_t nt = e->h_tiles.size();
+  if (nt) {
+    IMX_ECUDA(e->d_tiles.reserve(nt));
+    IMX_ECUDA(cudaMemcpyAsync(e->d_tiles.p, e->h_tiles.data(), nt * sizeof(Tile), cudaMemcpyHostToDevice, e->stream));
+    IMX_ECUDA(e->d_part.reserve(2 * nt));
+  }
+  const size_t ns = e->seg_slots.size();
+  if (ns) {
+    std::vector<int> seg(2 * ns);
+    std::copy(sb.begin(), sb.end(), seg.begin());
+    std::copy(se.begin(), se.end(), seg.begin() + ns);
+    IMX_ECUDA(e->d_seg.reserve(2 * ns));
+    IMX_ECUDA(cudaMemcpyAsync(e->d_seg.p, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    IMX_ECUDA(e->d_res.reserve(2 * ns));
+  }
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));  // host vectors may change before the next call
+  e->dirty = false;
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  return IMEXLB_OK;
+}
+
+cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), parity, store};
+  if (ea.ntiles == 0) return cudaSuccess;
+  const int grid = std::min(e->grid, ea.ntiles);
+  switch (e->storage) {
+    case IMEXLB_F64:
+      if (e->exact)
+        engine_step_kernel<Store::F64, true><<<grid, 256, 0, e->stream>>>(ea);
+      else
+        engine_step_kernel<Store::F64, false><<<grid, 256, 0, e->stream>>>(ea);
+      break;
+    case IMEXLB_F32: engine_step_kernel<Store::F32, false><<<grid, 256, 0, e->stream>>>(ea); break;
+    case IMEXLB_F16: engine_step_kernel<Store::F16, false><<<grid, 256, 0, e->stream>>>(ea); break;
+    case IMEXLB_BF16: engine_step_kernel<Store::BF16, false><<<grid, 256, 0, e->stream>>>(ea); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budget_bytes, int max_instances,
+                         void* stream, imexlb_engine** out) {
+  if (!out) return efail(IMEXLB_E_ARG, "null output");
+  *out = nullptr;
+  if (storage < IMEXLB_F64 || storage > IMEXLB_BF16) return efail(IMEXLB_E_ARG, "unknown storage");
+  if (max_instances < 1 || max_instances > 65536) return efail(IMEXLB_E_ARG, "max_instances must be 1..65536");
+  if (budget_bytes < (size_t(1) << 20)) return efail(IMEXLB_E_ARG, "budget below 1 MiB");
+  std::unique_ptr<imexlb_engine> e(new imexlb_engine);
+  e->storage = storage;
+  e->exact = storage == IMEXLB_F64 && arith == IMEXLB_ARITH_EXACT;
+  if (stream) {
+    e->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    IMX_ECUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    e->own_stream = true;
+  }
+  void* base = nullptr;
+  IMX_ECUDA(cudaMalloc(&base, budget_bytes));
+  e->arena.base = static_cast<char*>(base);
+  e->arena.size = budget_bytes;
+  e->arena.free_[0] = budget_bytes & ~static_cast<size_t>(511);
+  e->slots.resize(max_instances);
+  e->h_inst.resize(max_instances);
+  IMX_ECUDA(e->d_inst.reserve(max_instances));
+  int dev = 0, sms = 148;
+  IMX_ECUDA(cudaGetDevice(&dev));
+  IMX_ECUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  e->grid = 2 * sms;
+  *out = e.release();
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot_out) {
+  if (!e || !d || !slot_out) return efail(IMEXLB_E_ARG, "null argument");
+  if (d->kase != IMEXLB_TGV && d->kase != IMEXLB_CAVITY && d->kase != IMEXLB_SPHERE)
+    return efail(IMEXLB_E_ARG, "unknown case");
+  if (d->nx < 2 || d->ny < 2 || d->nz < 2 || d->nz > 65535) return efail(IMEXLB_E_ARG, "bad extents");
+  if (!(d->tau0 > 0.0)) return efail(IMEXLB_E_ARG, "tau0 must be positive");
+  int s = -1;
+  for (int i = 0; i < static_cast<int>(e->slots.size()); ++i)
+    if (!e->slots[i].used) {
+      s = i;
+      break;
+    }
+  if (s < 0) return efail(IMEXLB_E_NOMEM, "no free instance slot");
+  const int elem = e->storage == IMEXLB_F64 ? 8 : (e->storage == IMEXLB_F32 ? 4 : 2);
+  Slot sl;
+  sl.d = *d;
+  sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem);
+  if (static_cast<double>(sl.L.sq) * Q >= 2147483647.0) return efail(IMEXLB_E_ARG, "instance too large for the engine");
+  sl.ncell = static_cast<int64_t>(d->nx) * d->ny * d->nz;
+  const size_t fbytes = (sl.L.bytes() + 511) & ~static_cast<size_t>(511);
+  const size_t mbytes = ((4 * sl.ncell * 8) + 511) & ~static_cast<size_t>(511);
+  const size_t pbytes = ((3 * sl.ncell * 8) + 511) & ~static_cast<size_t>(511);
+  const size_t mask_bytes = static_cast<size_t>((sl.ncell + 255) & ~int64_t(255));
+  const size_t sbytes = d->kase == IMEXLB_SPHERE ? ((mask_bytes + 4 * sl.ncell + 511) & ~static_cast<size_t>(511)) : 0;
+  sl.bytes = 2 * fbytes + mbytes + pbytes + sbytes;
+  if (!e->arena.alloc(sl.bytes, &sl.off))
+    return efail(IMEXLB_E_NOMEM, "instance does not fit the engine's memory budget");
+  char* b = e->arena.base + sl.off;
+  void* buf0 = b;
+  void* buf1 = b + fbytes;
+  double* mom = reinterpret_cast<double*>(b + 2 * fbytes);
+  double* prev = reinterpret_cast<double*>(b + 2 * fbytes + mbytes);
+  uint8_t* usr = d->kase == IMEXLB_SPHERE ? reinterpret_cast<uint8_t*>(b + 2 * fbytes + mbytes + pbytes) : nullptr;
+  uint32_t* links = usr ? reinterpret_cast<uint32_t*>(usr + mask_bytes) : nullptr;
+
+  // initial fields (the same set-up as a single lattice)
+  imexlb_params P;
+  imexlb_params_default(&P);
+  P.kase = d->kase;
+  P.bc = d->kase == IMEXLB_TGV ? IMEXLB_BC_REFERENCE : IMEXLB_BC_STANDARD;
+  P.storage = e->storage;
+  P.nx = d->nx;
+  P.ny = d->ny;
+  P.nz = d->nz;
+  P.tau0 = d->tau0;
+  P.rho0 = d->rho0;
+  P.u0 = d->u0;
+  P.lid_u = d->lid_u != 0.0 ? d->lid_u : d->u0;
+  P.inlet_u = d->inlet_u != 0.0 ? d->inlet_u : d->u0;
+  P.sphere_d = d->sphere_d != 0.0 ? d->sphere_d : d->nx / 24.0;
+  P.sphere_c[0] = d->sphere_c[0];
+  P.sphere_c[1] = d->sphere_c[1];
+  P.sphere_c[2] = d->sphere_c[2];
+  if (d->kase == IMEXLB_SPHERE && P.sphere_c[0] == 0.0 && P.sphere_c[1] == 0.0 && P.sphere_c[2] == 0.0) {
+    P.sphere_c[0] = d->nx / 4.0;
+    P.sphere_c[1] = d->ny / 2.0;
+    P.sphere_c[2] = d->nz / 2.0;
+  }
+  std::vector<int32_t> usr_pad(d->kase == IMEXLB_SPHERE ? static_cast<size_t>(sl.ncell) : 0, 1);
+  std::vector<double> U, V, W, Pf;
+  case_fields(P, sl.L, nullptr, &usr_pad, U, V, W, Pf);
+  const size_t n = static_cast<size_t>(sl.ncell);
+  IMX_ECUDA(cudaMemcpyAsync(mom, U.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaMemcpyAsync(mom + n, V.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaMemcpyAsync(mom + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaMemcpyAsync(mom + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
+
+  EngInst& in = e->h_inst[s];
+  in = EngInst{};
+  StepArgs& a = in.a;
+  a.nx = d->nx;
+  a.ny = d->ny;
+  a.nz = d->nz;
+  a.sq = sl.L.sq;
+  a.sz = sl.L.sz;
+  a.pitch = sl.L.pitch;
+  a.base = sl.L.idx(0, 0, 0, 0);
+  for (int q = 0; q < Q; ++q) {
+    a.rel[q] = static_cast<int32_t>(-(D3Q27::ez[q] * sl.L.sz + D3Q27::ey[q] * sl.L.pitch + D3Q27::ex[q]));
+    a.off[q] = q * sl.L.sq + a.rel[q];
+  }
+  a.base32 = static_cast<int32_t>(a.base);
+  a.sz32 = static_cast<int32_t>(sl.L.sz);
+  a.pitch32 = static_cast<int32_t>(sl.L.pitch);
+  a.tau_half = d->tau0 + 0.5;
+  a.omega = 1.0 / (d->tau0 + 0.5);
+  a.mu = mom;
+  a.mv = mom + n;
+  a.mw = mom + 2 * n;
+  a.mp = mom + 3 * n;
+  a.lid_u = P.lid_u;
+  a.rho_w = P.rho0;
+  a.inlet_u = P.inlet_u;
+  const double p_rest = d->kase == IMEXLB_TGV ? d->rho0 / 3.0 : 0.0;
+  a.p_shift = e->storage == IMEXLB_F64 ? 0.0 : p_rest;
+  for (int q = 0; q < Q; ++q) {
+    const double t = weight_of_class(D3Q27::wclass[q]);
+    const double sc = e->storage == IMEXLB_F16 ? 16384.0 / t : (e->storage == IMEXLB_BF16 ? 1.0 / t : 1.0);
+    a.enc.scale[q] = static_cast<float>(sc);
+    a.enc.inv_scale[q] = static_cast<float>(1.0 / sc);
+  }
+  in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
+                                                   : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
+  if (d->kase == IMEXLB_SPHERE) {
+    std::vector<uint8_t> m(n);
+    for (size_t c = 0; c < n; ++c) m[c] = static_cast<uint8_t>(usr_pad[c]);
+    std::vector<uint32_t> lk;
+    int lo[3], hi[3];
+    solid_links(d->nx, d->ny, d->nz, m.data(), lk, lo, hi);
+    IMX_ECUDA(cudaMemcpyAsync(usr, m.data(), n, cudaMemcpyHostToDevice, e->stream));
+    IMX_ECUDA(cudaMemcpyAsync(links, lk.data(), n * 4, cudaMemcpyHostToDevice, e->stream));
+    a.usr = usr;
+    a.links = links;
+    for (int c = 0; c < 3; ++c) {
+      a.near_lo[c] = lo[c];
+      a.near_hi[c] = hi[c];
+    }
+    const double ui = P.inlet_u;
+    for (int q = 0; q < Q; ++q) {
+      const double t = weight_of_class(D3Q27::wclass[q]);
+      const double ev = D3Q27::ex[q] * ui;
+      a.feq_in[q] = t * (3.0 * (0.0 - a.p_shift) + 3.0 * ev + 4.5 * ev * ev - 1.5 * ui * ui);
+    }
+  }
+  in.buf[0] = buf0;
+  in.buf[1] = buf1;
+  in.prev = prev;
+  sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
+  in.bx_log2 = sl.bx_log2;
+  in.parity0 = static_cast<int>(e->gstep & 1);
+  LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
+                e->exact};
+  IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
+  IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + s, &in, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  sl.used = true;
+  e->slots[s] = sl;
+  e->dirty = true;
+  *slot_out = s;
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_remove(imexlb_engine* e, int slot) {
+  if (!e || slot < 0 || slot >= static_cast<int>(e->slots.size()) || !e->slots[slot].used)
+    return efail(IMEXLB_E_ARG, "no such instance");
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  Slot& sl = e->slots[slot];
+  e->arena.release(sl.off, sl.bytes);
+  sl = Slot{};
+  e->dirty = true;
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_step(imexlb_engine* e, int nsteps) {
+  if (!e) return efail(IMEXLB_E_ARG, "null engine");
+  if (nsteps < 0) return efail(IMEXLB_E_ARG, "negative step count");
+  if (nsteps == 0) return IMEXLB_OK;
+  int rc = rebuild_tiles(e);
+  if (rc) return rc;
+  int left = nsteps;
+  while (left > 0) {
+    const bool last = left == 1;
+    if (!last && left >= 3 && (e->gstep & 1) == 0 && e->use_graph && !e->h_tiles.empty()) {
+      if (!e->graph) {
+        cudaGraph_t g = nullptr;
+        IMX_ECUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = launch_engine(e, 0, 0);
+        cudaError_t e2 = launch_engine(e, 1, 0);
+        cudaError_t e3 = cudaStreamEndCapture(e->stream, &g);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+          if (g) cudaGraphDestroy(g);
+          return efail(IMEXLB_E_CUDA, "capturing the engine's step graph failed");
+        }
+        cudaError_t e4 = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e4 != cudaSuccess) return efail(IMEXLB_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e4));
+      }
+      IMX_ECUDA(cudaGraphLaunch(e->graph, e->stream));
+      e->gstep += 2;
+      left -= 2;
+      continue;
+    }
+    IMX_ECUDA(launch_engine(e, static_cast<int>(e->gstep & 1), last ? 1 : 0));
+    ++e->gstep;
+    --left;
+  }
+  for (auto& sl : e->slots)
+    if (sl.used) sl.steps += nsteps;
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, double* w, double* p) {
+  if (!e || slot < 0 || slot >= static_cast<int>(e->slots.size()) || !e->slots[slot].used)
+    return efail(IMEXLB_E_ARG, "no such instance");
+  const EngInst& in = e->h_inst[slot];
+  const size_t n = static_cast<size_t>(e->slots[slot].ncell);
+  double* dst[4] = {u, v, w, p};
+  double* src[4] = {in.a.mu, in.a.mv, in.a.mw, in.a.mp};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c]) IMX_ECUDA(cudaMemcpyAsync(dst[c], src[c], n * 8, cudaMemcpyDeviceToHost, e->stream));
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
+  if (!e || !out) return efail(IMEXLB_E_ARG, "null argument");
+  if (n_out < static_cast<int>(e->slots.size())) return efail(IMEXLB_E_ARG, "output shorter than max_instances");
+  int rc = rebuild_tiles(e);
+  if (rc) return rc;
+  for (int s = 0; s < n_out; ++s) out[s] = NAN;
+  if (e->h_tiles.empty()) return IMEXLB_OK;
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), 0, 0};
+  const int grid = std::min(e->grid * 2, ea.ntiles);
+  if (cpt_of(e->storage) == 1)
+    engine_resid_kernel<1><<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
+  else
+    engine_resid_kernel<2><<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
+  const int ns = static_cast<int>(e->seg_slots.size());
+  engine_resid_reduce<<<ns, 256, 0, e->stream>>>(e->d_seg.p, e->d_seg.p + ns, e->d_part.p, e->d_res.p);
+  IMX_ECUDA(cudaGetLastError());
+  std::vector<double> res(2 * static_cast<size_t>(ns));
+  IMX_ECUDA(cudaMemcpyAsync(res.data(), e->d_res.p, res.size() * 8, cudaMemcpyDeviceToHost, e->stream));
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  for (int g = 0; g < ns; ++g) {
+    Slot& sl = e->slots[e->seg_slots[g]];
+    const double d2 = res[2 * g], n2 = res[2 * g + 1];
+    out[e->seg_slots[g]] = !sl.have_prev ? INFINITY : (n2 > 0 ? std::sqrt(d2 / n2) : (d2 > 0 ? INFINITY : 0.0));
+    if (!std::isfinite(d2) || !std::isfinite(n2)) out[e->seg_slots[g]] = NAN;
+    sl.have_prev = true;
+  }
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st) {
+  if (!e || !st) return efail(IMEXLB_E_ARG, "null argument");
+  st->instances = 0;
+  st->cells = 0;
+  for (const auto& sl : e->slots)
+    if (sl.used) {
+      ++st->instances;
+      st->cells += sl.ncell;
+    }
+  st->budget_bytes = e->arena.size;
+  st->used_bytes = e->arena.used;
+  st->tiles = static_cast<int64_t>(e->h_tiles.size());
+  st->steps = e->gstep;
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes) {
+  if (!d || !bytes) return efail(IMEXLB_E_ARG, "null argument");
+  const int elem = storage == IMEXLB_F64 ? 8 : (storage == IMEXLB_F32 ? 4 : 2);
+  const Layout L = make_layout(d->nx, d->ny, d->nz, 0, elem);
+  const int64_t n = static_cast<int64_t>(d->nx) * d->ny * d->nz;
+  auto r = [](size_t x) { return (x + 511) & ~static_cast<size_t>(511); };
+  const size_t mask = static_cast<size_t>((n + 255) & ~int64_t(255));
+  *bytes = 2 * r(L.bytes()) + r(4 * n * 8) + r(3 * n * 8) + (d->kase == IMEXLB_SPHERE ? r(mask + 4 * n) : 0);
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_synchronize(imexlb_engine* e) {
+  if (!e) return efail(IMEXLB_E_ARG, "null engine");
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  return IMEXLB_OK;
+}
+
+void imexlb_engine_destroy(imexlb_engine* e) {
+  if (!e) return;
+  cudaStreamSynchronize(e->stream);
+  delete e;
+}
+
+}  // extern "C"

@@ -92,6 +92,40 @@ Layout make_layout(int nx, int ny, int nz, int g, int elem) {
 }
 }  // namespace imx
 
+namespace imx {
+// Standard sphere channel: bit q of a fluid cell's word is set when its pull
+// along -e_q starts in a solid cell (y and z periodic; the x ends belong to
+// the inlet and outlet rules).  lo/hi: bounding box of cells with a set bit.
+void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]) {
+  links.assign(static_cast<size_t>(nx) * ny * nz, 0u);
+  lo[0] = nx;
+  lo[1] = ny;
+  lo[2] = nz;
+  hi[0] = hi[1] = hi[2] = -1;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t c = i + static_cast<size_t>(nx) * (j + static_cast<size_t>(ny) * k);
+        if (!fluid[c]) continue;
+        uint32_t bits = 0;
+        for (int q = 0; q < Q; ++q) {
+          const int si = i - D3Q27::ex[q];
+          if (si < 0 || si >= nx) continue;
+          const int sj = (j - D3Q27::ey[q] + ny) % ny, sk = (k - D3Q27::ez[q] + nz) % nz;
+          if (!fluid[si + static_cast<size_t>(nx) * (sj + static_cast<size_t>(ny) * sk)]) bits |= 1u << q;
+        }
+        links[c] = bits;
+        if (bits) {
+          const int x[3] = {i, j, k};
+          for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], x[d]);
+            hi[d] = std::max(hi[d], x[d]);
+          }
+        }
+      }
+}
+}  // namespace imx
+
 struct imexlb_lattice {
   imexlb_params P{};
   Layout L;
@@ -153,8 +187,14 @@ bool is_float_store(imexlb_storage s) { return s != IMEXLB_F64; }
 // reference boundaries, interior otherwise), x fastest.
 void init_fields(imexlb_lattice* h, std::vector<double>& U, std::vector<double>& V, std::vector<double>& W,
                  std::vector<double>& Pf) {
-  const Layout& L = h->L;
-  const imexlb_params& P = h->P;
+  case_fields(h->P, h->L, h->ran.empty() ? nullptr : h->ran.data(), &h->usr_padded, U, V, W, Pf);
+}
+
+}  // namespace
+
+namespace imx {
+void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
+                 std::vector<double>& U, std::vector<double>& V, std::vector<double>& W, std::vector<double>& Pf) {
   const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
   U.assign(n, 0.0);
   V.assign(n, 0.0);
@@ -191,9 +231,9 @@ void init_fields(imexlb_lattice* h, std::vector<double>& U, std::vector<double>&
           const int dx = i - GHOST - c8, dy = j - GHOST - c8, dz = k - GHOST - c8;
           const double d2 = static_cast<double>(dx) * dx + static_cast<double>(dy) * dy + static_cast<double>(dz) * dz;
           const int s = (d2 <= r * r) ? 0 : 1;
-          h->usr_padded[c] = s;
+          (*usr_padded)[c] = s;
           U[c] = (u0 * 4.0 * (k - GHOST) * (glz - 1 - (k - GHOST)) / (static_cast<double>(glz - 1) * (glz - 1))) * s *
-                 (1.0 + h->ran[c] * 0.001);
+                 (1.0 + ran[c] * 0.001);
         }
   } else if (P.kase == IMEXLB_SPHERE) {
     // standard channel: uniform inlet velocity in the fluid at rest pressure
@@ -204,12 +244,15 @@ void init_fields(imexlb_lattice* h, std::vector<double>& U, std::vector<double>&
           const size_t c = at(i, j, k);
           const double dx = i - P.sphere_c[0], dy = j - P.sphere_c[1], dz = k - P.sphere_c[2];
           const bool solid = dx * dx + dy * dy + dz * dz <= 0.25 * P.sphere_d * P.sphere_d;
-          h->usr_padded[c] = solid ? 0 : 1;
+          (*usr_padded)[c] = solid ? 0 : 1;
           U[c] = solid ? 0.0 : ui;
         }
   }
   // cavity (both boundary kinds): u = p = 0 (lid_driven_cavity/src/lbm.cpp:191-198)
 }
+}  // namespace imx
+
+namespace {
 
 int upload_case(imexlb_lattice* h) {
   const Layout& L = h->L;
@@ -305,6 +348,8 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   if (P.storage < IMEXLB_F64 || P.storage > IMEXLB_BF16) return fail(IMEXLB_E_ARG, "unknown storage");
   if (P.nx < 2 || P.ny < 2 || P.nz < 2) return fail(IMEXLB_E_ARG, "lattice extents must be >= 2");
   if (P.nz > 65535) return fail(IMEXLB_E_ARG, "nz above 65535");
+  if (static_cast<double>(P.nx + 80) * (P.ny + 6) * (P.nz + 6) >= 2147483647.0)
+    return fail(IMEXLB_E_ARG, "lattice too large: one population plane must stay below 2^31 values");
   if (!(P.tau0 > 0.0) || !std::isfinite(P.tau0)) return fail(IMEXLB_E_ARG, "tau0 must be positive");
   const bool ref_sphere = P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE;
   if (ref_sphere && (P.nx - 1) / 8 + (P.nx - 1) / 64.0 + 2 >= std::min(P.ny, P.nz))
@@ -376,8 +421,13 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   a.sz = L.sz;
   a.pitch = L.pitch;
   a.base = L.idx(0, L.g, L.g, L.g);
-  for (int q = 0; q < Q; ++q)
+  for (int q = 0; q < Q; ++q) {
     a.off[q] = q * L.sq - (D3Q27::ez[q] * L.sz + D3Q27::ey[q] * L.pitch + D3Q27::ex[q]);
+    a.rel[q] = static_cast<int32_t>(-(D3Q27::ez[q] * L.sz + D3Q27::ey[q] * L.pitch + D3Q27::ex[q]));
+  }
+  a.base32 = static_cast<int32_t>(a.base);
+  a.sz32 = static_cast<int32_t>(L.sz);
+  a.pitch32 = static_cast<int32_t>(L.pitch);
   a.tau_half = P.tau0 + 0.5;
   a.omega = 1.0 / (P.tau0 + 0.5);
   a.mu = h->mom.p;
@@ -412,31 +462,9 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       IMX_CUDA(cudaMemcpy(h->inlet.p, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
       a.inlet = h->inlet.p;
     } else {
-      // per-cell bit q: the cell's pull along -e_q starts in a solid cell
-      // (y and z periodic; the x ends are handled by the inlet/outlet rules)
-      std::vector<uint32_t> links(static_cast<size_t>(h->ncell), 0u);
-      int lo[3] = {P.nx, P.ny, P.nz}, hi[3] = {-1, -1, -1};
-      for (int k = 0; k < P.nz; ++k)
-        for (int j = 0; j < P.ny; ++j)
-          for (int i = 0; i < P.nx; ++i) {
-            const size_t c = i + static_cast<size_t>(P.nx) * (j + static_cast<size_t>(P.ny) * k);
-            if (!m[c]) continue;
-            uint32_t bits = 0;
-            for (int q = 0; q < Q; ++q) {
-              const int si = i - D3Q27::ex[q];
-              if (si < 0 || si >= P.nx) continue;
-              const int sj = (j - D3Q27::ey[q] + P.ny) % P.ny, sk = (k - D3Q27::ez[q] + P.nz) % P.nz;
-              if (!m[si + static_cast<size_t>(P.nx) * (sj + static_cast<size_t>(P.ny) * sk)]) bits |= 1u << q;
-            }
-            links[c] = bits;
-            if (bits) {
-              const int x[3] = {i, j, k};
-              for (int d = 0; d < 3; ++d) {
-                lo[d] = std::min(lo[d], x[d]);
-                hi[d] = std::max(hi[d], x[d]);
-              }
-            }
-          }
+      std::vector<uint32_t> links;
+      int lo[3], hi[3];
+      solid_links(P.nx, P.ny, P.nz, m.data(), links, lo, hi);
       IMX_CUDA(h->links.alloc(links.size()));
       IMX_CUDA(cudaMemcpy(h->links.p, links.data(), links.size() * 4, cudaMemcpyHostToDevice));
       a.links = h->links.p;
@@ -504,6 +532,10 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     a.src = h->buf[h->cur].p;
     a.dst = h->buf[1 - h->cur].p;
+    for (int q = 0; q < Q; ++q) {
+      a.srcq[q] = h->buf[h->cur].p + static_cast<size_t>(q) * h->L.sq * h->L.elem;
+      a.dstq[q] = h->buf[1 - h->cur].p + static_cast<size_t>(q) * h->L.sq * h->L.elem;
+    }
     a.store = s == nsteps - 1;
     a.drag_part = (a.store && h->drag_part.p) ? h->drag_part.p : nullptr;
     imexlb_lattice::Timed t0{nullptr, nullptr, 0}, t1{nullptr, nullptr, 1};

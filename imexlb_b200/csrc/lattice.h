@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "d3q27.cuh"
+#include "../../include/imexlb.h"
 
 namespace imx {
 
@@ -57,6 +58,12 @@ struct StepArgs {
   int64_t sq = 0, sz = 0, pitch = 0;
   int64_t base = 0;    // stored index of interior cell (0,0,0), population 0
   int64_t off[Q] = {}; // pull offset of population q relative to a cell's base index
+  // plane addressing (step kernels): population q of a cell is
+  // plane_q[base32 + k*sz32 + j*pitch32 + i], pulled from index + rel[q]
+  const void* srcq[Q] = {};
+  void* dstq[Q] = {};
+  int32_t rel[Q] = {};
+  int32_t base32 = 0, sz32 = 0, pitch32 = 0;
   double tau_half = 1; // tau0 + 0.5
   double omega = 1;    // 1 / (tau0 + 0.5)
   double* mu = nullptr;
@@ -93,6 +100,15 @@ struct GhostPlan {
 // Returns false and sets *err if the passes would race.
 bool build_ghost_plan_keys(int kase, int nx, int ny, int nz, const int32_t* usr_padded, GhostPlan* out,
                            std::string* err);
+
+// Case set-up shared by single lattices and the engine: the initial u, v, w,
+// p over the box the layout stores (x fastest) and, for spheres, the solid
+// mask over the same box (reference: sphere/src/lbm.cpp:231-242; standard:
+// the voxelised sphere |x - c|^2 <= d^2/4).  `ran` is the reference sphere's
+// padded random field (unused otherwise).
+void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
+                 std::vector<double>& U, std::vector<double>& V, std::vector<double>& W, std::vector<double>& Pf);
+void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]);
 
 // Record the calling thread's last error message (imexlb_last_error) and
 // return `code`.

@@ -1,0 +1,523 @@
+// Per-cell device machinery of the fused D3Q27 step, shared by the
+// single-lattice kernels (kernels.cu) and the batched engine (engine.cu):
+// arithmetic modes, equilibrium, moments, storage encodings, and the load and
+// compute phases of one cell.  See kernels.cu for the step's structure.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <type_traits>
+#include <utility>
+
+#include "lattice.h"
+
+namespace imx {
+namespace core {
+
+template <int A, int B, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (A < B) {
+    f(std::integral_constant<int, A>{});
+    static_for<A + 1, B>(f);
+  }
+}
+
+// ------------------------------------------------------------ arithmetic
+// EXACT: one rounding per operation in the reference's order (the __d*_rn
+// intrinsics are never contracted into fused multiply-adds), and true IEEE
+// division.  FAST: ordinary operators; nvcc fuses multiply-adds.
+template <class R, bool EXACT> struct Ar {
+  static __device__ __forceinline__ R add(R a, R b) { return a + b; }
+  static __device__ __forceinline__ R sub(R a, R b) { return a - b; }
+  static __device__ __forceinline__ R mul(R a, R b) { return a * b; }
+};
+template <> struct Ar<double, true> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+};
+
+// e_q . (u, v, w) for e components in {-1, 0, 1}.  The reference forms
+// (e0*u + e1*v) + e2*w; multiplying by +-1 is exact and adding a zero product
+// leaves the sum unchanged, so dropping zero terms and negating for -1 gives
+// the same value (up to the sign of an all-zero result, which no later
+// operation can observe).
+template <int q, class R, bool EXACT>
+__device__ __forceinline__ R edu_of(R u, R v, R w) {
+  using A = Ar<R, EXACT>;
+  constexpr int a = D3Q27::ex[q], b = D3Q27::ey[q], c = D3Q27::ez[q];
+  R t = R(0);
+  if constexpr (a != 0) t = a > 0 ? u : -u;
+  if constexpr (b != 0) {
+    if constexpr (a != 0)
+      t = b > 0 ? A::add(t, v) : A::sub(t, v);
+    else
+      t = b > 0 ? v : -v;
+  }
+  if constexpr (c != 0) {
+    if constexpr (a != 0 || b != 0)
+      t = c > 0 ? A::add(t, w) : A::sub(t, w);
+    else
+      t = c > 0 ? w : -w;
+  }
+  return t;
+}
+
+// RN(x / 3) in three FP64 operations (Markstein's correction step: P.
+// Markstein, IBM J. Res. Dev. 34(1), 1990).  With z = RN(1/3):
+//   q0 = RN(x z) is within 1.75 ulp of x/3, so r = x - 3 q0 is a multiple of
+//   ulp(q0) of magnitude <= 5.25 ulp(q0): the fma computes it exactly;
+//   q1 = RN(q0 + r z) = RN(x/3 + eta) with |eta| < 2^-52 ulp.
+// x/3 is never within ulp/6 of a midpoint between doubles (a midpoint has an
+// odd 54-bit significand, 3 times it cannot equal the 53-bit x), so q1 is
+// exactly the correctly rounded quotient, as IEEE division gives.  Valid for
+// zero and every x whose quotient is normal (the lattice values are O(1)).
+__device__ __forceinline__ double div3_rn(double x) {
+  const double z = 0x1.5555555555555p-2;
+  const double q0 = __dmul_rn(x, z);
+  const double r = __fma_rn(-q0, 3.0, x);
+  return __fma_rn(r, z, q0);
+}
+
+// RN(x / d) for d > 0, given z = RN(1/d), proven on the fast path and
+// deferred to IEEE division otherwise:
+//   q0 = RN(x z), r0 = x - q0 d (fma), q1 = RN(q0 + r0 z)   (Markstein 1990)
+//   r1 = x - q1 d by fma is exact whenever q1 is within one ulp of x/d (the
+//   remainder is then an integer multiple of ulp(q1) ulp(d) below 2^53 of them);
+//   q1 is the correctly rounded quotient if x/d lies strictly within half the
+//   smaller neighbouring gap of q1, i.e. |r1| < d * gap_below(q1) / 2.  If q1 is
+//   further than one ulp away, |r1| exceeds that bound, so a wrong q1 is never
+//   accepted; rejected cases (ties, near-ties, zero, tiny quotients) take
+//   __ddiv_rn.  The bound is a power of two times d, so it is exact.
+__device__ __forceinline__ double div_rn(double x, double d, double z) {
+  const double q0 = __dmul_rn(x, z);
+  const double r0 = __fma_rn(-q0, d, x);
+  const double q1 = __fma_rn(r0, z, q0);
+  const double r1 = __fma_rn(-q1, d, x);
+  const long long bits = __double_as_longlong(q1);
+  const int e = static_cast<int>((bits >> 52) & 0x7ff);
+  const int he = e - 53 - ((bits & 0xFFFFFFFFFFFFFLL) == 0 ? 1 : 0);  // exponent field of gap_below / 2
+  if (he > 0 && fabs(r1) < __dmul_rn(d, __longlong_as_double(static_cast<long long>(he) << 52))) return q1;
+  return __ddiv_rn(x, d);
+}
+
+template <class R>
+__device__ __forceinline__ R wgt(int cls) {
+  return cls == 0 ? R(8.0 / 27.0) : (cls == 1 ? R(2.0 / 27.0) : (cls == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0)));
+}
+
+// Moments of the pulled populations.  EXACT follows the reference sums term
+// by term in population order from a zero accumulator: p += f/3.0,
+// u += f*e_x, ...  (a product with e = 0 adds nothing).
+template <class R, bool EXACT>
+__device__ __forceinline__ void moments(const R (&f)[Q], R& u, R& v, R& w, R& p) {
+  if constexpr (EXACT) {
+    using A = Ar<double, true>;
+    double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      pm = A::add(pm, div3_rn(f[q]));
+      if constexpr (D3Q27::ex[q] == 1) um = A::add(um, f[q]);
+      if constexpr (D3Q27::ex[q] == -1) um = A::sub(um, f[q]);
+      if constexpr (D3Q27::ey[q] == 1) vm = A::add(vm, f[q]);
+      if constexpr (D3Q27::ey[q] == -1) vm = A::sub(vm, f[q]);
+      if constexpr (D3Q27::ez[q] == 1) wm = A::add(wm, f[q]);
+      if constexpr (D3Q27::ez[q] == -1) wm = A::sub(wm, f[q]);
+    });
+    u = um;
+    v = vm;
+    w = wm;
+    p = pm;
+  } else {
+    R s = R(0), um = R(0), vm = R(0), wm = R(0);
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      s += f[q];
+      if constexpr (D3Q27::ex[q] == 1) um += f[q];
+      if constexpr (D3Q27::ex[q] == -1) um -= f[q];
+      if constexpr (D3Q27::ey[q] == 1) vm += f[q];
+      if constexpr (D3Q27::ey[q] == -1) vm -= f[q];
+      if constexpr (D3Q27::ez[q] == 1) wm += f[q];
+      if constexpr (D3Q27::ez[q] == -1) wm -= f[q];
+    });
+    u = um;
+    v = vm;
+    w = wm;
+    p = s * R(1.0 / 3.0);
+  }
+}
+
+// Equilibrium of the reference (tgv/src/lbm.cpp:228-232):
+//   feq = t*p*3 + t*(3 edu + 4.5 edu^2 - 1.5 u.u)
+template <int q, class R, bool EXACT>
+__device__ __forceinline__ R feq_of(R u, R v, R w, const R (&tp3)[4], R udu15) {
+  using A = Ar<R, EXACT>;
+  constexpr int cls = D3Q27::wclass[q];
+  const R e = edu_of<q, R, EXACT>(u, v, w);
+  const R br = A::sub(A::add(A::mul(R(3.0), e), A::mul(R(4.5), A::mul(e, e))), udu15);
+  return A::add(tp3[cls], A::mul(wgt<R>(cls), br));
+}
+
+template <class R, bool EXACT>
+__device__ __forceinline__ void feq_prep(R u, R v, R w, R p, R (&tp3)[4], R& udu15) {
+  using A = Ar<R, EXACT>;
+  const R udu = A::add(A::add(A::mul(u, u), A::mul(v, v)), A::mul(w, w));
+  udu15 = A::mul(R(1.5), udu);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tp3[c] = A::mul(A::mul(wgt<R>(c), p), R(3.0));
+}
+
+// ------------------------------------------------------------ storage
+template <Store S> struct StoreT;
+template <> struct StoreT<Store::F64> { using T = double; using R = double; };
+template <> struct StoreT<Store::F32> { using T = float; using R = float; };
+template <> struct StoreT<Store::F16> { using T = __half; using R = float; };
+template <> struct StoreT<Store::BF16> { using T = __nv_bfloat16; using R = float; };
+
+// Reduced-precision storage holds the deviation d_q = f_q - 3 w_q p_shift
+// (p_shift = the rest pressure) times a per-population scale.  The step works
+// on deviations throughout: their moments are (u, v, w, p - p_shift) and
+// feq(u, p) - 3 w_q p_shift = feq(u, p - p_shift), so nothing large cancels in
+// FP32.  FP64 storage keeps f itself (p_shift = 0).
+template <Store S>
+__device__ __forceinline__ typename StoreT<S>::R decode(typename StoreT<S>::T x, int q, const Encoding& e) {
+  if constexpr (S == Store::F64 || S == Store::F32) {
+    return x;
+  } else if constexpr (S == Store::F16) {
+    return __half2float(x) * e.inv_scale[q];
+  } else {
+    return __bfloat162float(x) * e.inv_scale[q];
+  }
+}
+template <Store S>
+__device__ __forceinline__ typename StoreT<S>::T encode(typename StoreT<S>::R x, int q, const Encoding& e) {
+  if constexpr (S == Store::F64 || S == Store::F32) {
+    return x;
+  } else if constexpr (S == Store::F16) {
+    return __float2half_rn(x * e.scale[q]);
+  } else {
+    return __float2bfloat16_rn(x * e.scale[q]);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T ldg_stream(const T* p) {
+  return __ldg(p);
+}
+
+// ------------------------------------------------------------ step
+// The step is split into a load phase (pull the 27 populations of a cell,
+// applying the boundary rule of each link) and a compute phase (moments,
+// case rules, collision, stores).  A thread handles CPT cells stacked along
+// y and issues the loads of all of them before any arithmetic, so enough
+// bytes are in flight per thread for the narrow storage formats.  Every
+// boundary rule is expressed as a per-link choice of source address, never
+// as divergent control flow: a warp always issues its loads back to back.
+//
+// Addressing: each population q lives in its own plane; a cell's value is
+// plane_q[idx] with idx = base + k*sz + j*pitch + i (32-bit, in elements),
+// and the pull adds the plane-independent offset rel[q] = -(ez sz + ey pitch
+// + ex).  The single-lattice kernels take the 27 plane pointers as launch
+// parameters; the engine derives them from one buffer and the plane stride.
+
+// Cell flags for the standard boundaries: which walls the cell touches
+// (bit 0..5: x-, x+, y-, y+, z-, z+) -- the lid is z+.
+__device__ __forceinline__ unsigned wall_flags(const StepArgs& a, int i, int j, int k) {
+  return (i == 0 ? 1u : 0u) | (i == a.nx - 1 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == a.ny - 1 ? 8u : 0u) |
+         (k == 0 ? 16u : 0u) | (k == a.nz - 1 ? 32u : 0u);
+}
+// the link of population q leaves the box through a wall the cell touches
+template <int q>
+__device__ __forceinline__ bool leaves(unsigned w) {
+  constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+  constexpr unsigned m = (ex > 0 ? 1u : 0u) | (ex < 0 ? 2u : 0u) | (ey > 0 ? 4u : 0u) | (ey < 0 ? 8u : 0u) |
+                         (ez > 0 ? 16u : 0u) | (ez < 0 ? 32u : 0u);
+  return (w & m) != 0u;
+}
+
+// Population planes of the source and destination buffers.
+template <class T>
+struct Planes {
+  const T* const* srcq;  // 27 source plane pointers
+  T* const* dstq;        // 27 destination plane pointers
+  __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(srcq[q] + idx); }
+  __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dstq[q][idx] = v; }
+};
+
+template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG, class P>
+__device__ __forceinline__ void load_cell(const StepArgs& a, const P& pl, const int i, const int j, const int k,
+                                          typename StoreT<S>::R (&f)[Q], double (&drag)[3]) {
+  using R = typename StoreT<S>::R;
+  const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + i;
+  if constexpr (B == Bc::Ghost) {
+    // reference boundaries: the ghost slots the pull reaches were filled by
+    // the ghost-slot gather after the previous step
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = decode<S>(pl.load(q, b + a.rel[q]), q, a.enc);
+    });
+  } else if constexpr (B == Bc::Periodic) {
+    const int im = i == 0 ? a.nx - 1 : i - 1, ip = i == a.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? a.ny - 1 : j - 1, jp = j == a.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1, kp = k == a.nz - 1 ? 0 : k + 1;
+    const int32_t rz[3] = {a.base32 + km * a.sz32, a.base32 + k * a.sz32, a.base32 + kp * a.sz32};
+    const int32_t ry[3] = {jm * a.pitch32, j * a.pitch32, jp * a.pitch32};
+    const int32_t cx[3] = {im, i, ip};
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const int32_t s = rz[1 - D3Q27::ez[q]] + ry[1 - D3Q27::ey[q]] + cx[1 - D3Q27::ex[q]];
+      f[q] = decode<S>(pl.load(q, s), q, a.enc);
+    });
+  } else if constexpr (RULE == CaseRule::CavityStd) {
+    // halfway bounce-back on the six walls: a link leaving the box returns
+    // the cell's own opposite population; through the lid (z+) it gains
+    // -2 w rho_w (c_bb . u_w)/cs^2 = 6 w rho_w e_q.u_w
+    const unsigned wf = wall_flags(a, i, j, k);
+    const bool lid = (wf & 32u) != 0u;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q];
+      constexpr int exq = D3Q27::ex[q];
+      constexpr int cls = D3Q27::wclass[q];
+      const bool out = leaves<q>(wf);
+      // q and bb(q) share the weight class, hence the storage scale
+      R val = decode<S>(out ? pl.load(qb, b) : pl.load(q, b + a.rel[q]), q, a.enc);
+      if constexpr (exq != 0 && D3Q27::ez[q] < 0) {
+        // ((6 rho_w u_w) w_q) e_q rounded on its own, then added (EXACT keeps
+        // the multiply and the add apart, as the specification does)
+        using A = Ar<R, EXACT>;
+        if (lid) val = A::add(val, A::mul(A::mul(R(6.0 * a.rho_w * a.lid_u), wgt<R>(cls)), R(exq)));
+      }
+      f[q] = val;
+    });
+  } else {
+    static_assert(RULE == CaseRule::SphereStd, "standard rule");
+    // channel periodic in y and z; x-: equilibrium inlet; x+: zero-gradient
+    // outlet (the link re-enters from the cell's own column); solid links
+    // (bit q of the cell's link mask) bounce back
+    const int jm = j == 0 ? a.ny - 1 : j - 1, jp = j == a.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? a.nz - 1 : k - 1, kp = k == a.nz - 1 ? 0 : k + 1;
+    const int32_t rz[3] = {a.base32 + km * a.sz32, a.base32 + k * a.sz32, a.base32 + kp * a.sz32};
+    const int32_t ry[3] = {jm * a.pitch32, j * a.pitch32, jp * a.pitch32};
+    const bool inlet = i == 0, outlet = i == a.nx - 1;
+    const int32_t cx[3] = {i - 1, i, outlet ? i : i + 1};
+    const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+    const bool near = k >= a.near_lo[2] && k <= a.near_hi[2] && j >= a.near_lo[1] && j <= a.near_hi[1] &&
+                      i >= a.near_lo[0] && i <= a.near_hi[0];
+    const uint32_t links = near ? a.links[cell] : 0u;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q];
+      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+      [[maybe_unused]] constexpr int cls = D3Q27::wclass[q];
+      const bool solid = (links >> q) & 1u;
+      const int32_t s_pull = rz[1 - ez] + ry[1 - ey] + cx[1 - ex];
+      R val = decode<S>(solid ? pl.load(qb, b) : pl.load(q, s_pull), q, a.enc);
+      if constexpr (ex > 0) {
+        if (inlet) val = R(a.feq_in[q]);
+      }
+      if constexpr (DRAG) {
+        if (solid) {
+          const double fd = static_cast<double>(val) + (S == Store::F64 ? 0.0 : 3.0 * wgt<double>(cls) * a.p_shift);
+          if constexpr (ex != 0) drag[0] -= 2.0 * fd * ex;
+          if constexpr (ey != 0) drag[1] -= 2.0 * fd * ey;
+          if constexpr (ez != 0) drag[2] -= 2.0 * fd * ez;
+        }
+      }
+      f[q] = val;
+    });
+  }
+}
+
+// Moment rules of the reference cases, applied to one cell's moments.
+template <CaseRule RULE, class R>
+__device__ __forceinline__ void case_rules(const StepArgs& a, const int i, const int k, const int64_t cell, R& u,
+                                           R& v, R& w, R& p) {
+  if constexpr (RULE == CaseRule::CavityRef) {
+    // lid_driven_cavity/src/lbm.cpp:343-344: ua forced on the top plane
+    if (k == a.nz - 1) u = R(a.lid_u);
+  } else if constexpr (RULE == CaseRule::SphereRef) {
+    // sphere/src/lbm.cpp:399-412: moments times the mask, then the inlet
+    // velocity on the first plane and zero pressure on the last
+    if (!a.usr[cell]) {
+      u = R(0);
+      v = R(0);
+      w = R(0);
+      p = R(-a.p_shift);
+    }
+    if (i == 0) {
+      u = R(a.inlet[k]);
+      v = R(0);
+      w = R(0);
+    }
+    if (i == a.nx - 1) p = R(-a.p_shift);
+  }
+}
+
+template <Store S, CaseRule RULE, bool EXACT, class P>
+__device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, const int i, const int j, const int k,
+                                             typename StoreT<S>::R (&f)[Q]) {
+  using R = typename StoreT<S>::R;
+  const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + i;
+  const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+
+  R u, v, w, p;
+  moments<R, EXACT>(f, u, v, w, p);
+  case_rules<RULE>(a, i, k, cell, u, v, w, p);
+
+  if (a.store) {
+    a.mu[cell] = u;
+    a.mv[cell] = v;
+    a.mw[cell] = w;
+    a.mp[cell] = static_cast<double>(p) + a.p_shift;
+  }
+
+  R tp3[4], udu15;
+  feq_prep<R, EXACT>(u, v, w, p, tp3, udu15);
+  using A = Ar<R, EXACT>;
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+    R fs;
+    if constexpr (EXACT) {
+      fs = A::sub(f[q], div_rn(A::sub(f[q], feq), a.tau_half, a.omega));
+    } else {
+      fs = f[q] - R(a.omega) * (f[q] - feq);
+    }
+    pl.store(q, b, encode<S>(fs, q, a.enc));
+  });
+}
+
+// Two cells at once in FP32 with Blackwell's paired FP32 instructions
+// (__fadd2_rn, __fmul2_rn, __ffma2_rn): every operation of the collision
+// acts on the same quantity of both cells, so the pair costs about the
+// instructions of one.  Same arithmetic as compute_cell's FP32 path.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+template <int q>
+__device__ __forceinline__ float2 edu2(float2 u, float2 v, float2 w) {
+  constexpr int a = D3Q27::ex[q], b = D3Q27::ey[q], c = D3Q27::ez[q];
+  float2 t = f2s(0.f);
+  bool have = false;
+  if constexpr (a != 0) {
+    t = a > 0 ? u : f2(-u.x, -u.y);
+    have = true;
+  }
+  if constexpr (b != 0) {
+    if (have)
+      t = b > 0 ? __fadd2_rn(t, v) : __fadd2_rn(t, f2(-v.x, -v.y));
+    else
+      t = b > 0 ? v : f2(-v.x, -v.y);
+    have = true;
+  }
+  if constexpr (c != 0) {
+    if (have)
+      t = c > 0 ? __fadd2_rn(t, w) : __fadd2_rn(t, f2(-w.x, -w.y));
+    else
+      t = c > 0 ? w : f2(-w.x, -w.y);
+  }
+  return t;
+}
+
+template <Store S, CaseRule RULE, class P>
+__device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, const int i, const int j, const int k,
+                                             float (&f0)[Q], float (&f1)[Q]) {
+  // cells (i, j, k) and (i, j + 1, k)
+  const int32_t b0 = a.base32 + k * a.sz32 + j * a.pitch32 + i;
+  const int32_t b1 = b0 + a.pitch32;
+  const int64_t c0 = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+  const int64_t c1 = c0 + a.nx;
+  float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const float2 x = f2(f0[q], f1[q]);
+    s = __fadd2_rn(s, x);
+    if constexpr (D3Q27::ex[q] == 1) u = __fadd2_rn(u, x);
+    if constexpr (D3Q27::ex[q] == -1) u = __fadd2_rn(u, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ey[q] == 1) v = __fadd2_rn(v, x);
+    if constexpr (D3Q27::ey[q] == -1) v = __fadd2_rn(v, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ez[q] == 1) w = __fadd2_rn(w, x);
+    if constexpr (D3Q27::ez[q] == -1) w = __fadd2_rn(w, f2(-x.x, -x.y));
+  });
+  float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
+  case_rules<RULE>(a, i, k, c0, u.x, v.x, w.x, p.x);
+  case_rules<RULE>(a, i, k, c1, u.y, v.y, w.y, p.y);
+  if (a.store) {
+    a.mu[c0] = u.x;
+    a.mv[c0] = v.x;
+    a.mw[c0] = w.x;
+    a.mp[c0] = static_cast<double>(p.x) + a.p_shift;
+    a.mu[c1] = u.y;
+    a.mv[c1] = v.y;
+    a.mw[c1] = w.y;
+    a.mp[c1] = static_cast<double>(p.y) + a.p_shift;
+  }
+  const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+  float2 tp3[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tp3[c] = __fmul2_rn(p, f2s(3.0f * wgt<float>(c)));
+  const float2 om = f2s(-static_cast<float>(a.omega));
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    constexpr int cls = D3Q27::wclass[q];
+    const float2 e = edu2<q>(u, v, w);
+    // t (3e + 4.5 e^2 - 1.5 u.u) + 3 t p, with e (3 + 4.5 e) for the bracket
+    const float2 br = __fadd2_rn(__fmul2_rn(e, __ffma2_rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
+    const float2 feq = __ffma2_rn(f2s(wgt<float>(cls)), br, tp3[cls]);
+    const float2 x = f2(f0[q], f1[q]);
+    const float2 fs = __ffma2_rn(om, __fadd2_rn(x, f2(-feq.x, -feq.y)), x);
+    pl.store(q, b0, encode<S>(fs.x, q, a.enc));
+    pl.store(q, b1, encode<S>(fs.y, q, a.enc));
+  });
+}
+
+template <Store S> struct CellsPerThread { static constexpr int value = 1; };
+template <> struct CellsPerThread<Store::F32> { static constexpr int value = 2; };
+template <> struct CellsPerThread<Store::F16> { static constexpr int value = 2; };
+template <> struct CellsPerThread<Store::BF16> { static constexpr int value = 2; };
+
+// The step of the CPT cells (i, j0 .. j0 + CPT - 1, k) a thread owns.
+// Returns nothing; writes the next buffer and, with a.store, the moments.
+template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG, class P>
+__device__ __forceinline__ void step_cells(const StepArgs& a, const P& pl, const int i, const int j0, const int k,
+                                           double (&drag)[3]) {
+  using R = typename StoreT<S>::R;
+  constexpr int CPT = CellsPerThread<S>::value;
+  R f[CPT][Q];
+  bool act[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int j = j0 + c;
+    act[c] = i < a.nx && j < a.ny;
+    if constexpr (RULE == CaseRule::SphereStd) {
+      // solid cells are not updated; they report zero moments
+      if (act[c]) {
+        const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+        if (!a.usr[cell]) {
+          if (a.store) {
+            a.mu[cell] = 0;
+            a.mv[cell] = 0;
+            a.mw[cell] = 0;
+            a.mp[cell] = a.p_shift;
+          }
+          act[c] = false;
+        }
+      }
+    }
+    if (act[c]) load_cell<S, B, RULE, EXACT, DRAG>(a, pl, i, j, k, f[c], drag);
+  }
+  if constexpr (CPT == 2 && !std::is_same<R, double>::value) {
+    if (act[0] && act[1]) {
+      compute_pair<S, RULE>(a, pl, i, j0, k, f[0], f[1]);
+      return;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < CPT; ++c)
+    if (act[c]) compute_cell<S, RULE, EXACT>(a, pl, i, j0 + c, k, f[c]);
+}
+
+}  // namespace core
+}  // namespace imx

@@ -203,6 +203,55 @@ void imexlb_destroy(imexlb_lattice* h);
 /* Message of the calling thread's last failure ("" if none). */
 const char* imexlb_last_error(void);
 
+/* ------------------------------------------------------------ engine
+ * Many independent lattices ("instances") on one GPU, every active one
+ * advanced one time step per persistent kernel launch over a device-side
+ * (instance, tile) work list; the steps run as CUDA-graph replays while the
+ * set of instances is unchanged.  Instances live in one device arena
+ * reserved at creation (budget_bytes); an instance that does not fit is
+ * refused with IMEXLB_E_NOMEM, so a server admits work against an HBM
+ * budget.  Instances can be added and removed between any two steps.
+ * Supported instance kinds: TGV (periodic), lid-driven cavity and sphere
+ * channel with standard boundaries (IMEXLB_BC_STANDARD semantics), in the
+ * engine's storage format.  No counterpart in the reference, which runs one
+ * lattice per process (BASELINE batched and served configurations). */
+typedef struct imexlb_engine imexlb_engine;
+
+typedef struct imexlb_instance_desc {
+  imexlb_case kase;
+  int nx, ny, nz;
+  double tau0, rho0, u0;  /* as imexlb_params */
+  double lid_u, inlet_u, sphere_d, sphere_c[3];  /* 0 = defaults (u0, u0, nx/24, (nx/4, ny/2, nz/2)) */
+  int tile_bx; /* threads along x per tile (power of two, 8..256); 0 = default */
+} imexlb_instance_desc;
+
+typedef struct imexlb_engine_stats {
+  int instances;
+  int64_t cells;
+  size_t budget_bytes, used_bytes;
+  int64_t tiles, steps;
+} imexlb_engine_stats;
+
+int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budget_bytes, int max_instances,
+                         void* stream, imexlb_engine** out);
+/* Add an instance (initial state as imexlb_create); *slot identifies it. */
+int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot);
+int imexlb_engine_remove(imexlb_engine* e, int slot);
+/* Every active instance advances nsteps steps; the moments of the last are stored. */
+int imexlb_engine_step(imexlb_engine* e, int nsteps);
+/* u, v, w, p of one instance after the last step (host arrays, x fastest). */
+int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, double* w, double* p);
+/* Velocity residual per slot, sqrt(sum|u - u_prev|^2 / sum|u|^2) between this
+ * call and the previous one (INFINITY on an instance's first call, NaN for
+ * empty slots or a non-finite lattice); out has max_instances entries.  Call
+ * it right after imexlb_engine_step. */
+int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out);
+int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st);
+/* Arena bytes one instance needs in a given storage format. */
+int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes);
+int imexlb_engine_synchronize(imexlb_engine* e);
+void imexlb_engine_destroy(imexlb_engine* e);
+
 /* Library version string. */
 const char* imexlb_version(void);
 

@@ -68,6 +68,9 @@ def oracle_lib():
         lib.oracle_threads.restype = ctypes.c_int
         lib.oracle_check_div3.argtypes = [ctypes.c_long, ctypes.c_ulonglong, ctypes.c_int]
         lib.oracle_check_div3.restype = ctypes.c_int
+        lib.oracle_check_div.argtypes = [ctypes.c_long, ctypes.c_ulonglong, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_long)]
+        lib.oracle_check_div.restype = ctypes.c_int
         lib.oracle_std_create.restype = ctypes.c_void_p
         lib.oracle_std_create.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 9
         lib.oracle_std_destroy.argtypes = [ctypes.c_void_p]

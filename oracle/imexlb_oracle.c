@@ -800,3 +800,69 @@ int oracle_check_div3(long n, unsigned long long seed, int planted) {
   }
   return bad;
 }
+
+/* Check of the EXACT mode's collision division (kernels' div_rn): x/d by
+ * Markstein's correction with an exactness test and IEEE division for the
+ * cases the test rejects.  n random x (random signs, exponents within 2^+-60,
+ * random significands) against random divisors d in [0.5, 4) (a fresh d every
+ * 1024 samples; every 997th x is zero and every 1009th tiny, which the
+ * exactness test rejects on purpose).  Returns the number of quotients that
+ * differ from x / d; *fallbacks counts the rejected cases.  planted = 1
+ * returns the uncorrected q0 = RN(x RN(1/d)) (a known-wrong variant). */
+int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbacks) {
+  unsigned long long s = seed ? seed : 0x9E3779B97F4A7C15ULL;
+  int bad = 0;
+  long fb = 0;
+  double d = 1.0, z = 1.0;
+  for (long t = 0; t < n; ++t) {
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    union {
+      unsigned long long u;
+      double v;
+    } cv;
+    if ((t & 1023) == 0) {
+      cv.u = (1023ULL << 52) | (s & 0xFFFFFFFFFFFFFULL);
+      d = cv.v * (double)(1u << ((s >> 60) & 1)) * 0.5 * (((s >> 61) & 1) ? 4.0 : 1.0);
+      if (d >= 4.0) d *= 0.5;
+      z = 1.0 / d;
+      s ^= s << 13;
+      s ^= s >> 7;
+      s ^= s << 17;
+    }
+    const long e = (t % 1009 == 0) ? -1000 : (long)((s >> 52) % 121) - 60;
+    cv.u = ((s >> 63) << 63) | ((unsigned long long)(1023 + e) << 52) | (s & 0xFFFFFFFFFFFFFULL);
+    const double x = (t % 997 == 0) ? 0.0 : cv.v;
+    const double q0 = x * z;
+    const double r0 = fma(-q0, d, x);
+    const double q1 = fma(r0, z, q0);
+    const double r1 = fma(-q1, d, x);
+    union {
+      double v;
+      unsigned long long u;
+    } qb = {q1};
+    const int ef = (int)((qb.u >> 52) & 0x7ff);
+    const int he = ef - 53 - ((qb.u & 0xFFFFFFFFFFFFFULL) == 0 ? 1 : 0);
+    double q;
+    int accept = 0;
+    if (he > 0) {
+      union {
+        unsigned long long u;
+        double v;
+      } hg = {(unsigned long long)he << 52};
+      accept = fabs(r1) < d * hg.v;
+    }
+    if (planted) {
+      q = q0;
+    } else if (accept) {
+      q = q1;
+    } else {
+      q = x / d;
+      ++fb;
+    }
+    if (q != x / d) ++bad;
+  }
+  if (fallbacks) *fallbacks = fb;
+  return bad;
+}

@@ -60,6 +60,10 @@ int oracle_write_tecplot(const oracle_lbm* o, const char* path, int n);
  * random doubles (test of the EXACT-mode moment arithmetic). */
 int oracle_check_div3(long n, unsigned long long seed, int planted);
 
+/* Mismatches of the device's checked Markstein division x/d against IEEE
+ * division over n random (x, d), d in [0.5, 4); *fallbacks = rejected cases. */
+int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbacks);
+
 /* Number of OpenMP threads the oracle will use (for the CPU baseline). */
 int oracle_threads(void);
 

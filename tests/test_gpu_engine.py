@@ -1,0 +1,100 @@
+"""GPU checks of the engine (many lattices advanced by one persistent launch).
+
+Each instance's result must be identical to the same lattice run alone
+through the single-lattice API: same per-cell code, same arithmetic, so the
+fields are compared bit for bit.  That holds while other instances share
+the launches, join part-way (at either step parity) and leave; this is the
+"same result alone and in the mix" property the serving loop relies on.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    from imexlb_b200 import api as a
+
+    return a
+
+
+MIX = [
+    ("tgv", (24, 24, 24), 0.02, 0.05, {}),
+    ("cavity", (32, 20, 28), 0.03, 0.1, dict(lid_u=0.1)),
+    ("sphere", (48, 16, 16), 0.015, 0.05, dict(inlet_u=0.05, sphere_d=6.0, sphere_c=(12.0, 8.0, 8.0))),
+    ("cavity", (17, 9, 11), 0.05, 0.1, dict(lid_u=0.08)),
+    ("tgv", (40, 16, 20), 0.01, 0.05, {}),
+]
+
+
+def alone(api, case, n, tau, u0, kw, steps, storage, arith):
+    bc = "reference" if case == "tgv" else "standard"
+    with api.LBM(case, *n, tau, 1.0, u0, bc=bc, storage=storage, arith=arith, **kw) as lbm:
+        if steps:
+            lbm.step(steps)
+        return lbm.fields()
+
+
+@pytest.mark.parametrize("storage,arith", [("f64", "exact"), ("f64", "fast"), ("f16", "fast"), ("f32", "fast")])
+def test_instances_match_single_lattices(api, storage, arith):
+    steps_a, steps_b = 23, 18
+    with api.Engine(storage=storage, arith=arith, budget_bytes=1 << 30, max_instances=16) as eng:
+        slots = [eng.add(api.instance_desc(c, *n, tau, 1.0, u0, **kw)) for c, n, tau, u0, kw in MIX[:3]]
+        eng.step(steps_a)  # odd: the late instances join at the other parity
+        late = [eng.add(api.instance_desc(c, *n, tau, 1.0, u0, **kw)) for c, n, tau, u0, kw in MIX[3:]]
+        eng.step(steps_b)
+        got = {s: eng.fields(s) for s in slots + late}
+        eng.remove(slots[1])  # the cavity leaves; the others carry on
+        eng.step(5)
+        got_after = {s: eng.fields(s) for s in (slots[0], late[0])}
+    for (c, n, tau, u0, kw), s in zip(MIX[:3], slots):
+        want = alone(api, c, n, tau, u0, kw, steps_a + steps_b, storage, arith)
+        for k in "uvwp":
+            assert np.array_equal(got[s][k], want[k]), (c, k, np.abs(got[s][k] - want[k]).max())
+    for (c, n, tau, u0, kw), s in zip(MIX[3:], late):
+        want = alone(api, c, n, tau, u0, kw, steps_b, storage, arith)
+        for k in "uvwp":
+            assert np.array_equal(got[s][k], want[k]), (c, k)
+    c, n, tau, u0, kw = MIX[0]
+    want = alone(api, c, n, tau, u0, kw, steps_a + steps_b + 5, storage, arith)
+    assert np.array_equal(got_after[slots[0]]["u"], want["u"])
+    c, n, tau, u0, kw = MIX[3]
+    want = alone(api, c, n, tau, u0, kw, steps_b + 5, storage, arith)
+    assert np.array_equal(got_after[late[0]]["u"], want["u"])
+
+
+def test_tile_widths_do_not_change_results(api):
+    outs = []
+    for bx in (8, 16, 32, 64, 128):
+        with api.Engine(storage="f16", budget_bytes=1 << 28, max_instances=2) as eng:
+            s = eng.add(api.instance_desc("cavity", 40, 24, 20, 0.03, 1.0, 0.1, lid_u=0.1, tile_bx=bx))
+            eng.step(30)
+            outs.append(eng.fields(s))
+    for o in outs[1:]:
+        for k in "uvwp":
+            assert np.array_equal(o[k], outs[0][k])
+
+
+def test_budget_admission_and_residuals(api):
+    d = api.instance_desc("cavity", 32, 32, 32, 0.03, 1.0, 0.1, lid_u=0.1)
+    need = api.instance_bytes("f16", d)
+    with api.Engine(storage="f16", budget_bytes=2 * need + need // 2, max_instances=8) as eng:
+        a = eng.add(d)
+        b = eng.add(d)
+        assert eng.try_add(d) is None  # over budget
+        eng.remove(a)
+        c = eng.add(d)  # fits again after a removal
+        eng.step(50)
+        r1 = eng.residuals()
+        assert np.isinf(r1[b]) and np.isinf(r1[c])
+        eng.step(50)
+        r2 = eng.residuals()
+        assert 0.0 < r2[b] < 1.0 and 0.0 < r2[c] < 1.0
+        assert np.isnan(r2[a]) or a == c
+        st = eng.stats()
+        assert st["instances"] == 2 and st["used_bytes"] <= st["budget_bytes"]
