@@ -46,7 +46,7 @@ struct __align__(16) EngInst {
   int rule;      // CaseRule
   int bx_log2;   // tile width 2^bx_log2 threads along x
   int parity0;   // engine step parity at admission
-  int pad;
+  int x2;        // 2-byte format with nx even: threads own x-pairs (step_cells_x2)
 };
 
 struct Tile {
@@ -70,15 +70,31 @@ struct FlatPlanes {
   int32_t sq;
   __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(src + (q * sq + idx)); }
   __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dst[q * sq + idx] = v; }
+  __device__ __forceinline__ uint32_t load_pair(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const unsigned int*>(src + (q * sq + idx)));
+  }
+  __device__ __forceinline__ uint32_t load_half(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const unsigned short*>(src + (q * sq + idx)));
+  }
+  __device__ __forceinline__ void store_pair(int q, int32_t idx, uint32_t v) const {
+    *reinterpret_cast<unsigned int*>(dst + (q * sq + idx)) = v;
+  }
+  __device__ __forceinline__ void store_half(int q, int32_t idx, uint16_t v) const {
+    *reinterpret_cast<unsigned short*>(dst + (q * sq + idx)) = v;
+  }
 };
 
-template <Store S, bool EXACT>
-__global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea) {
+// The persistent step over one group of tiles: every instance in a group
+// shares the boundary rule (and, for 2-byte formats, the x-pair mapping), so
+// the per-cell code is inlined once, exactly as in the single-lattice
+// kernels.  Block b takes tiles t0 + b, t0 + b + grid, ... of [t0, t1).
+template <Store S, bool EXACT, Bc B, CaseRule RULE, bool X2>
+__global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, const int t0, const int t1) {
   using T = typename StoreT<S>::T;
   constexpr int CPT = CellsPerThread<S>::value;
   __shared__ EngInst sh;
   int loaded = -1;  // same tile sequence in every thread: a block-uniform value
-  for (int t = blockIdx.x; t < ea.ntiles; t += gridDim.x) {
+  for (int t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
     const Tile tile = ea.tiles[t];
     if (tile.slot != loaded) {
       __syncthreads();
@@ -95,18 +111,12 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea) {
                            static_cast<int32_t>(sh.a.sq)};
     const int bxl = sh.bx_log2;
     const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
-    const int i = tile.i0 + tx, j0 = tile.j0 + ty * CPT, k = tile.k;
     double drag[3] = {0.0, 0.0, 0.0};
-    switch (sh.rule) {
-      case static_cast<int>(CaseRule::None):
-        step_cells<S, Bc::Periodic, CaseRule::None, EXACT, false>(sh.a, pl, i, j0, k, drag);
-        break;
-      case static_cast<int>(CaseRule::CavityStd):
-        step_cells<S, Bc::Standard, CaseRule::CavityStd, EXACT, false>(sh.a, pl, i, j0, k, drag);
-        break;
-      default:
-        step_cells<S, Bc::Standard, CaseRule::SphereStd, EXACT, false>(sh.a, pl, i, j0, k, drag);
-        break;
+    if constexpr (X2) {
+      const int seg = (1 << bxl) < 32 ? (1 << bxl) : 32;
+      step_cells_x2<S, B, RULE, false>(sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k, tx % seg, seg, drag);
+    } else {
+      step_cells<S, B, RULE, EXACT, false>(sh.a, pl, tile.i0 + tx, tile.j0 + ty * CPT, tile.k, drag);
     }
   }
 }
@@ -122,14 +132,16 @@ __global__ void engine_resid_kernel(const EngArgs ea, double* part) {
     const EngInst& in = ea.inst[tile.slot];
     const int bxl = in.bx_log2;
     const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
-    const int i = tile.i0 + tx, k = tile.k;
+    const int cx = in.x2 ? 2 : 1;  // cells per thread along x
+    const int k = tile.k;
     const int nx = in.a.nx, ny = in.a.ny;
     const int64_t n = static_cast<int64_t>(nx) * ny * in.a.nz;
     double d2 = 0.0, n2 = 0.0;
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int j = tile.j0 + ty * CPT + c;
-      if (i < nx && j < ny) {
+    for (int c = 0; c < 2 * CPT; ++c) {
+      const int i = tile.i0 + cx * tx + (c & 1);
+      const int j = tile.j0 + ty * CPT + (c >> 1);
+      if ((c & 1) < cx && (c >> 1) < CPT && i < nx && j < ny) {
         const int64_t cell = i + static_cast<int64_t>(nx) * (j + static_cast<int64_t>(ny) * k);
         const double u = in.a.mu[cell], v = in.a.mv[cell], w = in.a.mw[cell];
         double* pu = in.prev + cell;
@@ -292,6 +304,10 @@ struct imexlb_engine {
   DevBuf<int> d_seg;  // begin[nseg], end[nseg]
   DevBuf<double> d_res;
   std::vector<int> seg_slots;
+  // tile ranges of the kernel groups: group = rule (0 periodic, 1 cavity,
+  // 2 sphere) * 2 + x2
+  int group_begin[6] = {0, 0, 0, 0, 0, 0};
+  int group_end[6] = {0, 0, 0, 0, 0, 0};
   bool dirty = true;
   int64_t gstep = 0;
   int grid = 296;
@@ -323,18 +339,39 @@ int rebuild_tiles(imexlb_engine* e) {
   e->seg_slots.clear();
   std::vector<int> sb, se;
   const int cpt = cpt_of(e->storage);
-  for (int s = 0; s < static_cast<int>(e->slots.size()); ++s) {
+  // instances ordered by kernel group, so that each group's tiles are one range
+  std::vector<int> order;
+  for (int g = 0; g < 6; ++g) {
+    for (int s = 0; s < static_cast<int>(e->slots.size()); ++s) {
+      const Slot& sl = e->slots[s];
+      if (!sl.used) continue;
+      const int rule = e->h_inst[s].rule;
+      const int rg = rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2);
+      if (rg * 2 + e->h_inst[s].x2 == g) order.push_back(s);
+    }
+  }
+  for (int g = 0; g < 6; ++g) e->group_begin[g] = e->group_end[g] = 0;
+  int prev_group = -1;
+  for (int s : order) {
     Slot& sl = e->slots[s];
-    if (!sl.used) continue;
+    const int rule = e->h_inst[s].rule;
+    const int g = (rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2)) * 2 +
+                  e->h_inst[s].x2;
+    if (g != prev_group) {
+      e->group_begin[g] = static_cast<int>(e->h_tiles.size());
+      prev_group = g;
+    }
     sl.seg = static_cast<int>(e->seg_slots.size());
     e->seg_slots.push_back(s);
     sb.push_back(static_cast<int>(e->h_tiles.size()));
     const int bx = 1 << sl.bx_log2;
     const int rows = (256 / bx) * cpt;
+    const int cols = bx * (e->h_inst[s].x2 ? 2 : 1);
     for (int k = 0; k < sl.L.nz; ++k)
       for (int j0 = 0; j0 < sl.L.ny; j0 += rows)
-        for (int i0 = 0; i0 < sl.L.nx; i0 += bx) e->h_tiles.push_back(Tile{s, i0, j0, k});
+        for (int i0 = 0; i0 < sl.L.nx; i0 += cols) e->h_tiles.push_back(Tile{s, i0, j0, k});
     se.push_back(static_cast<int>(e->h_tiles.size()));
+    e->group_end[g] = static_cast<int>(e->h_tiles.size());
   }
   const size_t nt = e->h_tiles.size();
   if (nt) {
@@ -360,22 +397,45 @@ int rebuild_tiles(imexlb_engine* e) {
   return IMEXLB_OK;
 }
 
+template <Store S, bool EXACT>
+cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
+  for (int g = 0; g < 6; ++g) {
+    const int t0 = e->group_begin[g], t1 = e->group_end[g];
+    if (t1 <= t0) continue;
+    const int grid = std::min(e->grid, t1 - t0);
+    const int rule = g / 2;
+    const bool x2 = (g & 1) != 0;
+    if constexpr (S == Store::F16 || S == Store::BF16) {
+      if (x2) {
+        if (rule == 0)
+          engine_step_kernel<S, false, Bc::Periodic, CaseRule::None, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+        else if (rule == 1)
+          engine_step_kernel<S, false, Bc::Standard, CaseRule::CavityStd, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+        else
+          engine_step_kernel<S, false, Bc::Standard, CaseRule::SphereStd, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+        continue;
+      }
+    }
+    if (rule == 0)
+      engine_step_kernel<S, EXACT, Bc::Periodic, CaseRule::None, false><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+    else if (rule == 1)
+      engine_step_kernel<S, EXACT, Bc::Standard, CaseRule::CavityStd, false><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+    else
+      engine_step_kernel<S, EXACT, Bc::Standard, CaseRule::SphereStd, false><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
   EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), parity, store};
   if (ea.ntiles == 0) return cudaSuccess;
-  const int grid = std::min(e->grid, ea.ntiles);
   switch (e->storage) {
-    case IMEXLB_F64:
-      if (e->exact)
-        engine_step_kernel<Store::F64, true><<<grid, 256, 0, e->stream>>>(ea);
-      else
-        engine_step_kernel<Store::F64, false><<<grid, 256, 0, e->stream>>>(ea);
-      break;
-    case IMEXLB_F32: engine_step_kernel<Store::F32, false><<<grid, 256, 0, e->stream>>>(ea); break;
-    case IMEXLB_F16: engine_step_kernel<Store::F16, false><<<grid, 256, 0, e->stream>>>(ea); break;
-    case IMEXLB_BF16: engine_step_kernel<Store::BF16, false><<<grid, 256, 0, e->stream>>>(ea); break;
+    case IMEXLB_F64: return e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
+    case IMEXLB_F32: return launch_groups<Store::F32, false>(e, ea);
+    case IMEXLB_F16: return launch_groups<Store::F16, false>(e, ea);
+    case IMEXLB_BF16: return launch_groups<Store::BF16, false>(e, ea);
   }
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -544,6 +604,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
   in.bx_log2 = sl.bx_log2;
   in.parity0 = static_cast<int>(e->gstep & 1);
+  in.x2 = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
                 e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));

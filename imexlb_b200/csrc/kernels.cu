@@ -94,6 +94,39 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
   }
 }
 
+// 2-byte formats with nx even: each thread owns an x-pair in two rows
+// (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
+template <Store S, Bc B, CaseRule RULE, bool DRAG>
+__global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
+  using T = typename StoreT<S>::T;
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
+  const int k = blockIdx.z;
+  const int seg = blockDim.x < 32 ? blockDim.x : 32;
+  double drag[3] = {0.0, 0.0, 0.0};
+  const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
+  step_cells_x2<S, B, RULE, DRAG>(a, pl, x0, j0, k, static_cast<int>(threadIdx.x) % seg, seg, drag);
+  if constexpr (DRAG) {
+    __shared__ double sh[3][8];
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double x = drag[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[c][warp] = x;
+    }
+    __syncthreads();
+    if (t < 3) {
+      double x = 0.0;
+      for (int w = 0; w < 8; ++w) x += sh[t][w];
+      const int64_t blk = blockIdx.x + static_cast<int64_t>(gridDim.x) * (blockIdx.y + static_cast<int64_t>(gridDim.y) * blockIdx.z);
+      a.drag_part[3 * blk + t] = x;
+    }
+  }
+}
+
 // Sum the per-block drag partials (3 components, fixed order).
 __global__ void drag_sum_kernel(const double* part, int64_t nblk, double* out) {
   const int c = blockIdx.x;  // component
@@ -218,10 +251,23 @@ dim3 step_block(int nx) {
   return dim3(32, 8, 1);
 }
 
+// 2-byte x-pair kernel: threads along x cover two cells each
+static dim3 step_block_x2(int nx) {
+  if (nx >= 128) return dim3(64, 4, 1);
+  if (nx >= 64) return dim3(32, 8, 1);
+  return dim3(16, 16, 1);
+}
+
+static bool use_x2(Store s, int nx) { return (s == Store::F16 || s == Store::BF16) && nx % 2 == 0; }
+
 // ------------------------------------------------------------ launchers
 int reduce_blocks() { return RED_BLOCKS; }
 
 int64_t step_grid_blocks(int nx, int ny, int nz, int storage) {
+  if (use_x2(static_cast<Store>(storage), nx)) {
+    const dim3 b = step_block_x2(nx);
+    return static_cast<int64_t>((nx + 2 * b.x - 1) / (2 * b.x)) * ((ny + 2 * b.y - 1) / (2 * b.y)) * nz;
+  }
   const dim3 b = step_block(nx);
   const int cpt = storage == static_cast<int>(Store::F64) ? 1 : CellsPerThread<Store::F16>::value;
   const int rows = b.y * cpt;
@@ -269,6 +315,20 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
 
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
+  if constexpr (S == Store::F16 || S == Store::BF16) {
+    if (use_x2(S, a.nx)) {
+      const dim3 block = step_block_x2(a.nx);
+      const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
+      if constexpr (R == CaseRule::SphereStd) {
+        if (a.drag_part) {
+          step_kernel_x2<S, B, R, true><<<grid, block, 0, s>>>(a);
+          return cudaGetLastError();
+        }
+      }
+      step_kernel_x2<S, B, R, false><<<grid, block, 0, s>>>(a);
+      return cudaGetLastError();
+    }
+  }
   const dim3 block = step_block(a.nx);
   const int rows = block.y * CellsPerThread<S>::value;
   const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);

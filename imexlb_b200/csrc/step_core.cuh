@@ -243,6 +243,19 @@ struct Planes {
   T* const* dstq;        // 27 destination plane pointers
   __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(srcq[q] + idx); }
   __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dstq[q][idx] = v; }
+  // 2-byte formats: an aligned pair (idx even) or one value, as raw bits
+  __device__ __forceinline__ uint32_t load_pair(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const unsigned int*>(srcq[q] + idx));
+  }
+  __device__ __forceinline__ uint32_t load_half(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const unsigned short*>(srcq[q] + idx));
+  }
+  __device__ __forceinline__ void store_pair(int q, int32_t idx, uint32_t v) const {
+    *reinterpret_cast<unsigned int*>(dstq[q] + idx) = v;
+  }
+  __device__ __forceinline__ void store_half(int q, int32_t idx, uint16_t v) const {
+    *reinterpret_cast<unsigned short*>(dstq[q] + idx) = v;
+  }
 };
 
 template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG, class P>
@@ -517,6 +530,243 @@ __device__ __forceinline__ void step_cells(const StepArgs& a, const P& pl, const
 #pragma unroll
   for (int c = 0; c < CPT; ++c)
     if (act[c]) compute_cell<S, RULE, EXACT>(a, pl, i, j0 + c, k, f[c]);
+}
+
+
+// ------------------------------------------------------------ 2-byte x-pairs
+// For the 2-byte formats a thread owns a 2 x 2 block of cells: the x-pair
+// (x0, x0 + 1), x0 even, in rows j0 and j0 + 1.  Every population moves as an
+// aligned 4-byte pair, which the paired FP32 instructions then process as one
+// float2, so a thread keeps 90 four-byte loads in flight (the 18 populations
+// with e_x != 0 take two pairs each, see below).  Needs nx even.
+
+template <Store S> struct Pack2;
+template <> struct Pack2<Store::F16> {
+  static __device__ __forceinline__ float2 to_f2(uint32_t b) {
+    __half2 h = *reinterpret_cast<__half2*>(&b);
+    return __half22float2(h);
+  }
+  static __device__ __forceinline__ uint32_t from_f2(float2 f) {
+    __half2 h = __float22half2_rn(f);
+    return *reinterpret_cast<uint32_t*>(&h);
+  }
+  static __device__ __forceinline__ uint16_t from_f(float f) { return __half_as_ushort(__float2half_rn(f)); }
+};
+template <> struct Pack2<Store::BF16> {
+  static __device__ __forceinline__ float2 to_f2(uint32_t b) {
+    __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&b);
+    return __bfloat1622float2(h);
+  }
+  static __device__ __forceinline__ uint32_t from_f2(float2 f) {
+    __nv_bfloat162 h = __float22bfloat162_rn(f);
+    return *reinterpret_cast<uint32_t*>(&h);
+  }
+  static __device__ __forceinline__ uint16_t from_f(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
+};
+
+// pair (lo = cell x0, hi = cell x0 + 1) from two 16-bit halves
+__device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { return (lo16 & 0xffffu) | (hi16 << 16); }
+
+template <Store S, Bc B, CaseRule RULE, bool DRAG, class P>
+__device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, const int x0, const int j0, const int k,
+                                              const int seg_lane, const int seg, double (&drag)[3]) {
+  constexpr int RY = 2;
+  const bool xin = x0 < a.nx;  // nx even: both cells of the pair or neither
+  const int xs = xin ? x0 : a.nx - 2;
+  (void)seg_lane;
+  (void)seg;
+  const bool left_edge = xs == 0, right_edge = xs + 2 >= a.nx;
+  uint32_t raw[RY][Q];
+  int32_t rowb[RY][3][3];  // [r][1 - ez][1 - ey]: index of x = xs in the source row
+  bool act[RY];
+  uint32_t row_out_bits[RY];  // cavity: bit (3 dz + dy) = source row outside the box
+  uint32_t lid_mask = 0;      // cavity: rows whose cells sit under the lid
+  uint32_t solid0[RY], solid1[RY];  // sphere: per-cell solid-link bits
+  int32_t bself[RY];
+
+  // Every population of both rows arrives as aligned 4-byte pairs issued
+  // back to back.  A population with e_x = +1 needs (x0 - 1, x0): the high
+  // half of the pair at x0 - 2 and the low half of the pair at x0; e_x = -1
+  // needs (x0 + 1, x0 + 2) from the pairs at x0 and x0 + 2.  The second pair
+  // is the neighbouring thread's own pair, so it shares the warp's cache
+  // lines.  At the ends of a row the second pair's address carries the x
+  // rule: the periodic image, or any in-range pair whose value a wall or the
+  // inlet then replaces.
+#pragma unroll
+  for (int r = 0; r < RY; ++r) {
+    const int j = j0 + r;
+    act[r] = xin && j < a.ny;
+    const int js = j < a.ny ? j : a.ny - 1;
+    const int32_t b = a.base32 + k * a.sz32 + js * a.pitch32 + xs;  // own pair, aligned
+    bself[r] = b;
+    row_out_bits[r] = 0;
+    if constexpr (B == Bc::Ghost) {
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) rowb[r][dz][dy] = b - (1 - dz) * a.sz32 - (1 - dy) * a.pitch32;
+    } else {
+      const bool wrap = B == Bc::Periodic || RULE == CaseRule::SphereStd;
+      const int jj[3] = {js == 0 ? (wrap ? a.ny - 1 : -1) : js - 1, js, js == a.ny - 1 ? (wrap ? 0 : a.ny) : js + 1};
+      const int kk[3] = {k == 0 ? (wrap ? a.nz - 1 : -1) : k - 1, k, k == a.nz - 1 ? (wrap ? 0 : a.nz) : k + 1};
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+          const bool out = jj[dy] < 0 || jj[dy] >= a.ny || kk[dz] < 0 || kk[dz] >= a.nz;
+          if (out) row_out_bits[r] |= 1u << (3 * dz + dy);
+          rowb[r][dz][dy] = out ? b : a.base32 + kk[dz] * a.sz32 + jj[dy] * a.pitch32 + xs;
+        }
+    }
+    uint32_t links0 = 0, links1 = 0;
+    if constexpr (RULE == CaseRule::SphereStd) {
+      const bool near = act[r] && k >= a.near_lo[2] && k <= a.near_hi[2] && js >= a.near_lo[1] &&
+                        js <= a.near_hi[1] && xs + 1 >= a.near_lo[0] && xs <= a.near_hi[0];
+      const int64_t cell = xs + static_cast<int64_t>(a.nx) * (js + static_cast<int64_t>(a.ny) * k);
+      links0 = near ? a.links[cell] : 0u;
+      links1 = near ? a.links[cell + 1] : 0u;
+    }
+    solid0[r] = links0;
+    solid1[r] = links1;
+    if constexpr (RULE == CaseRule::CavityStd) {
+      if (k == a.nz - 1) lid_mask |= 1u << r;
+    }
+    // offset of the neighbouring pair on each side, x rule included
+    int32_t dleft, dright;
+    if constexpr (B == Bc::Periodic) {
+      dleft = left_edge ? a.nx - 2 : -2;
+      dright = right_edge ? 2 - a.nx : 2;
+    } else if constexpr (B == Bc::Ghost) {
+      dleft = -2;
+      dright = 2;
+    } else {
+      dleft = left_edge ? 0 : -2;   // wall / inlet replace the value
+      dright = right_edge ? 0 : 2;  // wall replaces it; the outlet keeps the own column
+    }
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+      [[maybe_unused]] constexpr int qb = D3Q27::bb[q];
+      const int32_t srow = rowb[r][1 - ez][1 - ey];
+      const uint32_t pv = pl.load_pair(q, srow);
+      uint32_t v = pv;
+      if constexpr (ex == 1) {
+        const uint32_t lv = pl.load_pair(q, srow + dleft);
+        v = pair_of(lv >> 16, pv);
+      } else if constexpr (ex == -1) {
+        const uint32_t rv = pl.load_pair(q, srow + dright);
+        uint32_t rlo = rv & 0xffffu;
+        if constexpr (RULE == CaseRule::SphereStd) {
+          if (right_edge) rlo = pv >> 16;  // zero-gradient outlet: the own column
+        }
+        v = pair_of(pv >> 16, rlo);
+      }
+      if constexpr (RULE == CaseRule::CavityStd) {
+        // halfway bounce-back: a link leaving the box returns the cell's own
+        // opposite population
+        const bool out_row = (row_out_bits[r] >> (3 * (1 - ez) + (1 - ey))) & 1u;
+        const bool out0 = out_row || (ex == 1 && left_edge);
+        const bool out1 = out_row || (ex == -1 && right_edge);
+        if (out0 || out1) {
+          const uint32_t bbp = pl.load_pair(qb, b);
+          v = pair_of(out0 ? bbp : v, out1 ? (bbp >> 16) : (v >> 16));
+        }
+      } else if constexpr (RULE == CaseRule::SphereStd) {
+        const bool s0 = (links0 >> q) & 1u, s1 = (links1 >> q) & 1u;
+        if (s0 || s1) {
+          const uint32_t bbp = pl.load_pair(qb, b);
+          v = pair_of(s0 ? bbp : v, s1 ? (bbp >> 16) : (v >> 16));
+        }
+      }
+      raw[r][q] = v;
+    });
+  }
+
+#pragma unroll
+  for (int r = 0; r < RY; ++r) {
+    const int j = j0 + r;
+    float2 f[Q];
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int ex = D3Q27::ex[q];
+      [[maybe_unused]] constexpr int ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+      constexpr int cls = D3Q27::wclass[q];
+      float2 x = __fmul2_rn(Pack2<S>::to_f2(raw[r][q]), f2s(a.enc.inv_scale[q]));
+      if constexpr (RULE == CaseRule::CavityStd && ex != 0 && ez < 0) {
+        if ((lid_mask >> r) & 1u) {
+          const float t = static_cast<float>(6.0 * a.rho_w * a.lid_u) * wgt<float>(cls) * static_cast<float>(ex);
+          x = __fadd2_rn(x, f2s(t));
+        }
+      }
+      if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
+        if (left_edge) x.x = static_cast<float>(a.feq_in[q]);
+      }
+      if constexpr (DRAG && RULE == CaseRule::SphereStd) {
+        const bool s0 = (solid0[r] >> q) & 1u, s1 = (solid1[r] >> q) & 1u;
+        const double add = (s0 ? static_cast<double>(x.x) : 0.0) + (s1 ? static_cast<double>(x.y) : 0.0);
+        if (act[r] && (s0 || s1)) {
+          const double shift = 3.0 * wgt<double>(cls) * a.p_shift * ((s0 ? 1.0 : 0.0) + (s1 ? 1.0 : 0.0));
+          if constexpr (ex != 0) drag[0] -= 2.0 * (add + shift) * ex;
+          if constexpr (ey != 0) drag[1] -= 2.0 * (add + shift) * ey;
+          if constexpr (ez != 0) drag[2] -= 2.0 * (add + shift) * ez;
+        }
+      }
+      f[q] = x;
+    });
+    if (!act[r]) continue;
+    const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + x0;
+    const int64_t c0 = x0 + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+    bool live0 = true, live1 = true;
+    if constexpr (RULE == CaseRule::SphereStd) {
+      live0 = a.usr[c0] != 0;
+      live1 = a.usr[c0 + 1] != 0;
+    }
+    float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const float2 x = f[q];
+      s = __fadd2_rn(s, x);
+      if constexpr (D3Q27::ex[q] == 1) u = __fadd2_rn(u, x);
+      if constexpr (D3Q27::ex[q] == -1) u = __fadd2_rn(u, f2(-x.x, -x.y));
+      if constexpr (D3Q27::ey[q] == 1) v = __fadd2_rn(v, x);
+      if constexpr (D3Q27::ey[q] == -1) v = __fadd2_rn(v, f2(-x.x, -x.y));
+      if constexpr (D3Q27::ez[q] == 1) w = __fadd2_rn(w, x);
+      if constexpr (D3Q27::ez[q] == -1) w = __fadd2_rn(w, f2(-x.x, -x.y));
+    });
+    float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
+    case_rules<RULE>(a, x0, k, c0, u.x, v.x, w.x, p.x);
+    case_rules<RULE>(a, x0 + 1, k, c0 + 1, u.y, v.y, w.y, p.y);
+    if (a.store) {
+      a.mu[c0] = live0 ? u.x : 0.f;
+      a.mv[c0] = live0 ? v.x : 0.f;
+      a.mw[c0] = live0 ? w.x : 0.f;
+      a.mp[c0] = live0 ? static_cast<double>(p.x) + a.p_shift : a.p_shift;
+      a.mu[c0 + 1] = live1 ? u.y : 0.f;
+      a.mv[c0 + 1] = live1 ? v.y : 0.f;
+      a.mw[c0 + 1] = live1 ? w.y : 0.f;
+      a.mp[c0 + 1] = live1 ? static_cast<double>(p.y) + a.p_shift : a.p_shift;
+    }
+    const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+    float2 tp3[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) tp3[c] = __fmul2_rn(p, f2s(3.0f * wgt<float>(c)));
+    const float2 om = f2s(-static_cast<float>(a.omega));
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int cls = D3Q27::wclass[q];
+      const float2 e = edu2<q>(u, v, w);
+      const float2 br = __fadd2_rn(__fmul2_rn(e, __ffma2_rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
+      const float2 feq = __ffma2_rn(f2s(wgt<float>(cls)), br, tp3[cls]);
+      const float2 x = f[q];
+      const float2 fs = __fmul2_rn(__ffma2_rn(om, __fadd2_rn(x, f2(-feq.x, -feq.y)), x), f2s(a.enc.scale[q]));
+      if (live0 && live1) {
+        pl.store_pair(q, b, Pack2<S>::from_f2(fs));
+      } else {
+        if (live0) pl.store_half(q, b, Pack2<S>::from_f(fs.x));
+        if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(fs.y));
+      }
+    });
+  }
 }
 
 }  // namespace core
