@@ -67,6 +67,15 @@ WORKLOADS = {
                           u0=0.1, R=256.0, lid_u=0.1),
     "cavity128-f32": dict(case="cavity", bc="standard", storage="f32", arith="fast", n=(128, 128, 128), Re=1000,
                           u0=0.1, R=128.0, lid_u=0.1),
+    "tgv256-f16": dict(case="tgv", bc="standard", storage="f16", arith="fast", n=(256, 256, 256), Re=1600,
+                       u0=0.05, R=0.1, lid_u=0.0),
+    # flow past a sphere: 768 x 192 x 192 channel, D = 32 at (192, 96, 96), Re 100
+    "sphere768-f16": dict(case="sphere", bc="standard", storage="f16", arith="fast", n=(768, 192, 192), Re=100,
+                          u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
+    "sphere768-bf16": dict(case="sphere", bc="standard", storage="bf16", arith="fast", n=(768, 192, 192), Re=100,
+                           u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
+    "sphere768-f64": dict(case="sphere", bc="standard", storage="f64", arith="fast", n=(768, 192, 192), Re=100,
+                          u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
 }
 DEFAULT_WORKLOAD = "cavity128-f64"
 
@@ -240,6 +249,9 @@ def main(argv=None) -> int:
     cells = nx * ny * nz
     tau = tau_of(w)
     kw = dict(bc=w["bc"], storage=w["storage"], arith=w["arith"], lid_u=w["lid_u"])
+    for key in ("inlet_u", "sphere_d", "sphere_c"):
+        if key in w:
+            kw[key] = w[key]
 
     def barrier():
         torch.cuda.synchronize()

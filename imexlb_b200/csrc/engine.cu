@@ -111,11 +111,10 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
                            static_cast<int32_t>(sh.a.sq)};
     const int bxl = sh.bx_log2;
     const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
-    double drag[3] = {0.0, 0.0, 0.0};
     if constexpr (X2) {
-      const int seg = (1 << bxl) < 32 ? (1 << bxl) : 32;
-      step_cells_x2<S, B, RULE, false>(sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k, tx % seg, seg, drag);
+      step_cells_x2<S, B, RULE>(sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k);
     } else {
+      double drag[3] = {0.0, 0.0, 0.0};
       step_cells<S, B, RULE, EXACT, false>(sh.a, pl, tile.i0 + tx, tile.j0 + ty * CPT, tile.k, drag);
     }
   }
@@ -575,6 +574,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
     a.enc.scale[q] = static_cast<float>(sc);
     a.enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
+  a.enc.unit = e->storage == IMEXLB_F16 ? 16384.f : 1.f;
   in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {

@@ -24,6 +24,7 @@
 
 #include "lattice.h"
 #include "step_core.cuh"
+#include "stage_core.cuh"
 
 namespace imx {
 namespace {
@@ -96,34 +97,176 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
 
 // 2-byte formats with nx even: each thread owns an x-pair in two rows
 // (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
-template <Store S, Bc B, CaseRule RULE, bool DRAG>
+template <Store S, Bc B, CaseRule RULE>
 __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
   using T = typename StoreT<S>::T;
   const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
   const int k = blockIdx.z;
-  const int seg = blockDim.x < 32 ? blockDim.x : 32;
-  double drag[3] = {0.0, 0.0, 0.0};
   const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
-  step_cells_x2<S, B, RULE, DRAG>(a, pl, x0, j0, k, static_cast<int>(threadIdx.x) % seg, seg, drag);
-  if constexpr (DRAG) {
-    __shared__ double sh[3][8];
-    const int t = threadIdx.x + blockDim.x * threadIdx.y;
-    const int lane = t & 31, warp = t >> 5;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double x = drag[c];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) sh[c][warp] = x;
+  step_cells_x2<S, B, RULE>(a, pl, x0, j0, k);
+}
+
+// 2-byte formats, standard and periodic boundaries: rows staged in shared
+// memory by bulk copies (stage_core.cuh).  A persistent grid; block b takes
+// tiles b, b + grid, ... (y fastest, then z), so the blocks in flight cover
+// a few consecutive planes.  Warp 0 also issues the copies.
+template <Store S, Bc B, CaseRule RULE>
+__global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArgs a, const stage::Geo g) {
+  using T = typename StoreT<S>::T;
+  using namespace stage;
+  constexpr bool WRAP = B == Bc::Periodic || RULE == CaseRule::SphereStd;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* stages = reinterpret_cast<T*>(smem);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T));
+  uint64_t* empty = full + MAX_STAGES;
+  __shared__ int abort_flag;
+  const int NS = g.stages;
+  const int stage_elems = Q * g.cap;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; ++s) {
+      bar_init(&full[s], 1);
+      bar_init(&empty[s], THREADS / 32);
     }
-    __syncthreads();
-    if (t < 3) {
-      double x = 0.0;
-      for (int w = 0; w < 8; ++w) x += sh[t][w];
-      const int64_t blk = blockIdx.x + static_cast<int64_t>(gridDim.x) * (blockIdx.y + static_cast<int64_t>(gridDim.y) * blockIdx.z);
-      a.drag_part[3 * blk + t] = x;
+    abort_flag = 0;
+    bar_init_fence();
+  }
+  __syncthreads();
+  volatile int* abort_v = &abort_flag;
+  const int ntiles = g.nty * a.nz;
+  const int grid = gridDim.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const T* src = static_cast<const T*>(a.src);
+  const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
+  const int half = g.P >> 1;
+  const int npairs = g.R * half;
+
+  // the block's first NS - 1 tiles
+  int issued = 0;  // tiles of this block whose copies are issued (warp 0)
+  if (warp == 0) {
+    for (; issued < NS - 1; ++issued) {
+      const int t = blockIdx.x + issued * grid;
+      if (t >= ntiles) break;
+      issue_tile<T, WRAP>(a, g, src, (t % g.nty) * g.R, t / g.nty, stages + issued * stage_elems, &full[issued]);
     }
+  }
+  int i = 0;
+  for (int t = blockIdx.x; t < ntiles; t += grid, ++i) {
+    const int s = i % NS;
+    if (warp == 0) {
+      // refill the stage of tile i - 1 with tile i + NS - 1 once every warp
+      // has released it; the decision to stop is warp-uniform
+      const int tn = t + (NS - 1) * grid;
+      if (tn < ntiles) {
+        if (i > 0 && !__all_sync(0xffffffffu, bar_wait(&empty[(i - 1) % NS], ((i - 1) / NS) & 1u))) {
+          *abort_v = 1;
+          break;
+        }
+        const int sn = (i + NS - 1) % NS;
+        issue_tile<T, WRAP>(a, g, src, (tn % g.nty) * g.R, tn / g.nty, stages + sn * stage_elems, &full[sn]);
+        ++issued;
+      }
+    }
+    if (!__all_sync(0xffffffffu, bar_wait(&full[s], (i / NS) & 1u))) {
+      *abort_v = 1;
+      break;
+    }
+    const int j0 = (t % g.nty) * g.R, k = t / g.nty;
+    const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
+    const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
+    if constexpr (RULE == CaseRule::CavityStd) {
+      // Pairs next to a wall take the checked path; the pairs at the x walls
+      // go last, to as few warps as possible: their bounce-back reads global
+      // memory, and a warp waits for its slowest lane.
+      const int nx2 = a.nx >> 1;
+      const int ni = nx2 > 2 ? nx2 - 2 : 0;  // interior pairs per row
+      const int ne = nx2 < 2 ? nx2 : 2;      // edge pairs per row
+      const int n_int = rv * ni, n_all = n_int + rv * ne;
+      const bool wall_plane = k == 0 || k == a.nz - 1;
+      for (int p = threadIdx.x; p < n_all; p += THREADS) {
+        if (p < n_int) {
+          const int r = p / ni, x = 2 + 2 * (p - r * ni);
+          const int j = j0 + r;
+          if (wall_plane || j == 0 || j == a.ny - 1)
+            pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
+          else
+            pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k);
+        } else {
+          const int e = p - n_int, r = e / ne, x = (e - r * ne) == 0 ? 0 : a.nx - 2;
+          pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
+        }
+      }
+    } else {
+      for (int p = threadIdx.x; p < npairs; p += THREADS) {
+        const int r = p / half, x = 2 * (p - r * half);
+        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) bar_arrive(&empty[s]);
+    if (__any_sync(0xffffffffu, *abort_v != 0)) break;
+  }
+  if (warp == 0 && lane == 0 && *abort_v) {
+    // let copies still in flight land before the block exits (bounded)
+    for (int m = i; m < issued; ++m) (void)bar_wait(&full[m % NS], (m / NS) & 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && abort_flag) atomicOr(a.err, 1);
+}
+
+// Momentum-exchange drag of the 2-byte sphere channel, from the buffer a
+// step reads: every fluid cell c with a solid link along -e_q takes back
+// f*(bb(q), c), so the body receives -2 (f*(bb(q), c)) e_q.  Its own kernel
+// over the box of linked cells, so the step kernels carry no drag code;
+// per-block partial sums (3 per block) are added in a fixed order by
+// drag_sum_kernel, so the force is deterministic.
+template <Store S>
+__global__ void __launch_bounds__(256) drag_links_kernel(const StepArgs a) {
+  using T = typename StoreT<S>::T;
+  const T* src = static_cast<const T*>(a.src);
+  const int bx = a.near_hi[0] - a.near_lo[0] + 1, by = a.near_hi[1] - a.near_lo[1] + 1;
+  const int bz = a.near_hi[2] - a.near_lo[2] + 1;
+  const int64_t nbox = bx > 0 && by > 0 && bz > 0 ? static_cast<int64_t>(bx) * by * bz : 0;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < nbox;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = a.near_lo[0] + static_cast<int>(n % bx);
+    const int j = a.near_lo[1] + static_cast<int>((n / bx) % by);
+    const int k = a.near_lo[2] + static_cast<int>(n / (static_cast<int64_t>(bx) * by));
+    const int64_t cell = i + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+    const uint32_t bits = a.links[cell];
+    if (!bits) continue;
+    const int64_t b = a.base + k * a.sz + j * a.pitch + i;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q], cls = D3Q27::wclass[q];
+      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+      if ((bits >> q) & 1u) {
+        const T raw = src[static_cast<int64_t>(qb) * a.sq + b];
+        float d;
+        if constexpr (S == Store::F16) d = __fmul_rn(__half2float(raw), a.enc.inv_scale[qb]);
+        else d = __fmul_rn(__bfloat162float(raw), a.enc.inv_scale[qb]);
+        const double f = static_cast<double>(d) + 3.0 * wgt<double>(cls) * a.p_shift;
+        if constexpr (ex != 0) acc[0] -= 2.0 * f * ex;
+        if constexpr (ey != 0) acc[1] -= 2.0 * f * ey;
+        if constexpr (ez != 0) acc[2] -= 2.0 * f * ez;
+      }
+    });
+  }
+  __shared__ double sh[3][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double x = acc[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[c][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double x = 0.0;
+    for (int w = 0; w < 8; ++w) x += sh[threadIdx.x][w];
+    a.drag_part[3 * blockIdx.x + threadIdx.x] = x;
   }
 }
 
@@ -260,16 +403,70 @@ static dim3 step_block_x2(int nx) {
 
 static bool use_x2(Store s, int nx) { return (s == Store::F16 || s == Store::BF16) && nx % 2 == 0; }
 
+// Shared-memory staged kernel: 2-byte formats with nx even and the standard
+// or periodic boundaries, rows of at most 1024 stored elements.
+static bool staged_geo(const LaunchCfg& c, int nx, int ny, int64_t pitch, stage::Geo* g) {
+  if (!use_x2(c.store, nx)) return false;
+  if (c.bc != Bc::Standard && c.bc != Bc::Periodic) return false;
+  return stage::make_geo(ny, pitch, g);
+}
+
+// Blocks of the persistent staged grid: as many as fit on the device at
+// once (queried once per kernel), no more than there are tiles.
+static int device_sms() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    sms = n > 0 ? n : 148;
+  }
+  return sms;
+}
+
+template <Store S, Bc B, CaseRule R>
+static int staged_blocks(const stage::Geo& g, int nz) {
+  static int resident = 0;  // blocks of this kernel resident on the device
+  if (resident == 0) {
+    const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)));
+    cudaFuncSetAttribute(staged_kernel<S, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_kernel<S, B, R>, stage::THREADS, smem);
+    resident = (per_sm > 0 ? per_sm : 1) * device_sms();
+  }
+  const int64_t ntiles = static_cast<int64_t>(g.nty) * nz;
+  return static_cast<int>(ntiles < resident ? ntiles : resident);
+}
+
+template <Store S, Bc B, CaseRule R>
+static cudaError_t launch_staged(const StepArgs& a, const stage::Geo& g, cudaStream_t s) {
+  const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)));
+  const int blocks = staged_blocks<S, B, R>(g, a.nz);
+  staged_kernel<S, B, R><<<blocks, stage::THREADS, smem, s>>>(a, g);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ launchers
 int reduce_blocks() { return RED_BLOCKS; }
 
-int64_t step_grid_blocks(int nx, int ny, int nz, int storage) {
-  if (use_x2(static_cast<Store>(storage), nx)) {
-    const dim3 b = step_block_x2(nx);
-    return static_cast<int64_t>((nx + 2 * b.x - 1) / (2 * b.x)) * ((ny + 2 * b.y - 1) / (2 * b.y)) * nz;
-  }
+constexpr int DRAG_LINK_BLOCKS = 148;
+
+bool drag_in_own_kernel(Store s) { return s == Store::F16 || s == Store::BF16; }
+
+cudaError_t launch_drag_links(Store st, const StepArgs& a, cudaStream_t s) {
+  if (st == Store::F16)
+    drag_links_kernel<Store::F16><<<DRAG_LINK_BLOCKS, 256, 0, s>>>(a);
+  else if (st == Store::BF16)
+    drag_links_kernel<Store::BF16><<<DRAG_LINK_BLOCKS, 256, 0, s>>>(a);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+int64_t step_grid_blocks(const LaunchCfg& c, int nx, int ny, int nz) {
+  if (drag_in_own_kernel(c.store)) return DRAG_LINK_BLOCKS;
   const dim3 b = step_block(nx);
-  const int cpt = storage == static_cast<int>(Store::F64) ? 1 : CellsPerThread<Store::F16>::value;
+  const int cpt = c.store == Store::F64 ? 1 : CellsPerThread<Store::F32>::value;
   const int rows = b.y * cpt;
   return static_cast<int64_t>((nx + b.x - 1) / b.x) * ((ny + rows - 1) / rows) * nz;
 }
@@ -315,24 +512,23 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
 
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
+  if constexpr ((S == Store::F16 || S == Store::BF16) && (B == Bc::Standard || B == Bc::Periodic)) {
+    stage::Geo g;
+    if (staged_geo(LaunchCfg{B, S, R, EXACT}, a.nx, a.ny, a.pitch, &g)) return launch_staged<S, B, R>(a, g, s);
+  }
   if constexpr (S == Store::F16 || S == Store::BF16) {
+    // (the 2-byte formats sum their drag in drag_links_kernel)
     if (use_x2(S, a.nx)) {
       const dim3 block = step_block_x2(a.nx);
       const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
-      if constexpr (R == CaseRule::SphereStd) {
-        if (a.drag_part) {
-          step_kernel_x2<S, B, R, true><<<grid, block, 0, s>>>(a);
-          return cudaGetLastError();
-        }
-      }
-      step_kernel_x2<S, B, R, false><<<grid, block, 0, s>>>(a);
+      step_kernel_x2<S, B, R><<<grid, block, 0, s>>>(a);
       return cudaGetLastError();
     }
   }
   const dim3 block = step_block(a.nx);
   const int rows = block.y * CellsPerThread<S>::value;
   const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);
-  if constexpr (R == CaseRule::SphereStd) {
+  if constexpr (R == CaseRule::SphereStd && S != Store::F16 && S != Store::BF16) {
     if (a.drag_part) {
       step_kernel<S, B, R, EXACT, true><<<grid, block, 0, s>>>(a);
       return cudaGetLastError();

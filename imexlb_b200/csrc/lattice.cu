@@ -83,7 +83,11 @@ Layout make_layout(int nx, int ny, int nz, int g, int elem) {
   L.ex = nx + 2 * g;
   L.ey = ny + 2 * g;
   L.ez = nz + 2 * g;
-  const int64_t line = 128 / elem;  // elements per 128-byte line
+  // Rows start on 128-byte lines, except for the 2-byte formats without
+  // ghosts: there a row is padded to 16 elements (one 32-byte sector) only,
+  // so the rows of a plane are contiguous for nx a multiple of 16 and the
+  // staged kernels copy several rows with one bulk copy.
+  const int64_t line = (elem == 2 && g == 0) ? 16 : 128 / elem;
   L.xoff = (line - (g % line)) % line;
   L.pitch = ((L.xoff + L.ex + line - 1) / line) * line;
   L.sz = L.pitch * L.ey;
@@ -144,6 +148,7 @@ struct imexlb_lattice {
   DevArray<double> red;       // reduction partials + result
   DevArray<double> drag_part; // standard sphere: per-block drag partials of the last step
   int64_t drag_blocks = 0;
+  DevArray<int> err;          // non-zero after a step kernel gave up waiting
   cudaStream_t stream = nullptr;
   int64_t steps = 0;
   std::vector<int32_t> usr_padded;  // host copy, padded box (reference sphere)
@@ -393,6 +398,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
     h->enc.scale[q] = static_cast<float>(sc);
     h->enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
+  h->enc.unit = P.storage == IMEXLB_F16 ? 16384.f : 1.f;
 
   const size_t padded = static_cast<size_t>(L.ex) * L.ey * L.ez;
   if (P.kase == IMEXLB_SPHERE) {
@@ -411,9 +417,12 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   IMX_CUDA(h->buf[1].alloc(L.bytes()));
   IMX_CUDA(h->mom.alloc(4 * static_cast<size_t>(h->ncell)));
   IMX_CUDA(h->red.alloc(reduce_blocks() + 8));
+  IMX_CUDA(h->err.alloc(1));
+  IMX_CUDA(cudaMemset(h->err.p, 0, sizeof(int)));
 
   // base step arguments
   StepArgs& a = h->base_args;
+  a.err = h->err.p;
   a.nx = P.nx;
   a.ny = P.ny;
   a.nz = P.nz;
@@ -472,7 +481,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
         a.near_lo[d] = lo[d];
         a.near_hi[d] = hi[d];
       }
-      h->drag_blocks = step_grid_blocks(P.nx, P.ny, P.nz, static_cast<int>(P.storage));
+      h->drag_blocks = step_grid_blocks(h->cfg, P.nx, P.ny, P.nz);
       IMX_CUDA(h->drag_part.alloc(3 * static_cast<size_t>(h->drag_blocks)));
       IMX_CUDA(cudaMemset(h->drag_part.p, 0, h->drag_part.n * sizeof(double)));
       // equilibrium populations of the inlet (deviation form)
@@ -537,7 +546,9 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
       a.dstq[q] = h->buf[1 - h->cur].p + static_cast<size_t>(q) * h->L.sq * h->L.elem;
     }
     a.store = s == nsteps - 1;
-    a.drag_part = (a.store && h->drag_part.p) ? h->drag_part.p : nullptr;
+    const bool drag = a.store && h->drag_part.p;
+    const bool drag_own = drag && drag_in_own_kernel(h->cfg.store);
+    a.drag_part = (drag && !drag_own) ? h->drag_part.p : nullptr;
     imexlb_lattice::Timed t0{nullptr, nullptr, 0}, t1{nullptr, nullptr, 1};
     if (h->profiling) {
       t0.a = h->take_event();
@@ -548,6 +559,11 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
     if (h->profiling) {
       IMX_CUDA(cudaEventRecord(t0.b, h->stream));
       h->timed.push_back(t0);
+    }
+    if (drag_own) {
+      StepArgs d = a;
+      d.drag_part = h->drag_part.p;
+      IMX_CUDA(launch_drag_links(h->cfg.store, d, h->stream));
     }
     if (h->gn) {
       if (h->profiling) {
@@ -567,6 +583,19 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
   return IMEXLB_OK;
 }
 
+// Wait for the lattice's stream and report a step kernel that gave up
+// waiting for its staged copies (its error word is then cleared).
+static int sync_checked(imexlb_lattice* h) {
+  int word = 0;
+  IMX_CUDA(cudaMemcpyAsync(&word, h->err.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  if (word) {
+    IMX_CUDA(cudaMemset(h->err.p, 0, sizeof(int)));
+    return fail(IMEXLB_E_CUDA, "a step kernel gave up waiting for its staged row copies; the lattice state is invalid");
+  }
+  return IMEXLB_OK;
+}
+
 int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double* p) {
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
   double* dst[4] = {u, v, w, p};
@@ -574,8 +603,7 @@ int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double
     if (dst[c])
       IMX_CUDA(cudaMemcpyAsync(dst[c], h->mom.p + c * h->ncell, h->ncell * sizeof(double), cudaMemcpyDeviceToHost,
                                h->stream));
-  IMX_CUDA(cudaStreamSynchronize(h->stream));
-  return IMEXLB_OK;
+  return sync_checked(h);
 }
 
 int imexlb_get_mask(imexlb_lattice* h, int32_t* usr) {
@@ -703,7 +731,7 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
         IMX_CUDA(cudaMemcpyAsync(&den, res + 1, 8, cudaMemcpyDeviceToHost, h->stream));
       }
       IMX_CUDA(cudaMemcpyAsync(h->prev_mom.p, u, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-      IMX_CUDA(cudaStreamSynchronize(h->stream));
+      if (const int rc = sync_checked(h)) return rc;
       const bool first = !h->have_prev;
       h->have_prev = true;
       *out = first ? INFINITY : (den > 0 ? std::sqrt(num / den) : (num > 0 ? INFINITY : 0.0));
@@ -715,7 +743,7 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
       if (!h->drag_part.p) return fail(IMEXLB_E_UNSUPPORTED, "drag needs the standard sphere channel");
       IMX_CUDA(launch_drag_sum(h->drag_part.p, h->drag_blocks, res, h->stream));
       IMX_CUDA(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-      IMX_CUDA(cudaStreamSynchronize(h->stream));
+      if (const int rc = sync_checked(h)) return rc;
       if (!std::isfinite(out[0]) || !std::isfinite(out[1]) || !std::isfinite(out[2]))
         return fail(IMEXLB_E_STATE, "drag is not finite");
       return IMEXLB_OK;
@@ -724,7 +752,7 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
       return fail(IMEXLB_E_ARG, "unknown or unsupported reduction");
   }
   IMX_CUDA(cudaMemcpyAsync(out, res, 8, cudaMemcpyDeviceToHost, h->stream));
-  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  if (const int rc = sync_checked(h)) return rc;
   if (!std::isfinite(*out)) return fail(IMEXLB_E_STATE, "lattice is not finite (NaN/Inf in the moments)");
   return IMEXLB_OK;
 }
@@ -797,8 +825,7 @@ int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out) {
 
 int imexlb_synchronize(imexlb_lattice* h) {
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
-  IMX_CUDA(cudaStreamSynchronize(h->stream));
-  return IMEXLB_OK;
+  return sync_checked(h);
 }
 
 void imexlb_destroy(imexlb_lattice* h) {

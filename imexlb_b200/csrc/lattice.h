@@ -27,7 +27,8 @@ enum class CaseRule : int {
 // Storage layout of one distribution buffer: 27 population planes, each a
 // (z, y, x) box of stored extents (n + 2g) with x fastest.  Stored x = 0 sits
 // `xoff` elements into its row so that interior x = 0 starts on a 128-byte
-// boundary; rows, planes and populations are padded to 128 bytes.
+// boundary; rows, planes and populations are padded to 128 bytes (to 32
+// bytes for the 2-byte formats without ghosts, see make_layout).
 struct Layout {
   int nx = 0, ny = 0, nz = 0;  // interior
   int g = 0;                   // stored ghost width (3 for reference boundaries)
@@ -45,9 +46,12 @@ Layout make_layout(int nx, int ny, int nz, int g, int elem);
 // Per-population scaling of reduced-precision storage:
 // stored = d_q * scale[q], d_q = stored * inv_scale[q], where d_q is the
 // deviation f_q - 3 w_q p_shift.
+// For the 2-byte formats scale[q] = unit / w_q, unit = 2^14 for FP16 (keeps
+// small deviations out of the subnormals) and 1 for BF16; FP32 stores d_q.
 struct Encoding {
   float scale[Q];
   float inv_scale[Q];
+  float unit = 1.f;
 };
 
 struct StepArgs {
@@ -82,6 +86,7 @@ struct StepArgs {
   const uint32_t* links = nullptr;  // standard sphere: per-cell bit q = the link along -e_q ends in the solid
   int near_lo[3] = {0, 0, 0};       // box of cells that have solid links
   int near_hi[3] = {-1, -1, -1};
+  int* err = nullptr;  // set non-zero by a kernel that gave up waiting (staged steps)
   Encoding enc;
 };
 
@@ -129,8 +134,15 @@ cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s);
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
                                 int64_t n, int64_t sq, const Encoding& enc, cudaStream_t s);
 dim3 step_block(int nx);
-int64_t step_grid_blocks(int nx, int ny, int nz, int storage);
+// Blocks that write one drag partial each: the step launch of this
+// configuration, or the drag kernel's blocks for the 2-byte formats.
+int64_t step_grid_blocks(const LaunchCfg& c, int nx, int ny, int nz);
 cudaError_t launch_drag_sum(const double* part, int64_t nblk, double* out, cudaStream_t s);
+// 2-byte formats: the sphere's drag is summed by its own kernel from the
+// buffer a step reads (launch it with that step's arguments after the step)
+// instead of inside the step kernel.
+bool drag_in_own_kernel(Store s);
+cudaError_t launch_drag_links(Store st, const StepArgs& a, cudaStream_t s);
 // Deterministic FP64 sums over n values: out[c] = sum of comp(c) over cells
 // for the requested quantity; partial sums of `blocks` blocks go to scratch.
 enum class RedKind : int { Mass = 0, Kinetic = 1, DiffSq = 2, NormSq = 3, UMax = 4 };

@@ -1,0 +1,291 @@
+// Shared-memory staged step for the 2-byte storage formats (FP16, BF16).
+//
+// The register-staged kernels keep every pulled population of a thread's
+// cells in registers until it is used, so the bytes a warp can have in
+// flight are bounded by its registers, and the step waits on DRAM latency
+// long before it reaches DRAM bandwidth.  Here the loads are bulk
+// asynchronous copies (cp.async.bulk, the untiled TMA path) into shared
+// memory, completed on an mbarrier, so a block keeps the next tile in flight
+// while it computes on the current one.
+//
+// A tile is R whole rows [j0, j0 + R) of plane k.  Population q of those
+// cells pulls from rows j0 - e_y .. j0 + R - 1 - e_y of plane k - e_z,
+// shifted by e_x along x.  The 2-byte layouts pad rows to 16 elements only,
+// so those R source rows are one contiguous run of memory and a tile needs
+// one bulk copy per population (two where a periodic y wraps).  Whole rows
+// also hold the x wrap of a periodic lattice.  A source plane outside the
+// box is not copied: the cavity's walls replace those values (halfway
+// bounce-back), and a periodic axis copies the wrapped plane.  Each copy
+// costs the copy engine about the same whatever its size, so few large
+// copies per tile are what keep DRAM busy.
+//
+// Warp 0 issues the copies of the block's tiles in order: tile i goes to
+// stage i mod STAGES once all eight warps have released that stage's
+// previous tile (its "empty" mbarrier), and the stage's "full" mbarrier
+// counts the tile's bytes.  Every warp waits on "full", updates its cells
+// and releases the stage.  Each thread updates x-pairs of cells with the
+// same arithmetic as the register-staged x-pair kernels (finish_pair_row).
+// Halfway bounce-back and solid links read the cell's own opposite
+// population from global memory, in a second pass that only boundary pairs
+// take.
+//
+// Every wait on an mbarrier gives up after about a second of wall-clock time
+// (%globaltimer), records the failure in the step's error word and leaves
+// the kernel; the host reports it at its next synchronising call.
+#pragma once
+
+#include "step_core.cuh"
+
+namespace imx {
+namespace stage {
+
+using namespace core;
+
+constexpr int THREADS = 256;
+constexpr int SLOT_UNITS = 2 * 1024;  // stages x elements per population slot
+constexpr uint64_t WAIT_NS = 1000000000ull;
+constexpr int MAX_STAGES = 2;
+
+// Tile geometry of one lattice.
+struct Geo {
+  int P;       // staged row length: the layout's pitch (whole rows)
+  int R;       // rows per tile
+  int cap;     // elements per population slot of a stage (R * P <= cap)
+  int stages;  // stages * cap == SLOT_UNITS
+  int nty;     // tiles along y
+};
+
+// Whole-row tiles for rows of `pitch` elements (a multiple of 16, at most
+// 1024): population slots of 1024 elements in 2 stages.  Fewer, larger
+// copies beat deeper pipelines here (2 KB copies in 2 stages measured
+// faster than 1 KB copies in 4 stages of the same shared memory).
+inline bool make_geo(int ny, int64_t pitch, Geo* g) {
+  if (pitch % 16 != 0 || pitch > 1024) return false;
+  g->P = static_cast<int>(pitch);
+  g->cap = 1024;
+  g->stages = SLOT_UNITS / g->cap;
+  g->R = g->cap / g->P;
+  if (g->R > ny) g->R = ny;
+  g->nty = (ny + g->R - 1) / g->R;
+  return true;
+}
+
+// stages of 27 population slots, then the full and empty mbarriers
+inline size_t smem_bytes(int elem) { return static_cast<size_t>(27) * SLOT_UNITS * elem + 16 * MAX_STAGES; }
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void bar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void bar_arrive_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for the phase of `parity` to complete; false after about a second.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+  if (bar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (true) {
+    if (bar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > WAIT_NS) return false;
+  }
+}
+
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from global to this block's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// e_y + 1 and e_z + 1 of population q, two bits each (q runtime)
+constexpr uint64_t pack_axis(int axis) {
+  uint64_t v = 0;
+  for (int q = 0; q < Q; ++q) v |= static_cast<uint64_t>((axis == 1 ? D3Q27::ey[q] : D3Q27::ez[q]) + 1) << (2 * q);
+  return v;
+}
+constexpr uint64_t EY_BITS = pack_axis(1), EZ_BITS = pack_axis(2);
+__device__ __forceinline__ int ey_of(int q) { return static_cast<int>((EY_BITS >> (2 * q)) & 3u) - 1; }
+__device__ __forceinline__ int ez_of(int q) { return static_cast<int>((EZ_BITS >> (2 * q)) & 3u) - 1; }
+
+// The copies of population q for a tile: the source rows of tile rows
+// [0, rv) as at most two contiguous runs, the second one a wrapped row
+// (bytes 0 = no copy).
+struct Run {
+  int32_t src;  // element index within plane q
+  int32_t dst;  // element offset within the stage
+  uint32_t bytes;
+};
+
+template <bool WRAP_YZ>
+__device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q, int j0, int k, int rv, int elem,
+                                          Run& main, Run& wrap) {
+  main.bytes = 0;
+  wrap.bytes = 0;
+  int kk = k - ez_of(q);
+  if (kk < 0 || kk >= a.nz) {
+    if (!WRAP_YZ) return;
+    kk = kk < 0 ? kk + a.nz : kk - a.nz;
+  }
+  const int y0 = j0 - ey_of(q);  // source row of tile row 0
+  const int32_t plane = a.base32 + kk * a.sz32;
+  const int32_t slot = q * g.cap;
+  const int r_lo = y0 < 0 ? -y0 : 0;
+  const int r_hi = y0 + rv > a.ny ? a.ny - y0 : rv;
+  main.src = plane + (y0 + r_lo) * a.pitch32;
+  main.dst = slot + r_lo * g.P;
+  main.bytes = r_hi > r_lo ? static_cast<uint32_t>((r_hi - r_lo) * g.P * elem) : 0u;
+  if (WRAP_YZ) {
+    // tile row 0 pulls from y = -1 (the last row), or the last tile row
+    // from y = ny (the first row); |e_y| <= 1 allows one of them at most
+    const bool first = r_lo > 0, last = r_hi < rv;
+    wrap.src = plane + (first ? (a.ny - 1) * a.pitch32 : 0);
+    wrap.dst = slot + (first ? 0 : (rv - 1) * g.P);
+    wrap.bytes = (first || last) ? static_cast<uint32_t>(g.P * elem) : 0u;
+  }
+}
+
+// Issue the copies of tile (j0, k) into stage `st` (called by a whole warp;
+// lane q < 27 copies population q).  `src` is the buffer being read,
+// population q at q * a.sq.
+template <class T, bool WRAP_YZ>
+__device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, const T* src, int j0, int k, T* st,
+                                           uint64_t* bar) {
+  const int lane = threadIdx.x & 31;
+  const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
+  Run m{0, 0, 0u}, w{0, 0, 0u};
+  if (lane < Q) tile_runs<WRAP_YZ>(a, g, lane, j0, k, rv, static_cast<int>(sizeof(T)), m, w);
+  uint32_t total = m.bytes + w.bytes;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+  if (lane == 0) bar_arrive_expect(bar, total);
+  __syncwarp();
+  const T* plane = src + static_cast<int64_t>(lane) * a.sq;
+  if (m.bytes) bulk_g2s(st + m.dst, plane + m.src, m.bytes, bar);
+  if (w.bytes) bulk_g2s(st + w.dst, plane + w.src, w.bytes, bar);
+}
+
+// The x-pair (x, x + 1) in tile row r of tile (j0, k), read from the staged
+// rows.  `st` is the stage as 4-byte words.  Boundary values (halfway
+// bounce-back at the cavity's walls, solid links of the sphere) are put in
+// place by a second pass that only boundary pairs take.  EDGE = false
+// promises that no boundary rule of the box applies to the pair:
+// 2 <= x < nx - 2 and, for the cavity, no wall row or plane around it.
+template <Store S, Bc B, CaseRule RULE, bool EDGE, class P>
+__device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
+                                                const int x, const int r, const int j0, const int k) {
+  const int j = j0 + r;
+  const int row = (r * g.P) >> 1;  // word offset of tile row r in a slot
+  const int pw = row + (x >> 1);
+  const bool left_edge = EDGE && x == 0, right_edge = EDGE && x + 2 >= a.nx;
+  const int lw = row + ((left_edge ? a.nx - 2 : x - 2) >> 1);  // holds x - 1 (wrapped)
+  const int rw = row + ((right_edge ? 0 : x + 2) >> 1);       // holds x + 2 (wrapped)
+  const int slotw = g.cap >> 1;
+
+  uint32_t raw[Q];
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    constexpr int ex = D3Q27::ex[q];
+    const uint32_t* slot = st + q * slotw;
+    const uint32_t pv = slot[pw];
+    uint32_t v = pv;
+    if constexpr (ex == 1) {
+      v = pair_of(slot[lw] >> 16, pv);
+    } else if constexpr (ex == -1) {
+      uint32_t rlo = slot[rw] & 0xffffu;
+      if constexpr (RULE == CaseRule::SphereStd) {
+        if (right_edge) rlo = pv >> 16;  // zero-gradient outlet: the own column
+      }
+      v = pair_of(pv >> 16, rlo);
+    }
+    raw[q] = v;
+  });
+
+  const int32_t bself = a.base32 + k * a.sz32 + j * a.pitch32 + x;
+  bool live0 = true, live1 = true;
+  if constexpr (RULE == CaseRule::CavityStd && EDGE) {
+    uint32_t out_bits = 0;  // bit (3 dz + dy): source row outside the box
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        const int jj = j + dy - 1, kk = k + dz - 1;
+        if (jj < 0 || jj >= a.ny || kk < 0 || kk >= a.nz) out_bits |= 1u << (3 * dz + dy);
+      }
+    if (out_bits || left_edge || right_edge) {
+      // halfway bounce-back: a link leaving the box returns the cell's own
+      // opposite population
+      static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+        constexpr int qb = D3Q27::bb[q];
+        const bool out_row = (out_bits >> (3 * (1 - ez) + (1 - ey))) & 1u;
+        const bool out0 = out_row || (ex == 1 && left_edge);
+        const bool out1 = out_row || (ex == -1 && right_edge);
+        if (out0 || out1) {
+          const uint32_t bbp = pl.load_pair(qb, bself);
+          raw[q] = pair_of(out0 ? bbp : raw[q], out1 ? (bbp >> 16) : (raw[q] >> 16));
+        }
+      });
+    }
+  } else if constexpr (RULE == CaseRule::SphereStd) {
+    // solid cells lie inside the box of linked cells: the sphere is enclosed
+    // by the fluid cells whose links end in it
+    const bool near = k >= a.near_lo[2] && k <= a.near_hi[2] && j >= a.near_lo[1] && j <= a.near_hi[1] &&
+                      x + 1 >= a.near_lo[0] && x <= a.near_hi[0];
+    if (near) {
+      const int64_t cell = x + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+      const uint32_t links0 = a.links[cell], links1 = a.links[cell + 1];
+      live0 = a.usr[cell] != 0;
+      live1 = a.usr[cell + 1] != 0;
+      if (links0 | links1) {
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          constexpr int qb = D3Q27::bb[q];
+          const bool s0 = (links0 >> q) & 1u, s1 = (links1 >> q) & 1u;
+          if (s0 || s1) {
+            const uint32_t bbp = pl.load_pair(qb, bself);
+            raw[q] = pair_of(s0 ? bbp : raw[q], s1 ? (bbp >> 16) : (raw[q] >> 16));
+          }
+        });
+      }
+    }
+  }
+  const bool lid = RULE == CaseRule::CavityStd && k == a.nz - 1;
+  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1);
+}
+
+}  // namespace stage
+}  // namespace imx

@@ -567,21 +567,98 @@ template <> struct Pack2<Store::BF16> {
 // pair (lo = cell x0, hi = cell x0 + 1) from two 16-bit halves
 __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { return (lo16 & 0xffffu) | (hi16 << 16); }
 
-template <Store S, Bc B, CaseRule RULE, bool DRAG, class P>
-__device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, const int x0, const int j0, const int k,
-                                              const int seg_lane, const int seg, double (&drag)[3]) {
+// Second half of a 2-byte x-pair update: decode the pulled pairs (boundary
+// values already in place), moments, case rules, collision and the paired
+// store.  Shared by the register-staged kernels and the shared-memory staged
+// kernels, so both produce the same bits.
+//
+// The collision runs in the stored units g_q = d_q * unit / w_q (d_q the
+// deviation f_q - 3 w_q p_shift), where the equilibrium needs no weight:
+//   g_q' = (1 - omega) g_q + omega unit (3 p~ + e(3 + 4.5 e) - 1.5 u.u),
+// e = c_q . u and p~ = sum d_q / 3 = p - p_shift, since the shift's own
+// equilibrium cancels (sum w_q = 1, sum w_q c_q = 0).  The moments take
+// d_q = g_q w_q / unit.  live0 / live1: the cell is fluid (a solid cell's
+// values are left as they are).
+template <Store S, CaseRule RULE, class P>
+__device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
+                                                const int j, const int k, const bool lid, const bool left_edge,
+                                                const bool live0, const bool live1) {
+  float2 g[Q];
+  float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
+  [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+    float2 x = Pack2<S>::to_f2(raw[q]);
+    if constexpr (RULE == CaseRule::CavityStd && ex != 0 && ez < 0) {
+      // moving lid: + 6 rho_w w_q (c_q . u_w), in stored units
+      if (lid) x = __fadd2_rn(x, f2s(ex > 0 ? lid_g : -lid_g));
+    }
+    if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
+      if (left_edge) x.x = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
+    }
+    const float2 d = __fmul2_rn(x, f2s(a.enc.inv_scale[q]));
+    s = __fadd2_rn(s, d);
+    if constexpr (ex == 1) u = __fadd2_rn(u, d);
+    if constexpr (ex == -1) u = __fadd2_rn(u, f2(-d.x, -d.y));
+    if constexpr (ey == 1) v = __fadd2_rn(v, d);
+    if constexpr (ey == -1) v = __fadd2_rn(v, f2(-d.x, -d.y));
+    if constexpr (ez == 1) w = __fadd2_rn(w, d);
+    if constexpr (ez == -1) w = __fadd2_rn(w, f2(-d.x, -d.y));
+    g[q] = x;
+  });
+  const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + x0;
+  const int64_t c0 = x0 + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
+  float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
+  case_rules<RULE>(a, x0, k, c0, u.x, v.x, w.x, p.x);
+  case_rules<RULE>(a, x0 + 1, k, c0 + 1, u.y, v.y, w.y, p.y);
+  if (a.store) {
+    a.mu[c0] = live0 ? u.x : 0.f;
+    a.mv[c0] = live0 ? v.x : 0.f;
+    a.mw[c0] = live0 ? w.x : 0.f;
+    a.mp[c0] = live0 ? static_cast<double>(p.x) + a.p_shift : a.p_shift;
+    a.mu[c0 + 1] = live1 ? u.y : 0.f;
+    a.mv[c0 + 1] = live1 ? v.y : 0.f;
+    a.mw[c0 + 1] = live1 ? w.y : 0.f;
+    a.mp[c0 + 1] = live1 ? static_cast<double>(p.y) + a.p_shift : a.p_shift;
+  }
+  const float om = static_cast<float>(a.omega);
+  const float om_u = om * a.enc.unit;
+  const float2 keep = f2s(1.0f - om);
+  const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+  // omega unit (3 p~ - 1.5 u.u)
+  const float2 K = __fmul2_rn(f2s(om_u), __ffma2_rn(p, f2s(3.0f), f2(-udu15.x, -udu15.y)));
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    float2 gn;
+    if constexpr (q == 0) {
+      gn = __ffma2_rn(g[q], keep, K);
+    } else {
+      const float2 e = edu2<q>(u, v, w);
+      const float2 t = __ffma2_rn(e, f2s(4.5f), f2s(3.0f));
+      const float2 h = __fmul2_rn(e, f2s(om_u));
+      gn = __ffma2_rn(h, t, __ffma2_rn(g[q], keep, K));
+    }
+    if (live0 && live1) {
+      pl.store_pair(q, b, Pack2<S>::from_f2(gn));
+    } else {
+      if (live0) pl.store_half(q, b, Pack2<S>::from_f(gn.x));
+      if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(gn.y));
+    }
+  });
+}
+
+template <Store S, Bc B, CaseRule RULE, class P>
+__device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, const int x0, const int j0, const int k) {
   constexpr int RY = 2;
   const bool xin = x0 < a.nx;  // nx even: both cells of the pair or neither
   const int xs = xin ? x0 : a.nx - 2;
-  (void)seg_lane;
-  (void)seg;
   const bool left_edge = xs == 0, right_edge = xs + 2 >= a.nx;
   uint32_t raw[RY][Q];
   int32_t rowb[RY][3][3];  // [r][1 - ez][1 - ey]: index of x = xs in the source row
   bool act[RY];
   uint32_t row_out_bits[RY];  // cavity: bit (3 dz + dy) = source row outside the box
   uint32_t lid_mask = 0;      // cavity: rows whose cells sit under the lid
-  uint32_t solid0[RY], solid1[RY];  // sphere: per-cell solid-link bits
   int32_t bself[RY];
 
   // Every population of both rows arrives as aligned 4-byte pairs issued
@@ -626,8 +703,6 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       links0 = near ? a.links[cell] : 0u;
       links1 = near ? a.links[cell + 1] : 0u;
     }
-    solid0[r] = links0;
-    solid1[r] = links1;
     if constexpr (RULE == CaseRule::CavityStd) {
       if (k == a.nz - 1) lid_mask |= 1u << r;
     }
@@ -684,88 +759,14 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
 
 #pragma unroll
   for (int r = 0; r < RY; ++r) {
-    const int j = j0 + r;
-    float2 f[Q];
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      constexpr int ex = D3Q27::ex[q];
-      [[maybe_unused]] constexpr int ey = D3Q27::ey[q], ez = D3Q27::ez[q];
-      constexpr int cls = D3Q27::wclass[q];
-      float2 x = __fmul2_rn(Pack2<S>::to_f2(raw[r][q]), f2s(a.enc.inv_scale[q]));
-      if constexpr (RULE == CaseRule::CavityStd && ex != 0 && ez < 0) {
-        if ((lid_mask >> r) & 1u) {
-          const float t = static_cast<float>(6.0 * a.rho_w * a.lid_u) * wgt<float>(cls) * static_cast<float>(ex);
-          x = __fadd2_rn(x, f2s(t));
-        }
-      }
-      if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
-        if (left_edge) x.x = static_cast<float>(a.feq_in[q]);
-      }
-      if constexpr (DRAG && RULE == CaseRule::SphereStd) {
-        const bool s0 = (solid0[r] >> q) & 1u, s1 = (solid1[r] >> q) & 1u;
-        const double add = (s0 ? static_cast<double>(x.x) : 0.0) + (s1 ? static_cast<double>(x.y) : 0.0);
-        if (act[r] && (s0 || s1)) {
-          const double shift = 3.0 * wgt<double>(cls) * a.p_shift * ((s0 ? 1.0 : 0.0) + (s1 ? 1.0 : 0.0));
-          if constexpr (ex != 0) drag[0] -= 2.0 * (add + shift) * ex;
-          if constexpr (ey != 0) drag[1] -= 2.0 * (add + shift) * ey;
-          if constexpr (ez != 0) drag[2] -= 2.0 * (add + shift) * ez;
-        }
-      }
-      f[q] = x;
-    });
     if (!act[r]) continue;
-    const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + x0;
-    const int64_t c0 = x0 + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
-    bool live0 = true, live1 = true;
+    bool live0 = true, live1 = true;  // sphere: fluid cells (solid cells keep their values)
     if constexpr (RULE == CaseRule::SphereStd) {
+      const int64_t c0 = x0 + static_cast<int64_t>(a.nx) * (j0 + r + static_cast<int64_t>(a.ny) * k);
       live0 = a.usr[c0] != 0;
       live1 = a.usr[c0 + 1] != 0;
     }
-    float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      const float2 x = f[q];
-      s = __fadd2_rn(s, x);
-      if constexpr (D3Q27::ex[q] == 1) u = __fadd2_rn(u, x);
-      if constexpr (D3Q27::ex[q] == -1) u = __fadd2_rn(u, f2(-x.x, -x.y));
-      if constexpr (D3Q27::ey[q] == 1) v = __fadd2_rn(v, x);
-      if constexpr (D3Q27::ey[q] == -1) v = __fadd2_rn(v, f2(-x.x, -x.y));
-      if constexpr (D3Q27::ez[q] == 1) w = __fadd2_rn(w, x);
-      if constexpr (D3Q27::ez[q] == -1) w = __fadd2_rn(w, f2(-x.x, -x.y));
-    });
-    float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
-    case_rules<RULE>(a, x0, k, c0, u.x, v.x, w.x, p.x);
-    case_rules<RULE>(a, x0 + 1, k, c0 + 1, u.y, v.y, w.y, p.y);
-    if (a.store) {
-      a.mu[c0] = live0 ? u.x : 0.f;
-      a.mv[c0] = live0 ? v.x : 0.f;
-      a.mw[c0] = live0 ? w.x : 0.f;
-      a.mp[c0] = live0 ? static_cast<double>(p.x) + a.p_shift : a.p_shift;
-      a.mu[c0 + 1] = live1 ? u.y : 0.f;
-      a.mv[c0 + 1] = live1 ? v.y : 0.f;
-      a.mw[c0 + 1] = live1 ? w.y : 0.f;
-      a.mp[c0 + 1] = live1 ? static_cast<double>(p.y) + a.p_shift : a.p_shift;
-    }
-    const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
-    float2 tp3[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) tp3[c] = __fmul2_rn(p, f2s(3.0f * wgt<float>(c)));
-    const float2 om = f2s(-static_cast<float>(a.omega));
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      constexpr int cls = D3Q27::wclass[q];
-      const float2 e = edu2<q>(u, v, w);
-      const float2 br = __fadd2_rn(__fmul2_rn(e, __ffma2_rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
-      const float2 feq = __ffma2_rn(f2s(wgt<float>(cls)), br, tp3[cls]);
-      const float2 x = f[q];
-      const float2 fs = __fmul2_rn(__ffma2_rn(om, __fadd2_rn(x, f2(-feq.x, -feq.y)), x), f2s(a.enc.scale[q]));
-      if (live0 && live1) {
-        pl.store_pair(q, b, Pack2<S>::from_f2(fs));
-      } else {
-        if (live0) pl.store_half(q, b, Pack2<S>::from_f(fs.x));
-        if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(fs.y));
-      }
-    });
+    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1);
   }
 }
 

@@ -98,3 +98,25 @@ def test_reduced_precision_error(api, case, storage, n, steps, bound):
         got = lbm.fields()
     err = rel_l2(got, want)
     assert err <= bound, f"{storage} {case}: relative velocity L2 error {err:.3e} > {bound:.1e}"
+
+
+# sphere channel: (storage, bound on the velocity L2 error, bound on the
+# relative error of the drag force along x), both against the FP64 run
+SPHERE_PRECISION = [("f32", 1e-5, 1e-5), ("f16", 1e-3, 2e-3), ("bf16", 1e-2, 2e-2)]
+
+
+@pytest.mark.parametrize("storage,vel_bound,drag_bound", SPHERE_PRECISION)
+def test_sphere_reduced_precision_velocity_and_drag(api, storage, vel_bound, drag_bound):
+    kw = dict(inlet_u=0.05, sphere_d=12.0, sphere_c=(24.0, 16.0, 16.0))
+    n, tau, steps = (96, 32, 32), 0.048, 300
+    with api.LBM("sphere", *n, tau, 1.0, 0.05, bc="standard", arith="fast", **kw) as ref:
+        ref.step(steps)
+        want, dwant = ref.fields(), ref.reduce("drag")
+    with api.LBM("sphere", *n, tau, 1.0, 0.05, bc="standard", storage=storage, **kw) as lbm:
+        lbm.step(steps)
+        got, dgot = lbm.fields(), lbm.reduce("drag")
+    assert dwant[0] > 0.0
+    err = rel_l2(got, want)
+    assert err <= vel_bound, f"{storage} sphere: relative velocity L2 error {err:.3e} > {vel_bound:.1e}"
+    derr = abs(dgot[0] - dwant[0]) / abs(dwant[0])
+    assert derr <= drag_bound, f"{storage} sphere: drag error {derr:.3e} > {drag_bound:.1e}"
