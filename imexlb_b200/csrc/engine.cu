@@ -33,6 +33,7 @@
 #include "../../include/imexlb.h"
 #include "lattice.h"
 #include "step_core.cuh"
+#include "stage_core.cuh"
 
 namespace imx {
 namespace {
@@ -40,13 +41,16 @@ namespace {
 using namespace core;
 
 struct __align__(16) EngInst {
-  StepArgs a;
+  StepArgs a;    // first member: the staged kernels copy its prefix from here
   void* buf[2];
   double* prev;  // u, v, w at the last residual check (3 n values)
   int rule;      // CaseRule
-  int bx_log2;   // tile width 2^bx_log2 threads along x
+  int bx_log2;   // tile width 2^bx_log2 threads along x (register-staged kernels)
   int parity0;   // engine step parity at admission
   int x2;        // 2-byte format with nx even: threads own x-pairs (step_cells_x2)
+  int staged;    // 2-byte format, rows staged in shared memory (stage_core.cuh)
+  int tw, th;    // cells of a tile along x and y
+  stage::Geo geo;
 };
 
 struct Tile {
@@ -59,6 +63,7 @@ struct EngArgs {
   int ntiles;
   int parity;
   int store;
+  int* err;  // set non-zero by a staged kernel that gave up waiting
 };
 
 // Population planes of one instance: plane q starts q * sq elements into the
@@ -120,27 +125,115 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
   }
 }
 
+// The persistent step over one group of staged tiles (2-byte formats with
+// rows staged in shared memory, stage_core.cuh): the single-lattice staged
+// kernel's pipeline, where each tile may belong to another instance.  With a
+// tile's rows, warp 0 copies the prefix of its instance's StepArgs into the
+// stage, so the per-cell code reads the instance's constants from shared
+// memory.
+template <Store S, Bc B, CaseRule RULE>
+__global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const EngArgs ea, const int t0,
+                                                                          const int t1) {
+  using T = typename StoreT<S>::T;
+  using namespace stage;
+  constexpr bool WRAP = B == Bc::Periodic || RULE == CaseRule::SphereStd;
+  constexpr int NS = MAX_STAGES;
+  constexpr int stage_elems = Q * (SLOT_UNITS / MAX_STAGES);
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* stages = reinterpret_cast<T*>(smem);
+  unsigned char* args = smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T);
+  uint64_t* full = reinterpret_cast<uint64_t*>(args + NS * STAGED_ARGS_BYTES);
+  uint64_t* empty = full + NS;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; ++s) {
+      bar_init(&full[s], 1);
+      bar_init(&empty[s], THREADS / 32);
+    }
+    abort_flag = 0;
+    bar_init_fence();
+  }
+  __syncthreads();
+  volatile int* abort_v = &abort_flag;
+  const int grid = gridDim.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // copies of tile t into stage sn (warp 0)
+  auto issue = [&](int t, int sn) {
+    const Tile tile = ea.tiles[t];
+    const EngInst* in = ea.inst + tile.slot;
+    const int cur = (ea.parity ^ in->parity0) & 1;
+    issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
+                        stages + sn * stage_elems, &full[sn], args + sn * STAGED_ARGS_BYTES, &in->a,
+                        static_cast<uint32_t>(STAGED_ARGS_BYTES));
+  };
+  int issued = 0;
+  if (warp == 0) {
+    for (; issued < NS - 1; ++issued) {
+      const int t = t0 + blockIdx.x + issued * grid;
+      if (t >= t1) break;
+      issue(t, issued);
+    }
+  }
+  int i = 0;
+  for (int t = t0 + blockIdx.x; t < t1; t += grid, ++i) {
+    const int s = i % NS;
+    if (warp == 0) {
+      const int tn = t + (NS - 1) * grid;
+      if (tn < t1) {
+        if (i > 0 && !__all_sync(0xffffffffu, bar_wait(&empty[(i - 1) % NS], ((i - 1) / NS) & 1u))) {
+          *abort_v = 1;
+          break;
+        }
+        issue(tn, (i + NS - 1) % NS);
+        ++issued;
+      }
+    }
+    if (!__all_sync(0xffffffffu, bar_wait(&full[s], (i / NS) & 1u))) {
+      *abort_v = 1;
+      break;
+    }
+    const Tile tile = ea.tiles[t];
+    const EngInst* in = ea.inst + tile.slot;
+    const int cur = (ea.parity ^ in->parity0) & 1;
+    const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
+    const FlatPlanes<T> pl{static_cast<const T*>(in->buf[cur]), static_cast<T*>(in->buf[1 - cur]),
+                           static_cast<int32_t>(a.sq)};
+    const Geo g = in->geo;
+    consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), tile.j0, tile.k,
+                             ea.store != 0);
+    __syncwarp();
+    if (lane == 0) bar_arrive(&empty[s]);
+    if (__any_sync(0xffffffffu, *abort_v != 0)) break;
+  }
+  if (warp == 0 && lane == 0 && *abort_v) {
+    for (int m = i; m < issued; ++m) (void)bar_wait(&full[m % NS], (m / NS) & 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && abort_flag) atomicOr(ea.err, 1);
+}
+
+inline size_t engine_staged_smem() {
+  return static_cast<size_t>(Q) * stage::SLOT_UNITS * 2 + stage::MAX_STAGES * STAGED_ARGS_BYTES +
+         16 * stage::MAX_STAGES;
+}
+
 // Residual partial sums per tile: sum |u - u_prev|^2 and sum |u|^2 over the
 // tile's cells, then u_prev = u.  Deterministic: per-tile partials are added
 // in tile order per instance afterwards.
-template <int CPT>
 __global__ void engine_resid_kernel(const EngArgs ea, double* part) {
   __shared__ double sh[2][8];
   for (int t = blockIdx.x; t < ea.ntiles; t += gridDim.x) {
     const Tile tile = ea.tiles[t];
     const EngInst& in = ea.inst[tile.slot];
-    const int bxl = in.bx_log2;
-    const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
-    const int cx = in.x2 ? 2 : 1;  // cells per thread along x
     const int k = tile.k;
     const int nx = in.a.nx, ny = in.a.ny;
+    const int tw = in.tw, th = in.th;
     const int64_t n = static_cast<int64_t>(nx) * ny * in.a.nz;
     double d2 = 0.0, n2 = 0.0;
-#pragma unroll
-    for (int c = 0; c < 2 * CPT; ++c) {
-      const int i = tile.i0 + cx * tx + (c & 1);
-      const int j = tile.j0 + ty * CPT + (c >> 1);
-      if ((c & 1) < cx && (c >> 1) < CPT && i < nx && j < ny) {
+    for (int c = threadIdx.x; c < tw * th; c += blockDim.x) {
+      const int i = tile.i0 + c % tw, j = tile.j0 + c / tw;
+      if (i < nx && j < ny) {
         const int64_t cell = i + static_cast<int64_t>(nx) * (j + static_cast<int64_t>(ny) * k);
         const double u = in.a.mu[cell], v = in.a.mv[cell], w = in.a.mw[cell];
         double* pu = in.prev + cell;
@@ -304,9 +397,11 @@ struct imexlb_engine {
   DevBuf<double> d_res;
   std::vector<int> seg_slots;
   // tile ranges of the kernel groups: group = rule (0 periodic, 1 cavity,
-  // 2 sphere) * 2 + x2
-  int group_begin[6] = {0, 0, 0, 0, 0, 0};
-  int group_end[6] = {0, 0, 0, 0, 0, 0};
+  // 2 sphere) * 3 + mode (0 one cell or y-pairs, 1 x-pairs, 2 staged rows)
+  int group_begin[9] = {};
+  int group_end[9] = {};
+  DevBuf<int> d_err;  // staged kernels' error word
+  int staged_resident = 0;  // staged blocks resident on the device
   bool dirty = true;
   int64_t gstep = 0;
   int grid = 296;
@@ -332,30 +427,42 @@ int efail(int code, const std::string& msg) { return imx::set_last_error(code, m
 
 int cpt_of(imexlb_storage s) { return s == IMEXLB_F64 ? 1 : 2; }
 
+// Wait for the engine's stream and report a staged kernel that gave up
+// waiting for its row copies (the error word is then cleared).
+int sync_checked(imexlb_engine* e) {
+  int word = 0;
+  IMX_ECUDA(cudaMemcpyAsync(&word, e->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  if (word) {
+    IMX_ECUDA(cudaMemset(e->d_err.p, 0, sizeof(int)));
+    return efail(IMEXLB_E_CUDA, "a staged step kernel gave up waiting for its row copies; instance states are invalid");
+  }
+  return IMEXLB_OK;
+}
+
+int mode_of(const EngInst& in) { return in.staged ? 2 : (in.x2 ? 1 : 0); }
+int group_of(const EngInst& in) {
+  const int rule = in.rule;
+  const int rg = rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2);
+  return rg * 3 + mode_of(in);
+}
+
 int rebuild_tiles(imexlb_engine* e) {
   if (!e->dirty) return IMEXLB_OK;
   e->h_tiles.clear();
   e->seg_slots.clear();
   std::vector<int> sb, se;
-  const int cpt = cpt_of(e->storage);
   // instances ordered by kernel group, so that each group's tiles are one range
   std::vector<int> order;
-  for (int g = 0; g < 6; ++g) {
-    for (int s = 0; s < static_cast<int>(e->slots.size()); ++s) {
-      const Slot& sl = e->slots[s];
-      if (!sl.used) continue;
-      const int rule = e->h_inst[s].rule;
-      const int rg = rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2);
-      if (rg * 2 + e->h_inst[s].x2 == g) order.push_back(s);
-    }
-  }
-  for (int g = 0; g < 6; ++g) e->group_begin[g] = e->group_end[g] = 0;
+  for (int g = 0; g < 9; ++g)
+    for (int s = 0; s < static_cast<int>(e->slots.size()); ++s)
+      if (e->slots[s].used && group_of(e->h_inst[s]) == g) order.push_back(s);
+  for (int g = 0; g < 9; ++g) e->group_begin[g] = e->group_end[g] = 0;
   int prev_group = -1;
   for (int s : order) {
     Slot& sl = e->slots[s];
-    const int rule = e->h_inst[s].rule;
-    const int g = (rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2)) * 2 +
-                  e->h_inst[s].x2;
+    const EngInst& in = e->h_inst[s];
+    const int g = group_of(in);
     if (g != prev_group) {
       e->group_begin[g] = static_cast<int>(e->h_tiles.size());
       prev_group = g;
@@ -363,12 +470,9 @@ int rebuild_tiles(imexlb_engine* e) {
     sl.seg = static_cast<int>(e->seg_slots.size());
     e->seg_slots.push_back(s);
     sb.push_back(static_cast<int>(e->h_tiles.size()));
-    const int bx = 1 << sl.bx_log2;
-    const int rows = (256 / bx) * cpt;
-    const int cols = bx * (e->h_inst[s].x2 ? 2 : 1);
     for (int k = 0; k < sl.L.nz; ++k)
-      for (int j0 = 0; j0 < sl.L.ny; j0 += rows)
-        for (int i0 = 0; i0 < sl.L.nx; i0 += cols) e->h_tiles.push_back(Tile{s, i0, j0, k});
+      for (int j0 = 0; j0 < sl.L.ny; j0 += in.th)
+        for (int i0 = 0; i0 < sl.L.nx; i0 += in.tw) e->h_tiles.push_back(Tile{s, i0, j0, k});
     se.push_back(static_cast<int>(e->h_tiles.size()));
     e->group_end[g] = static_cast<int>(e->h_tiles.size());
   }
@@ -396,16 +500,39 @@ int rebuild_tiles(imexlb_engine* e) {
   return IMEXLB_OK;
 }
 
+template <Store S>
+void set_staged_smem() {
+  const int smem = static_cast<int>(engine_staged_smem());
+  cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Periodic, CaseRule::None>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Standard, CaseRule::CavityStd>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Standard, CaseRule::SphereStd>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
 template <Store S, bool EXACT>
 cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
-  for (int g = 0; g < 6; ++g) {
+  for (int g = 0; g < 9; ++g) {
     const int t0 = e->group_begin[g], t1 = e->group_end[g];
     if (t1 <= t0) continue;
-    const int grid = std::min(e->grid, t1 - t0);
-    const int rule = g / 2;
-    const bool x2 = (g & 1) != 0;
+    const int rule = g / 3, mode = g % 3;
     if constexpr (S == Store::F16 || S == Store::BF16) {
-      if (x2) {
+      if (mode == 2) {
+        const int grid = std::min(e->staged_resident, t1 - t0);
+        const size_t smem = engine_staged_smem();
+        if (rule == 0)
+          engine_staged_kernel<S, Bc::Periodic, CaseRule::None><<<grid, stage::THREADS, smem, e->stream>>>(ea, t0, t1);
+        else if (rule == 1)
+          engine_staged_kernel<S, Bc::Standard, CaseRule::CavityStd><<<grid, stage::THREADS, smem, e->stream>>>(ea, t0,
+                                                                                                                 t1);
+        else
+          engine_staged_kernel<S, Bc::Standard, CaseRule::SphereStd><<<grid, stage::THREADS, smem, e->stream>>>(ea, t0,
+                                                                                                                 t1);
+        continue;
+      }
+      if (mode == 1) {
+        const int grid = std::min(e->grid, t1 - t0);
         if (rule == 0)
           engine_step_kernel<S, false, Bc::Periodic, CaseRule::None, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
         else if (rule == 1)
@@ -415,6 +542,7 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
         continue;
       }
     }
+    const int grid = std::min(e->grid, t1 - t0);
     if (rule == 0)
       engine_step_kernel<S, EXACT, Bc::Periodic, CaseRule::None, false><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
     else if (rule == 1)
@@ -426,7 +554,7 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
 }
 
 cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
-  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), parity, store};
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), parity, store, e->d_err.p};
   if (ea.ntiles == 0) return cudaSuccess;
   switch (e->storage) {
     case IMEXLB_F64: return e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
@@ -469,6 +597,25 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
   IMX_ECUDA(cudaGetDevice(&dev));
   IMX_ECUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   e->grid = 2 * sms;
+  IMX_ECUDA(e->d_err.reserve(1));
+  IMX_ECUDA(cudaMemset(e->d_err.p, 0, sizeof(int)));
+  if (storage == IMEXLB_F16 || storage == IMEXLB_BF16) {
+    // the staged kernels' shared memory, set once outside any capture
+    if (storage == IMEXLB_F16)
+      set_staged_smem<Store::F16>();
+    else
+      set_staged_smem<Store::BF16>();
+    int per_sm = 0;
+    if (storage == IMEXLB_F16)
+      IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, engine_staged_kernel<Store::F16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
+          engine_staged_smem()));
+    else
+      IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, engine_staged_kernel<Store::BF16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
+          engine_staged_smem()));
+    e->staged_resident = std::max(per_sm, 1) * sms;
+  }
   *out = e.release();
   return IMEXLB_OK;
 }
@@ -605,6 +752,17 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   in.bx_log2 = sl.bx_log2;
   in.parity0 = static_cast<int>(e->gstep & 1);
   in.x2 = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
+  // rows staged in shared memory where they fit a stage (and tile_bx asks
+  // for no register-staged tile width)
+  in.staged = in.x2 && d->tile_bx <= 0 && stage::make_geo(d->ny, sl.L.pitch, &in.geo) ? 1 : 0;
+  if (in.staged) {
+    in.tw = d->nx;
+    in.th = in.geo.R;
+  } else {
+    const int bx = 1 << sl.bx_log2;
+    in.th = (256 / bx) * cpt_of(e->storage);
+    in.tw = bx * (in.x2 ? 2 : 1);
+  }
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
                 e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
@@ -675,8 +833,7 @@ int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, doubl
   double* src[4] = {in.a.mu, in.a.mv, in.a.mw, in.a.mp};
   for (int c = 0; c < 4; ++c)
     if (dst[c]) IMX_ECUDA(cudaMemcpyAsync(dst[c], src[c], n * 8, cudaMemcpyDeviceToHost, e->stream));
-  IMX_ECUDA(cudaStreamSynchronize(e->stream));
-  return IMEXLB_OK;
+  return sync_checked(e);
 }
 
 int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
@@ -686,18 +843,15 @@ int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
   if (rc) return rc;
   for (int s = 0; s < n_out; ++s) out[s] = NAN;
   if (e->h_tiles.empty()) return IMEXLB_OK;
-  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), 0, 0};
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, static_cast<int>(e->h_tiles.size()), 0, 0, e->d_err.p};
   const int grid = std::min(e->grid * 2, ea.ntiles);
-  if (cpt_of(e->storage) == 1)
-    engine_resid_kernel<1><<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
-  else
-    engine_resid_kernel<2><<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
+  engine_resid_kernel<<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
   const int ns = static_cast<int>(e->seg_slots.size());
   engine_resid_reduce<<<ns, 256, 0, e->stream>>>(e->d_seg.p, e->d_seg.p + ns, e->d_part.p, e->d_res.p);
   IMX_ECUDA(cudaGetLastError());
   std::vector<double> res(2 * static_cast<size_t>(ns));
   IMX_ECUDA(cudaMemcpyAsync(res.data(), e->d_res.p, res.size() * 8, cudaMemcpyDeviceToHost, e->stream));
-  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  if (const int rc = sync_checked(e)) return rc;
   for (int g = 0; g < ns; ++g) {
     Slot& sl = e->slots[e->seg_slots[g]];
     const double d2 = res[2 * g], n2 = res[2 * g + 1];
@@ -737,8 +891,7 @@ int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_d
 
 int imexlb_engine_synchronize(imexlb_engine* e) {
   if (!e) return efail(IMEXLB_E_ARG, "null engine");
-  IMX_ECUDA(cudaStreamSynchronize(e->stream));
-  return IMEXLB_OK;
+  return sync_checked(e);
 }
 
 void imexlb_engine_destroy(imexlb_engine* e) {

@@ -138,8 +138,6 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const T* src = static_cast<const T*>(a.src);
   const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
-  const int half = g.P >> 1;
-  const int npairs = g.R * half;
 
   // the block's first NS - 1 tiles
   int issued = 0;  // tiles of this block whose copies are issued (warp 0)
@@ -171,37 +169,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       *abort_v = 1;
       break;
     }
-    const int j0 = (t % g.nty) * g.R, k = t / g.nty;
-    const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
     const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
-    if constexpr (RULE == CaseRule::CavityStd) {
-      // Pairs next to a wall take the checked path; the pairs at the x walls
-      // go last, to as few warps as possible: their bounce-back reads global
-      // memory, and a warp waits for its slowest lane.
-      const int nx2 = a.nx >> 1;
-      const int ni = nx2 > 2 ? nx2 - 2 : 0;  // interior pairs per row
-      const int ne = nx2 < 2 ? nx2 : 2;      // edge pairs per row
-      const int n_int = rv * ni, n_all = n_int + rv * ne;
-      const bool wall_plane = k == 0 || k == a.nz - 1;
-      for (int p = threadIdx.x; p < n_all; p += THREADS) {
-        if (p < n_int) {
-          const int r = p / ni, x = 2 + 2 * (p - r * ni);
-          const int j = j0 + r;
-          if (wall_plane || j == 0 || j == a.ny - 1)
-            pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
-          else
-            pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k);
-        } else {
-          const int e = p - n_int, r = e / ne, x = (e - r * ne) == 0 ? 0 : a.nx - 2;
-          pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
-        }
-      }
-    } else {
-      for (int p = threadIdx.x; p < npairs; p += THREADS) {
-        const int r = p / half, x = 2 * (p - r * half);
-        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k);
-      }
-    }
+    consume_tile<S, B, RULE>(a, pl, g, st, (t % g.nty) * g.R, t / g.nty, a.store != 0);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -55,11 +56,32 @@ struct Encoding {
 };
 
 struct StepArgs {
+  // Fields up to `src` are all that the shared-memory staged kernels read;
+  // the engine copies this prefix (STAGED_ARGS_BYTES) into shared memory
+  // with each tile.
+  int nx = 0, ny = 0, nz = 0;
+  int32_t base32 = 0, sz32 = 0, pitch32 = 0;
+  int64_t sq = 0;
+  double omega = 1;    // 1 / (tau0 + 0.5)
+  double lid_u = 0;    // standard cavity lid speed; reference lid value
+  double rho_w = 1;    // wall density of the moving-wall term
+  double p_shift = 0;  // rest pressure removed from stored values (0 for FP64)
+  double* mu = nullptr;
+  double* mv = nullptr;
+  double* mw = nullptr;
+  double* mp = nullptr;
+  const uint8_t* usr = nullptr;     // interior mask, 1 = fluid (sphere)
+  const uint32_t* links = nullptr;  // standard sphere: per-cell bit q = the link along -e_q ends in the solid
+  int near_lo[3] = {0, 0, 0};       // box of cells that have solid links
+  int near_hi[3] = {-1, -1, -1};
+  int store = 0;  // write moments this step
+  Encoding enc;
+  double feq_in[Q] = {};  // standard sphere: inlet equilibrium (deviation form)
+  // ---- not read by the staged kernels
   const void* src = nullptr;
   void* dst = nullptr;
   const void* prev = nullptr;  // ghost gather: buffer of the previous step
-  int nx = 0, ny = 0, nz = 0;
-  int64_t sq = 0, sz = 0, pitch = 0;
+  int64_t sz = 0, pitch = 0;
   int64_t base = 0;    // stored index of interior cell (0,0,0), population 0
   int64_t off[Q] = {}; // pull offset of population q relative to a cell's base index
   // plane addressing (step kernels): population q of a cell is
@@ -67,28 +89,14 @@ struct StepArgs {
   const void* srcq[Q] = {};
   void* dstq[Q] = {};
   int32_t rel[Q] = {};
-  int32_t base32 = 0, sz32 = 0, pitch32 = 0;
   double tau_half = 1; // tau0 + 0.5
-  double omega = 1;    // 1 / (tau0 + 0.5)
-  double* mu = nullptr;
-  double* mv = nullptr;
-  double* mw = nullptr;
-  double* mp = nullptr;
-  int store = 0;  // write moments this step
-  const uint8_t* usr = nullptr;  // interior mask, 1 = fluid (sphere)
   const double* inlet = nullptr; // per interior z: reference inlet velocity
-  double lid_u = 0;       // standard cavity lid speed; reference lid value
-  double rho_w = 1;       // wall density of the moving-wall term
   double inlet_u = 0;     // standard sphere inlet velocity
-  double feq_in[Q] = {};  // standard sphere: inlet equilibrium (deviation form)
-  double p_shift = 0;     // rest pressure removed from stored values (0 for FP64)
   double* drag_part = nullptr;  // standard sphere: per-block momentum-exchange partials (3 per block), or null
-  const uint32_t* links = nullptr;  // standard sphere: per-cell bit q = the link along -e_q ends in the solid
-  int near_lo[3] = {0, 0, 0};       // box of cells that have solid links
-  int near_hi[3] = {-1, -1, -1};
   int* err = nullptr;  // set non-zero by a kernel that gave up waiting (staged steps)
-  Encoding enc;
 };
+// Bytes of the StepArgs prefix the staged kernels read, rounded to 16.
+constexpr size_t STAGED_ARGS_BYTES = (offsetof(StepArgs, src) + 15) & ~static_cast<size_t>(15);
 
 // Ghost-slot plan for reference boundaries: after each step, slot tgt[n] of
 // the new buffer receives the value named by src[n]:

@@ -179,15 +179,17 @@ __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q
 
 // Issue the copies of tile (j0, k) into stage `st` (called by a whole warp;
 // lane q < 27 copies population q).  `src` is the buffer being read,
-// population q at q * a.sq.
+// population q at q * a.sq.  Lane 31 also copies `xbytes` (a multiple of
+// 16, 0 for none) from `xsrc` to `xdst` on the same mbarrier.
 template <class T, bool WRAP_YZ>
 __device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, const T* src, int j0, int k, T* st,
-                                           uint64_t* bar) {
+                                           uint64_t* bar, void* xdst = nullptr, const void* xsrc = nullptr,
+                                           uint32_t xbytes = 0) {
   const int lane = threadIdx.x & 31;
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   Run m{0, 0, 0u}, w{0, 0, 0u};
   if (lane < Q) tile_runs<WRAP_YZ>(a, g, lane, j0, k, rv, static_cast<int>(sizeof(T)), m, w);
-  uint32_t total = m.bytes + w.bytes;
+  uint32_t total = m.bytes + w.bytes + (lane == 31 ? xbytes : 0u);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
   if (lane == 0) bar_arrive_expect(bar, total);
@@ -195,17 +197,20 @@ __device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, cons
   const T* plane = src + static_cast<int64_t>(lane) * a.sq;
   if (m.bytes) bulk_g2s(st + m.dst, plane + m.src, m.bytes, bar);
   if (w.bytes) bulk_g2s(st + w.dst, plane + w.src, w.bytes, bar);
+  if (lane == 31 && xbytes) bulk_g2s(xdst, xsrc, xbytes, bar);
 }
 
 // The x-pair (x, x + 1) in tile row r of tile (j0, k), read from the staged
 // rows.  `st` is the stage as 4-byte words.  Boundary values (halfway
 // bounce-back at the cavity's walls, solid links of the sphere) are put in
-// place by a second pass that only boundary pairs take.  EDGE = false
+// place by a second pass that only boundary pairs take.  Reads only the
+// fields of `a` before StepArgs::src.  EDGE = false
 // promises that no boundary rule of the box applies to the pair:
 // 2 <= x < nx - 2 and, for the cavity, no wall row or plane around it.
 template <Store S, Bc B, CaseRule RULE, bool EDGE, class P>
 __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
-                                                const int x, const int r, const int j0, const int k) {
+                                                const int x, const int r, const int j0, const int k,
+                                                const bool store) {
   const int j = j0 + r;
   const int row = (r * g.P) >> 1;  // word offset of tile row r in a slot
   const int pw = row + (x >> 1);
@@ -284,7 +289,44 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
     }
   }
   const bool lid = RULE == CaseRule::CavityStd && k == a.nz - 1;
-  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1);
+  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store);
+}
+
+// The cells of tile (j0, k) from stage `st`, shared by the block's threads.
+// For the cavity, pairs next to a wall take the checked path, and the pairs
+// at the x walls go last, to as few warps as possible: their bounce-back
+// reads global memory, and a warp waits for its slowest lane.
+template <Store S, Bc B, CaseRule RULE, class P>
+__device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
+                                             const int j0, const int k, const bool store) {
+  const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
+  if constexpr (RULE == CaseRule::CavityStd) {
+    const int nx2 = a.nx >> 1;
+    const int ni = nx2 > 2 ? nx2 - 2 : 0;  // interior pairs per row
+    const int ne = nx2 < 2 ? nx2 : 2;      // edge pairs per row
+    const int n_int = rv * ni, n_all = n_int + rv * ne;
+    const bool wall_plane = k == 0 || k == a.nz - 1;
+    for (int p = threadIdx.x; p < n_all; p += THREADS) {
+      if (p < n_int) {
+        const int r = p / ni, x = 2 + 2 * (p - r * ni);
+        const int j = j0 + r;
+        if (wall_plane || j == 0 || j == a.ny - 1)
+          pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+        else
+          pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store);
+      } else {
+        const int e = p - n_int, r = e / ne, x = (e - r * ne) == 0 ? 0 : a.nx - 2;
+        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+      }
+    }
+  } else {
+    const int half = g.P >> 1;
+    const int npairs = g.R * half;
+    for (int p = threadIdx.x; p < npairs; p += THREADS) {
+      const int r = p / half, x = 2 * (p - r * half);
+      if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+    }
+  }
 }
 
 }  // namespace stage

@@ -578,11 +578,11 @@ __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { retu
 // e = c_q . u and p~ = sum d_q / 3 = p - p_shift, since the shift's own
 // equilibrium cancels (sum w_q = 1, sum w_q c_q = 0).  The moments take
 // d_q = g_q w_q / unit.  live0 / live1: the cell is fluid (a solid cell's
-// values are left as they are).
+// values are left as they are); store: write the moments.
 template <Store S, CaseRule RULE, class P>
 __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
-                                                const bool live0, const bool live1) {
+                                                const bool live0, const bool live1, const bool store) {
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
   [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
@@ -612,7 +612,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
   case_rules<RULE>(a, x0, k, c0, u.x, v.x, w.x, p.x);
   case_rules<RULE>(a, x0 + 1, k, c0 + 1, u.y, v.y, w.y, p.y);
-  if (a.store) {
+  if (store) {
     a.mu[c0] = live0 ? u.x : 0.f;
     a.mv[c0] = live0 ? v.x : 0.f;
     a.mw[c0] = live0 ? w.x : 0.f;
@@ -766,7 +766,7 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       live0 = a.usr[c0] != 0;
       live1 = a.usr[c0 + 1] != 0;
     }
-    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1);
+    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store);
   }
 }
 

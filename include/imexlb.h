@@ -222,7 +222,8 @@ typedef struct imexlb_instance_desc {
   int nx, ny, nz;
   double tau0, rho0, u0;  /* as imexlb_params */
   double lid_u, inlet_u, sphere_d, sphere_c[3];  /* 0 = defaults (u0, u0, nx/24, (nx/4, ny/2, nz/2)) */
-  int tile_bx; /* threads along x per tile (power of two, 8..256); 0 = default */
+  int tile_bx; /* threads along x per tile (power of two, 8..256); 0 = default (2-byte formats: whole rows
+                  staged in shared memory where a row fits) */
 } imexlb_instance_desc;
 
 typedef struct imexlb_engine_stats {

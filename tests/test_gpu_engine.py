@@ -70,7 +70,7 @@ def test_instances_match_single_lattices(api, storage, arith):
 
 def test_tile_widths_do_not_change_results(api):
     outs = []
-    for bx in (8, 16, 32, 64, 128):
+    for bx in (0, 8, 16, 32, 64, 128):  # 0: rows staged in shared memory
         with api.Engine(storage="f16", budget_bytes=1 << 28, max_instances=2) as eng:
             s = eng.add(api.instance_desc("cavity", 40, 24, 20, 0.03, 1.0, 0.1, lid_u=0.1, tile_bx=bx))
             eng.step(30)
@@ -109,12 +109,12 @@ def test_budget_admission_and_residuals(api):
 ])
 def test_staged_rows_match_register_path(api, storage, case, n, kw):
     """A single 2-byte lattice with standard or periodic boundaries runs the
-    shared-memory staged kernel; the engine runs the register-staged x-pair
-    kernel.  Both share the per-cell arithmetic, so the fields agree bit for
-    bit."""
+    shared-memory staged kernel; an engine instance given a tile width runs
+    the register-staged x-pair kernel.  Both share the per-cell arithmetic,
+    so the fields agree bit for bit."""
     tau, u0, steps = 0.03, 0.05, 40
     with api.Engine(storage=storage, arith="fast", budget_bytes=1 << 30, max_instances=2) as eng:
-        s = eng.add(api.instance_desc(case, *n, tau, 1.0, u0, **kw))
+        s = eng.add(api.instance_desc(case, *n, tau, 1.0, u0, tile_bx=32, **kw))
         eng.step(steps)
         got = eng.fields(s)
     want = alone(api, case, n, tau, u0, kw, steps, storage, "fast")
