@@ -76,6 +76,16 @@ WORKLOADS = {
                            u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
     "sphere768-f64": dict(case="sphere", bc="standard", storage="f64", arith="fast", n=(768, 192, 192), Re=100,
                           u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
+    # batched solves: 256 seeded TGV / cavity instances (imexlb_b200.batch) in
+    # one engine; case/n/R/Re/u0 name the instance the CPU baseline times
+    "batched256-f16": dict(kind="batch", storage="f16", arith="fast", count=256, case="cavity", bc="standard",
+                           n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
+    "batched256-bf16": dict(kind="batch", storage="bf16", arith="fast", count=256, case="cavity", bc="standard",
+                            n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
+    "batched256-f32": dict(kind="batch", storage="f32", arith="fast", count=256, case="cavity", bc="standard",
+                           n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
+    "batched256-f64": dict(kind="batch", storage="f64", arith="fast", count=256, case="cavity", bc="standard",
+                           n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
 }
 DEFAULT_WORKLOAD = "cavity128-f64"
 
@@ -205,6 +215,98 @@ def reference_arm(args, w, name, rank, world):
     return 0
 
 
+def bench_batch(args, w, name, cpu) -> int:
+    """The batched workload: all instances advance together in one engine
+    (persistent launches per kernel group, two steps per graph replay)."""
+    import numpy as np
+    import torch
+
+    from imexlb_b200 import api, batch, tune
+
+    specs = batch.batch_specs(w["count"])
+    cells = batch.total_cells(specs)
+    tiles = tune.tiles_for(specs, w["storage"], cache=args.tune_cache)
+    stream = torch.cuda.Stream()
+    budget = batch.budget_for(specs, w["storage"])
+    with torch.cuda.stream(stream):
+        eng = api.Engine(storage=w["storage"], arith=w["arith"], budget_bytes=budget, max_instances=len(specs),
+                         stream=stream.cuda_stream)
+        slots = batch.add_all(eng, specs, tiles)
+        eng.step(args.warmup)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(torch.cuda.current_device())
+        sampler.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        eng.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        clocks = sampler.stop()
+        ms = ev0.elapsed_time(ev1)
+        stats = eng.stats()
+        fields = [eng.fields(s) for s in slots] if args.check_error else None
+        eng.close()
+    value = cells * args.steps / (ms * 1e-3) / 1e6
+
+    # end to end: admission from host (initial fields uploaded), the steps,
+    # every instance's u, v, w, p read back into pinned host memory
+    pinned = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        eng = api.Engine(storage=w["storage"], arith=w["arith"], budget_bytes=budget, max_instances=len(specs),
+                         stream=stream.cuda_stream)
+        slots = batch.add_all(eng, specs, tiles)
+        eng.step(args.steps)
+        for s, sp in zip(slots, specs):
+            shp = (sp.edge,) * 3
+            if shp not in pinned:
+                pinned[shp] = {k: torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
+            eng.fields(s, out=pinned[shp])
+        eng.close()
+    e2e_s = time.perf_counter() - t0
+    e2e = cells * args.steps / e2e_s / 1e6
+
+    errs = None
+    if args.check_error:
+        # the timed run took warm-up + timed steps: the FP64 run takes as many
+        ref = batch.run(specs, "f64", args.warmup + args.steps, fields=True)
+        errs = batch.error_report(specs, fields, ref["fields"])
+
+    peaks = load_peaks()
+    bpv = api.BYTES_PER_VALUE[w["storage"]]
+    step_ms = ms / args.steps
+    achieved = 2 * 27 * bpv * cells / (step_ms * 1e-3) / 1e9
+    groups = len({(s.case, tiles.get(tune.key_of(w["storage"], s.case, (s.edge,) * 3), 0) == 0) for s in specs})
+    line = {
+        "metric": "D3Q27 MLUPS (aggregate over the batch)", "value": value, "unit": "MLUPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
+        "data": "synthetic: 256 seeded instances (analytic initial and boundary conditions)",
+        "config": {"workload": name, "instances": len(specs), "cells": cells, "storage": w["storage"],
+                   "mix": "TGV / lid-driven cavity 50/50, edge in {24..128}, Re log-uniform [50, 1000], U0 = 0.05",
+                   "seed": batch.BATCH_SEED, "tiles": "autotuned per (edge, case, storage)",
+                   "parallelism": "single GPU, one engine",
+                   "l2": f"inputs larger than L2 (distribution buffers {2 * 27 * bpv * cells / 1e9:.1f} GB)"},
+        "roofline": {"bound": "hbm", "kernel": "engine step launches (all kernel groups of one step)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
+                     "bytes_per_cell_update": 2 * 27 * bpv},
+        "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * cells / args.steps,
+                "d2h_bytes_per_step": 4 * 8 * cells / args.steps, "seconds": e2e_s},
+        "gpu_launches": args.steps * groups,
+        "clocks": clocks,
+        "cpu_baseline": ({"value": cpu["value"], "unit": "MLUPS", "cores": cpu["cores"], "kind": cpu["kind"],
+                          "sample": cpu["sample"] + " (the batch's median-size cavity instance, 64^3)"}
+                         if cpu else None),
+        "check": {"engine_tiles": stats["tiles"],
+                  "per_instance_velocity_l2_vs_fp64": errs},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,6 +316,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--check-error", action="store_true", help="batched workloads: per-instance error vs FP64")
+    ap.add_argument("--tune-cache", default=None, help="batched workloads: autotuner cache (JSON)")
     args = ap.parse_args(argv)
     w = WORKLOADS[args.workload]
     name = args.workload
@@ -229,6 +333,13 @@ def main(argv=None) -> int:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(w, args.cpu_seconds)
+
+    if w.get("kind") == "batch":
+        # one GPU: ranks other than 0 have no work in this workload
+        import torch
+
+        torch.cuda.set_device(local)
+        return bench_batch(args, w, name, cpu) if rank == 0 else 0
 
     import numpy as np
     import torch

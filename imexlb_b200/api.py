@@ -335,9 +335,11 @@ class Engine:
     def synchronize(self):
         _check(self.lib.imexlb_engine_synchronize(self.h))
 
-    def fields(self, slot: int) -> dict:
+    def fields(self, slot: int, out: dict | None = None) -> dict:
+        """u, v, w, p of one instance after the last step, each (nz, ny, nx)."""
         nx, ny, nz = self.shapes[slot]
-        out = {k: np.empty((nz, ny, nx)) for k in ("u", "v", "w", "p")}
+        if out is None:
+            out = {k: np.empty((nz, ny, nx)) for k in ("u", "v", "w", "p")}
         _check(self.lib.imexlb_engine_fields(self.h, slot, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]),
                                              _ptr(out["p"])))
         return out

@@ -1,0 +1,182 @@
+"""Batched solves: many independent lattices advanced together by the engine.
+
+The reference runs one lattice per process and has no batch mode; this is
+the batched configuration of this project: 256 independent instances drawn
+from a fixed seed, each a Taylor-Green vortex (periodic) or a lid-driven
+cavity (standard boundaries, moving lid) with equal odds, a cubic edge drawn
+uniformly from {24, 32, 48, 64, 96, 128}, Re log-uniform in [50, 1000] and
+U0 = u_w = 0.05.  tau0 follows the reference's System::tau
+(tgv/src/System.cpp:21, lid_driven_cavity/src/System.cpp:19):
+tau0 = 3 nu with nu = U0 (N / 2 pi) / Re for the vortex (pi = 3.1415926 as
+there) and nu = u_w N / Re for the cavity; the relaxation time is
+tau0 + 0.5.
+
+All instances live in one engine (imexlb_engine_*) and advance one time step
+per persistent launch per kernel group, two steps per CUDA-graph replay,
+with per-instance tile shapes from the autotuner (imexlb_b200.tune).
+
+    python -m imexlb_b200.batch --storage f16 --steps 2000 [--check]
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import math
+import time
+
+import numpy as np
+
+from . import api
+
+BATCH_SEED = 20240607
+EDGES = (24, 32, 48, 64, 96, 128)
+PI_REF = 3.1415926
+
+
+@dataclasses.dataclass(frozen=True)
+class Spec:
+    case: str    # "tgv" or "cavity"
+    edge: int    # cubic lattice edge
+    Re: float
+    u: float     # U0 (vortex) or lid speed (cavity)
+
+    @property
+    def tau0(self) -> float:
+        if self.case == "tgv":
+            return 3.0 * self.u * (self.edge / 2.0 / PI_REF) / self.Re
+        return 3.0 * self.u * self.edge / self.Re
+
+    @property
+    def cells(self) -> int:
+        return self.edge ** 3
+
+    def desc(self, tile_bx: int = 0) -> api.InstanceDesc:
+        kw = dict(lid_u=self.u) if self.case == "cavity" else {}
+        return api.instance_desc(self.case, self.edge, self.edge, self.edge, self.tau0, 1.0, self.u,
+                                 tile_bx=tile_bx, **kw)
+
+
+def batch_specs(count: int = 256, seed: int = BATCH_SEED, u: float = 0.05) -> list[Spec]:
+    """The seeded instance list of the batched configuration."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        case = "tgv" if rng.random() < 0.5 else "cavity"
+        edge = int(rng.choice(EDGES))
+        Re = float(math.exp(rng.uniform(math.log(50.0), math.log(1000.0))))
+        out.append(Spec(case, edge, Re, u))
+    return out
+
+
+def total_cells(specs) -> int:
+    return sum(s.cells for s in specs)
+
+
+def budget_for(specs, storage: str, slack: float = 1.05) -> int:
+    need = sum(api.instance_bytes(storage, s.desc()) for s in specs)
+    return int(need * slack) + (64 << 20)
+
+
+def velocity_l2(got: dict, want: dict) -> float:
+    """sqrt(sum |u - u_ref|^2 / sum |u_ref|^2) over the lattice."""
+    num = sum(float(((got[k] - want[k]) ** 2).sum()) for k in "uvw")
+    den = sum(float((want[k] ** 2).sum()) for k in "uvw")
+    return math.sqrt(num / den) if den > 0 else math.sqrt(num)
+
+
+def add_all(eng: api.Engine, specs, tiles: dict | None = None) -> list[int]:
+    """Admit every instance; `tiles` maps tune keys to tile_bx."""
+    from . import tune
+
+    slots = []
+    for s in specs:
+        bx = tiles.get(tune.key_of(eng.storage, s.case, (s.edge,) * 3), 0) if tiles else 0
+        slots.append(eng.add(s.desc(tile_bx=bx)))
+    return slots
+
+
+def run(specs, storage: str, steps: int, arith: str = "fast", tiles: dict | None = None, fields: bool = True,
+        warmup: int = 0) -> dict:
+    """Advance the whole batch `steps` steps; device-timed MLUPS and, when
+    asked, every instance's u, v, w, p afterwards."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    with api.Engine(storage=storage, arith=arith, budget_bytes=budget_for(specs, storage),
+                    max_instances=len(specs), stream=stream.cuda_stream) as eng:
+        slots = add_all(eng, specs, tiles)
+        if warmup:
+            eng.step(warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out = [eng.fields(s) for s in slots] if fields else None
+    cells = total_cells(specs)
+    return dict(mlups=cells * steps / (ms * 1e-3) / 1e6, ms=ms, cells=cells, steps=steps, fields=out)
+
+
+def errors_against(fields, ref_fields) -> list[float]:
+    return [velocity_l2(g, w) for g, w in zip(fields, ref_fields)]
+
+
+def finite(f: dict) -> bool:
+    return all(bool(np.isfinite(f[k]).all()) for k in "uvw")
+
+
+def error_report(specs, fields, ref_fields, worst: int = 5) -> dict:
+    """Per-instance relative velocity L2 against the FP64 run.  Instances
+    whose FP64 run itself diverged (BGK past its stability limit: the batch
+    draws Re up to 1000 on edges down to 24, tau - 1/2 down to 7e-4) have no
+    reference and are counted apart."""
+    errs, bad_ref, bad_run = [], [], []
+    for i, (s, g, w) in enumerate(zip(specs, fields, ref_fields)):
+        if not finite(w):
+            bad_ref.append(i)
+            continue
+        if not finite(g):
+            bad_run.append(i)
+            continue
+        errs.append((velocity_l2(g, w), i))
+    errs.sort(reverse=True)
+    vals = np.array([e for e, _ in errs]) if errs else np.array([np.nan])
+    return {
+        "compared": len(errs), "fp64_diverged": len(bad_ref), "diverged_only_here": len(bad_run),
+        "max": float(vals.max()), "p95": float(np.percentile(vals, 95)), "median": float(np.median(vals)),
+        "within_1e-3": int((vals <= 1e-3).sum()),
+        "worst": [dict(err=e, case=specs[i].case, edge=specs[i].edge, Re=round(specs[i].Re, 1),
+                       tau=round(specs[i].tau0 + 0.5, 6)) for e, i in errs[:worst]],
+        "fp64_diverged_instances": [dict(case=specs[i].case, edge=specs[i].edge, Re=round(specs[i].Re, 1))
+                                    for i in bad_ref[:worst]],
+    }
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--storage", default="f16", choices=sorted(api.STORAGES))
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--count", type=int, default=256)
+    ap.add_argument("--check", action="store_true", help="also run FP64 and report per-instance errors")
+    ap.add_argument("--tune-cache", default=None)
+    args = ap.parse_args(argv)
+    from . import tune
+
+    specs = batch_specs(args.count)
+    tiles = tune.tiles_for(specs, args.storage, cache=args.tune_cache)
+    t0 = time.perf_counter()
+    res = run(specs, args.storage, args.steps, tiles=tiles, fields=args.check)
+    line = dict(storage=args.storage, instances=len(specs), cells=res["cells"], steps=args.steps,
+                mlups=res["mlups"], device_ms=res["ms"], wall_s=time.perf_counter() - t0)
+    if args.check:
+        ref = run(specs, "f64", args.steps, fields=True)
+        line.update(fp64_mlups=ref["mlups"], errors=error_report(specs, res["fields"], ref["fields"]))
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
