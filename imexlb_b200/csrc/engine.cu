@@ -856,7 +856,9 @@ int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
     Slot& sl = e->slots[e->seg_slots[g]];
     const double d2 = res[2 * g], n2 = res[2 * g + 1];
     out[e->seg_slots[g]] = !sl.have_prev ? INFINITY : (n2 > 0 ? std::sqrt(d2 / n2) : (d2 > 0 ? INFINITY : 0.0));
-    if (!std::isfinite(d2) || !std::isfinite(n2)) out[e->seg_slots[g]] = NAN;
+    // NaN: the velocity field is not finite (before the first check the
+    // previous field is not yet defined, so only the current one counts)
+    if (!std::isfinite(n2) || (sl.have_prev && !std::isfinite(d2))) out[e->seg_slots[g]] = NAN;
     sl.have_prev = true;
   }
   return IMEXLB_OK;

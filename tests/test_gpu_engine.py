@@ -120,3 +120,24 @@ def test_staged_rows_match_register_path(api, storage, case, n, kw):
     want = alone(api, case, n, tau, u0, kw, steps, storage, "fast")
     for k in "uvwp":
         assert np.array_equal(got[k], want[k]), (case, k, np.abs(got[k] - want[k]).max())
+
+
+def test_first_residual_after_admission_is_infinite(api):
+    """An instance admitted into memory another instance used before reads
+    +inf (no previous field yet) on its first residual check, not NaN."""
+    d = api.instance_desc("tgv", 32, 32, 32, 0.02, 1.0, 0.05)
+    with api.Engine(storage="f16", budget_bytes=api.instance_bytes("f16", d) + (8 << 20), max_instances=2) as eng:
+        a = eng.add(d)
+        eng.step(20)
+        eng.residuals()
+        eng.step(20)
+        r = eng.residuals()
+        assert 0.0 < r[a] < 1.0
+        eng.remove(a)
+        b = eng.add(d)  # same arena bytes, previous field left over
+        eng.step(5)
+        r = eng.residuals()
+        assert np.isinf(r[b])
+        eng.step(5)
+        r = eng.residuals()
+        assert 0.0 < r[b] < 1.0
