@@ -78,10 +78,12 @@ class EngineStats(ctypes.Structure):
 EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imexlb_initialize", "imexlb_step",
            "imexlb_get_fields", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
            "imexlb_reduce_fields_noalloc", "imexlb_steps_taken",
-           "imexlb_footprint", "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
+           "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
+           "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
            "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_remove",
            "imexlb_engine_step", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
-           "imexlb_engine_instance_bytes", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
+           "imexlb_engine_instance_bytes", "imexlb_engine_checkpoint_size", "imexlb_engine_checkpoint_save",
+           "imexlb_engine_restore", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
 
 _LIB = None
 
@@ -109,6 +111,13 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_steps_taken.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.imexlb_footprint.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(d)]
     lib.imexlb_ghost_plan.argtypes = [i, i, i, i, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.imexlb_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    lib.imexlb_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
+    lib.imexlb_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
+    lib.imexlb_engine_checkpoint_size.argtypes = [vp, i, ctypes.POINTER(ctypes.c_size_t)]
+    lib.imexlb_engine_checkpoint_save.argtypes = [vp, i, vp, ctypes.c_size_t]
+    lib.imexlb_engine_restore.argtypes = [vp, ctypes.POINTER(InstanceDesc), vp, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_int)]
     lib.imexlb_profile.argtypes = [vp, i]
     lib.imexlb_profile_read.argtypes = [vp, ctypes.POINTER(KernelTimes)]
     lib.imexlb_synchronize.argtypes = [vp]
@@ -240,6 +249,18 @@ class LBM:
         _check(self.lib.imexlb_reduce(self.h, REDUCE[kind], out))
         return out[0] if kind != "drag" else (out[0], out[1], out[2])
 
+    def checkpoint(self) -> bytes:
+        """The lattice's state (both buffers, moments, step count) as bytes."""
+        n = ctypes.c_size_t()
+        _check(self.lib.imexlb_checkpoint_size(self.h, ctypes.byref(n)))
+        buf = (ctypes.c_char * n.value)()
+        _check(self.lib.imexlb_checkpoint_save(self.h, buf, n.value))
+        return bytes(buf)
+
+    def restore(self, data: bytes):
+        """Continue from a checkpoint of a lattice with the same parameters."""
+        _check(self.lib.imexlb_checkpoint_load(self.h, data, len(data)))
+
     def steps_taken(self) -> int:
         s = ctypes.c_int64()
         _check(self.lib.imexlb_steps_taken(self.h, ctypes.byref(s)))
@@ -322,6 +343,21 @@ class Engine:
         if rc == 4:
             return None
         _check(rc)
+        self.shapes[slot.value] = (desc.nx, desc.ny, desc.nz)
+        return slot.value
+
+    def checkpoint(self, slot: int) -> bytes:
+        """One instance's state (current buffer, moments, step count)."""
+        n = ctypes.c_size_t()
+        _check(self.lib.imexlb_engine_checkpoint_size(self.h, slot, ctypes.byref(n)))
+        buf = (ctypes.c_char * n.value)()
+        _check(self.lib.imexlb_engine_checkpoint_save(self.h, slot, buf, n.value))
+        return bytes(buf)
+
+    def restore(self, desc: InstanceDesc, data: bytes) -> int:
+        """Admit an instance from a checkpoint (same descriptor and storage)."""
+        slot = ctypes.c_int()
+        _check(self.lib.imexlb_engine_restore(self.h, ctypes.byref(desc), data, len(data), ctypes.byref(slot)))
         self.shapes[slot.value] = (desc.nx, desc.ny, desc.nz)
         return slot.value
 

@@ -891,6 +891,84 @@ int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_d
   return IMEXLB_OK;
 }
 
+static CheckpointHeader instance_header(const imexlb_engine* e, const Slot& sl) {
+  CheckpointHeader c{};
+  std::memcpy(c.magic, "IMXLBCK1", 8);
+  c.kind = 1;
+  c.kase = sl.d.kase;
+  c.storage = e->storage;
+  c.bc = IMEXLB_BC_STANDARD;
+  c.nx = sl.d.nx;
+  c.ny = sl.d.ny;
+  c.nz = sl.d.nz;
+  c.cur = 0;
+  c.steps = sl.steps;
+  c.buf_bytes = sl.L.bytes();
+  c.nbuf = 1;
+  c.mom_bytes = 4 * static_cast<uint64_t>(sl.ncell) * sizeof(double);
+  c.tau0 = sl.d.tau0;
+  return c;
+}
+
+int imexlb_engine_checkpoint_size(const imexlb_engine* e, int slot, size_t* bytes) {
+  if (!e || !bytes || slot < 0 || slot >= static_cast<int>(e->slots.size()) || !e->slots[slot].used)
+    return efail(IMEXLB_E_ARG, "no such instance");
+  const Slot& sl = e->slots[slot];
+  *bytes = sizeof(CheckpointHeader) + sl.L.bytes() + 4 * static_cast<size_t>(sl.ncell) * sizeof(double);
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_checkpoint_save(imexlb_engine* e, int slot, void* host, size_t bytes) {
+  size_t need = 0;
+  if (const int rc = imexlb_engine_checkpoint_size(e, slot, &need)) return rc;
+  if (!host || bytes < need) return efail(IMEXLB_E_ARG, "checkpoint buffer too small (see imexlb_engine_checkpoint_size)");
+  if (const int rc = sync_checked(e)) return rc;
+  const Slot& sl = e->slots[slot];
+  const EngInst& in = e->h_inst[slot];
+  const int cur = static_cast<int>((e->gstep & 1) ^ in.parity0) & 1;  // the buffer the next step reads
+  const CheckpointHeader c = instance_header(e, sl);
+  char* p = static_cast<char*>(host);
+  std::memcpy(p, &c, sizeof c);
+  p += sizeof c;
+  IMX_ECUDA(cudaMemcpyAsync(p, in.buf[cur], c.buf_bytes, cudaMemcpyDeviceToHost, e->stream));
+  p += c.buf_bytes;
+  IMX_ECUDA(cudaMemcpyAsync(p, in.a.mu, c.mom_bytes, cudaMemcpyDeviceToHost, e->stream));  // u, v, w, p contiguous
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_restore(imexlb_engine* e, const imexlb_instance_desc* d, const void* host, size_t bytes,
+                          int* slot_out) {
+  if (!e || !d || !host || !slot_out) return efail(IMEXLB_E_ARG, "null argument");
+  if (bytes < sizeof(CheckpointHeader)) return efail(IMEXLB_E_ARG, "not a checkpoint (too short)");
+  CheckpointHeader c;
+  std::memcpy(&c, host, sizeof c);
+  if (std::memcmp(c.magic, "IMXLBCK1", 8) != 0 || c.kind != 1) return efail(IMEXLB_E_ARG, "not an engine checkpoint");
+  if (c.kase != d->kase || c.storage != e->storage || c.nx != d->nx || c.ny != d->ny || c.nz != d->nz ||
+      c.tau0 != d->tau0 || c.nbuf != 1 || c.steps < 0)
+    return efail(IMEXLB_E_ARG, "checkpoint belongs to an instance with other parameters");
+  int slot = -1;
+  if (const int rc = imexlb_engine_add(e, d, &slot)) return rc;
+  Slot& sl = e->slots[slot];
+  const CheckpointHeader want = instance_header(e, sl);
+  if (c.buf_bytes != want.buf_bytes || c.mom_bytes != want.mom_bytes ||
+      bytes < sizeof c + c.buf_bytes + c.mom_bytes) {
+    imexlb_engine_remove(e, slot);
+    return efail(IMEXLB_E_ARG, "checkpoint truncated or of another layout");
+  }
+  EngInst& in = e->h_inst[slot];
+  // at admission the next step reads buf[0] (parity0 = engine step parity)
+  const char* p = static_cast<const char*>(host) + sizeof c;
+  IMX_ECUDA(cudaMemcpyAsync(in.buf[0], p, c.buf_bytes, cudaMemcpyHostToDevice, e->stream));
+  p += c.buf_bytes;
+  IMX_ECUDA(cudaMemcpyAsync(in.a.mu, p, c.mom_bytes, cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  sl.steps = c.steps;
+  sl.have_prev = false;
+  *slot_out = slot;
+  return IMEXLB_OK;
+}
+
 int imexlb_engine_synchronize(imexlb_engine* e) {
   if (!e) return efail(IMEXLB_E_ARG, "null engine");
   return sync_checked(e);

@@ -823,6 +823,78 @@ int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out) {
   return IMEXLB_OK;
 }
 
+int imexlb_checkpoint_size(const imexlb_lattice* h, size_t* bytes) {
+  if (!h || !bytes) return fail(IMEXLB_E_ARG, "null argument");
+  *bytes = sizeof(CheckpointHeader) + h->buf[0].n + h->buf[1].n + h->mom.n * sizeof(double);
+  return IMEXLB_OK;
+}
+
+static CheckpointHeader lattice_header(const imexlb_lattice* h) {
+  CheckpointHeader c{};
+  std::memcpy(c.magic, "IMXLBCK1", 8);
+  c.kind = 0;
+  c.kase = h->P.kase;
+  c.storage = h->P.storage;
+  c.bc = h->P.bc;
+  c.nx = h->P.nx;
+  c.ny = h->P.ny;
+  c.nz = h->P.nz;
+  c.cur = h->cur;
+  c.steps = h->steps;
+  c.buf_bytes = h->buf[0].n;
+  c.nbuf = 2;
+  c.mom_bytes = h->mom.n * sizeof(double);
+  c.tau0 = h->P.tau0;
+  return c;
+}
+
+int imexlb_checkpoint_save(imexlb_lattice* h, void* host, size_t bytes) {
+  if (!h || !host) return fail(IMEXLB_E_ARG, "null argument");
+  size_t need = 0;
+  imexlb_checkpoint_size(h, &need);
+  if (bytes < need) return fail(IMEXLB_E_ARG, "checkpoint buffer too small (see imexlb_checkpoint_size)");
+  if (const int rc = sync_checked(h)) return rc;
+  const CheckpointHeader c = lattice_header(h);
+  char* p = static_cast<char*>(host);
+  std::memcpy(p, &c, sizeof c);
+  p += sizeof c;
+  for (int b = 0; b < 2; ++b) {
+    IMX_CUDA(cudaMemcpyAsync(p, h->buf[b].p, h->buf[b].n, cudaMemcpyDeviceToHost, h->stream));
+    p += h->buf[b].n;
+  }
+  IMX_CUDA(cudaMemcpyAsync(p, h->mom.p, c.mom_bytes, cudaMemcpyDeviceToHost, h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  return IMEXLB_OK;
+}
+
+int imexlb_checkpoint_load(imexlb_lattice* h, const void* host, size_t bytes) {
+  if (!h || !host) return fail(IMEXLB_E_ARG, "null argument");
+  if (bytes < sizeof(CheckpointHeader)) return fail(IMEXLB_E_ARG, "not a checkpoint (too short)");
+  CheckpointHeader c;
+  std::memcpy(&c, host, sizeof c);
+  const CheckpointHeader want = lattice_header(h);
+  if (std::memcmp(c.magic, want.magic, 8) != 0 || c.kind != 0) return fail(IMEXLB_E_ARG, "not a lattice checkpoint");
+  if (c.kase != want.kase || c.storage != want.storage || c.bc != want.bc || c.nx != want.nx || c.ny != want.ny ||
+      c.nz != want.nz || c.buf_bytes != want.buf_bytes || c.nbuf != 2 || c.mom_bytes != want.mom_bytes ||
+      c.tau0 != want.tau0 || (c.cur != 0 && c.cur != 1) || c.steps < 0)
+    return fail(IMEXLB_E_ARG, "checkpoint belongs to a lattice with other parameters");
+  size_t need = 0;
+  imexlb_checkpoint_size(h, &need);
+  if (bytes < need) return fail(IMEXLB_E_ARG, "checkpoint truncated");
+  if (const int rc = sync_checked(h)) return rc;
+  const char* p = static_cast<const char*>(host) + sizeof c;
+  for (int b = 0; b < 2; ++b) {
+    IMX_CUDA(cudaMemcpyAsync(h->buf[b].p, p, h->buf[b].n, cudaMemcpyHostToDevice, h->stream));
+    p += h->buf[b].n;
+  }
+  IMX_CUDA(cudaMemcpyAsync(h->mom.p, p, c.mom_bytes, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  h->cur = c.cur;
+  h->steps = c.steps;
+  h->have_prev = false;
+  return IMEXLB_OK;
+}
+
 int imexlb_synchronize(imexlb_lattice* h) {
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
   return sync_checked(h);

@@ -123,6 +123,21 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
                  std::vector<double>& U, std::vector<double>& V, std::vector<double>& W, std::vector<double>& Pf);
 void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]);
 
+// Header of a checkpoint (imexlb_checkpoint_*, imexlb_engine_checkpoint_*):
+// the state follows it as nbuf distribution buffers of buf_bytes each, then
+// the moments (mom_bytes).
+struct CheckpointHeader {
+  char magic[8];       // "IMXLBCK1"
+  int32_t kind;        // 0 lattice, 1 engine instance
+  int32_t kase, storage, bc;
+  int32_t nx, ny, nz, cur;
+  int64_t steps;
+  uint64_t buf_bytes, nbuf, mom_bytes;
+  double tau0;
+  char pad[48];
+};
+static_assert(sizeof(CheckpointHeader) == 128, "checkpoint header layout");
+
 // Record the calling thread's last error message (imexlb_last_error) and
 // return `code`.
 int set_last_error(int code, const std::string& msg);

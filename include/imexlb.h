@@ -169,6 +169,17 @@ int imexlb_steps_taken(const imexlb_lattice* h, int64_t* steps);
 /* Device bytes the lattice holds, and HBM bytes one step moves by design. */
 int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* bytes_per_cell_update);
 
+/* Checkpoint / restore of a lattice's state: both distribution buffers, the
+ * moments of the last step and the step count, in a host buffer of
+ * imexlb_checkpoint_size bytes (a small header names the case, storage,
+ * boundaries and extents).  Restoring into a lattice created with the same
+ * parameters continues bit for bit as if it had never stopped; the residual
+ * history starts over.  No counterpart in the reference, which has no
+ * restart files; used to pre-empt and resume served solves. */
+int imexlb_checkpoint_size(const imexlb_lattice* h, size_t* bytes);
+int imexlb_checkpoint_save(imexlb_lattice* h, void* host, size_t bytes);
+int imexlb_checkpoint_load(imexlb_lattice* h, const void* host, size_t bytes);
+
 /* Host-only: the ghost-slot plan that reference boundaries apply after every
  * step (the reference's unpack + boundary passes at one rank, resolved into
  * one copy per slot; lid_driven_cavity/src/lbm.cpp:231-301,
@@ -250,6 +261,15 @@ int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out);
 int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st);
 /* Arena bytes one instance needs in a given storage format. */
 int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes);
+/* Pre-emption of one engine instance: its state (current distribution
+ * buffer, moments, step count) into a host buffer, and admission of an
+ * instance from such a buffer (same descriptor and storage), which then
+ * continues bit for bit.  The restored instance's residual history starts
+ * over.  No counterpart in the reference. */
+int imexlb_engine_checkpoint_size(const imexlb_engine* e, int slot, size_t* bytes);
+int imexlb_engine_checkpoint_save(imexlb_engine* e, int slot, void* host, size_t bytes);
+int imexlb_engine_restore(imexlb_engine* e, const imexlb_instance_desc* d, const void* host, size_t bytes,
+                          int* slot);
 int imexlb_engine_synchronize(imexlb_engine* e);
 void imexlb_engine_destroy(imexlb_engine* e);
 
