@@ -89,6 +89,10 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "cavity128-f64"
 
+# DRAM bytes (read + write) of one step launch from one ncu capture of the
+# workload (the summaries in profiles/ give the commands)
+TRAFFIC = {"cavity128-f64": 857.3e6, "cavity128-f16": 223.6e6}
+
 
 def tau_of(w) -> float:
     """tau0 = 3 nu: System::tau of the reference (tgv/src/System.cpp:21,
@@ -440,7 +444,7 @@ def main(argv=None) -> int:
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                          "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)",
-                         "traffic": None, "bytes_per_cell_update": 2 * 27 * bpv,
+                         "traffic": TRAFFIC.get(name), "bytes_per_cell_update": 2 * 27 * bpv,
                          "mean_launch_ms": step_ms,
                          "ghost_gather_ms_per_step": kt["ghost_ms"] / max(1, kt["ghost_launches"])
                          if kt["ghost_launches"] else 0.0},
