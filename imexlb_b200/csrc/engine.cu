@@ -376,12 +376,61 @@ int bx_log2_for(int nx, int tile_bx) {
   return std::min(std::max(l, 3), 8);
 }
 
+// Pinned host buffers for the uploads of engine_add: an admission copies its
+// initial fields through one of them and returns without waiting; a buffer
+// is reused once the event recorded after its copies has completed.
+class Staging {
+ public:
+  ~Staging() {
+    for (auto& b : bufs_) {
+      if (b.ev) cudaEventDestroy(b.ev);
+      if (b.p) cudaFreeHost(b.p);
+    }
+  }
+  // a free buffer of at least n bytes (index into the pool), or -1
+  int get(size_t n, cudaError_t* err) {
+    int best = -1;
+    for (int i = 0; i < static_cast<int>(bufs_.size()); ++i) {
+      Buf& b = bufs_[i];
+      if (b.busy && cudaEventQuery(b.ev) == cudaSuccess) b.busy = false;
+      if (!b.busy && b.cap >= n && (best < 0 || b.cap < bufs_[best].cap)) best = i;
+    }
+    *err = cudaSuccess;
+    if (best >= 0) return best;
+    Buf b;
+    const size_t cap = std::max(n, static_cast<size_t>(1) << 20);
+    if ((*err = cudaMallocHost(reinterpret_cast<void**>(&b.p), cap)) != cudaSuccess) return -1;
+    if ((*err = cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming)) != cudaSuccess) {
+      cudaFreeHost(b.p);
+      return -1;
+    }
+    b.cap = cap;
+    bufs_.push_back(b);
+    return static_cast<int>(bufs_.size()) - 1;
+  }
+  char* ptr(int i) { return bufs_[i].p; }
+  cudaError_t release_after(int i, cudaStream_t s) {
+    bufs_[i].busy = true;
+    return cudaEventRecord(bufs_[i].ev, s);
+  }
+
+ private:
+  struct Buf {
+    char* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+  };
+  std::vector<Buf> bufs_;
+};
+
 }  // namespace
 }  // namespace imx
 
 using namespace imx;
 
 struct imexlb_engine {
+  Staging staging;  // pinned uploads of admissions (declared first: destroyed last)
   imexlb_storage storage = IMEXLB_F64;
   bool exact = false;
   cudaStream_t stream = nullptr;
@@ -682,10 +731,24 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   std::vector<double> U, V, W, Pf;
   case_fields(P, sl.L, nullptr, &usr_pad, U, V, W, Pf);
   const size_t n = static_cast<size_t>(sl.ncell);
-  IMX_ECUDA(cudaMemcpyAsync(mom, U.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
-  IMX_ECUDA(cudaMemcpyAsync(mom + n, V.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
-  IMX_ECUDA(cudaMemcpyAsync(mom + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
-  IMX_ECUDA(cudaMemcpyAsync(mom + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, e->stream));
+  // everything this admission uploads goes through one pinned buffer:
+  // moments, then (sphere) mask and links, then the instance descriptor
+  const size_t up_mom = 4 * n * 8, up_mask = d->kase == IMEXLB_SPHERE ? n : 0;
+  const size_t up_links = d->kase == IMEXLB_SPHERE ? 4 * n : 0;
+  const size_t off_links = (up_mom + up_mask + 15) & ~static_cast<size_t>(15);
+  const size_t off_inst = (off_links + up_links + 15) & ~static_cast<size_t>(15);
+  cudaError_t serr = cudaSuccess;
+  const int sb = e->staging.get(off_inst + sizeof(EngInst), &serr);
+  if (sb < 0) {
+    e->arena.release(sl.off, sl.bytes);
+    return efail(IMEXLB_E_NOMEM, std::string("pinned upload buffer: ") + cudaGetErrorString(serr));
+  }
+  char* up = e->staging.ptr(sb);
+  std::memcpy(up, U.data(), n * 8);
+  std::memcpy(up + n * 8, V.data(), n * 8);
+  std::memcpy(up + 2 * n * 8, W.data(), n * 8);
+  std::memcpy(up + 3 * n * 8, Pf.data(), n * 8);
+  IMX_ECUDA(cudaMemcpyAsync(mom, up, up_mom, cudaMemcpyHostToDevice, e->stream));
 
   EngInst& in = e->h_inst[s];
   in = EngInst{};
@@ -725,13 +788,14 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {
-    std::vector<uint8_t> m(n);
+    uint8_t* m = reinterpret_cast<uint8_t*>(up + up_mom);
     for (size_t c = 0; c < n; ++c) m[c] = static_cast<uint8_t>(usr_pad[c]);
     std::vector<uint32_t> lk;
     int lo[3], hi[3];
-    solid_links(d->nx, d->ny, d->nz, m.data(), lk, lo, hi);
-    IMX_ECUDA(cudaMemcpyAsync(usr, m.data(), n, cudaMemcpyHostToDevice, e->stream));
-    IMX_ECUDA(cudaMemcpyAsync(links, lk.data(), n * 4, cudaMemcpyHostToDevice, e->stream));
+    solid_links(d->nx, d->ny, d->nz, m, lk, lo, hi);
+    std::memcpy(up + off_links, lk.data(), n * 4);
+    IMX_ECUDA(cudaMemcpyAsync(usr, m, n, cudaMemcpyHostToDevice, e->stream));
+    IMX_ECUDA(cudaMemcpyAsync(links, up + off_links, n * 4, cudaMemcpyHostToDevice, e->stream));
     a.usr = usr;
     a.links = links;
     for (int c = 0; c < 3; ++c) {
@@ -766,8 +830,11 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
                 e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
-  IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + s, &in, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
-  IMX_ECUDA(cudaStreamSynchronize(e->stream));
+  std::memcpy(up + off_inst, &in, sizeof(EngInst));
+  IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + s, up + off_inst, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
+  // no wait: the uploads follow the work already queued on the stream, and
+  // the pinned buffer is reused once they are done
+  IMX_ECUDA(e->staging.release_after(sb, e->stream));
   sl.used = true;
   e->slots[s] = sl;
   e->dirty = true;

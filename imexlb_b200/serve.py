@@ -135,17 +135,30 @@ class Server:
         self.active[slot] = (req, 0)
         return True
 
-    def advance(self) -> list[tuple]:
-        """One stepping call; returns [(request, fields, steps, residual)] of
-        the requests retired after it."""
+    def launch(self) -> int:
+        """Queue one stepping call for the admitted instances and return at
+        once; the steps run while the host admits more requests."""
         if not self.active:
-            return []
+            return 0
         n = min(self.chunk, min(r.max_steps - done for r, done in self.active.values()))
         self.eng.step(n)
         self.steps_run += n
+        self._stepped = (n, set(self.active))
+        return n
+
+    def collect(self) -> list[tuple]:
+        """Wait for the queued steps, read the residuals and retire; returns
+        [(request, fields, steps, residual)] of the retired requests.
+        Requests admitted after launch() did not take part in its steps."""
+        n, stepped = getattr(self, "_stepped", (0, set()))
+        self._stepped = (0, set())
+        if not n:
+            return []
         res = self.eng.residuals()
         done_now = []
         for slot in list(self.active):
+            if slot not in stepped:
+                continue
             req, done = self.active[slot]
             done += n
             self.active[slot] = (req, done)
@@ -159,6 +172,11 @@ class Server:
                 done_now.append((req, f, done, r))
         return done_now
 
+    def advance(self) -> list[tuple]:
+        """One stepping call and its retirements."""
+        self.launch()
+        return self.collect()
+
 
 def serve(requests: list[Request], storage: str = "f16", keep_fields: bool = False, **kw) -> dict:
     """Run the stream in real time; latencies and throughput on the host clock."""
@@ -169,18 +187,24 @@ def serve(requests: list[Request], storage: str = "f16", keep_fields: bool = Fal
     waiting = list(requests)
     results = {}
     t0 = time.perf_counter()
+    def admit_arrived():
+        now = time.perf_counter() - t0
+        while waiting and waiting[0].arrival <= now and srv.try_admit(waiting[0]):
+            waiting.pop(0)
+        return now
+
     try:
         while waiting or srv.active:
-            now = time.perf_counter() - t0
-            while waiting and waiting[0].arrival <= now and srv.try_admit(waiting[0]):
-                waiting.pop(0)
+            now = admit_arrived()
             if not srv.active:
                 if waiting[0].arrival <= now:
                     raise RuntimeError(f"request {waiting[0].rid} does not fit the engine's memory budget")
                 # idle until the next arrival
                 time.sleep(max(0.0, waiting[0].arrival - (time.perf_counter() - t0)))
                 continue
-            for req, f, steps, r in srv.advance():
+            srv.launch()
+            admit_arrived()  # host set-up of new arrivals overlaps the queued steps
+            for req, f, steps, r in srv.collect():
                 t = time.perf_counter() - t0
                 results[req.rid] = dict(latency=t - req.arrival, steps=steps, residual=r,
                                         fields=f if keep_fields else None)

@@ -246,7 +246,10 @@ typedef struct imexlb_engine_stats {
 
 int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budget_bytes, int max_instances,
                          void* stream, imexlb_engine** out);
-/* Add an instance (initial state as imexlb_create); *slot identifies it. */
+/* Add an instance (initial state as imexlb_create); *slot identifies it.
+ * Returns without waiting for the GPU: the instance's uploads and set-up
+ * follow the work already queued on the engine's stream, so a host can admit
+ * while earlier steps run. */
 int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot);
 int imexlb_engine_remove(imexlb_engine* e, int slot);
 /* Every active instance advances nsteps steps; the moments of the last are stored. */
