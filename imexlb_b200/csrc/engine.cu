@@ -803,10 +803,14 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
       a.near_hi[c] = hi[c];
     }
     const double ui = P.inlet_u;
+    // 2-byte x-pair formats store deviations from the inflow's equilibrium
+    const bool ref_flow = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
+    if (ref_flow) set_reference_flow(a.enc, ui, a.omega);
     for (int q = 0; q < Q; ++q) {
       const double t = weight_of_class(D3Q27::wclass[q]);
       const double ev = D3Q27::ex[q] * ui;
-      a.feq_in[q] = t * (3.0 * (0.0 - a.p_shift) + 3.0 * ev + 4.5 * ev * ev - 1.5 * ui * ui);
+      const double br = 3.0 * ev + 4.5 * ev * ev - 1.5 * ui * ui;
+      a.feq_in[q] = t * (3.0 * (0.0 - a.p_shift) + (ref_flow ? 0.0 : br));
     }
   }
   in.buf[0] = buf0;

@@ -54,7 +54,11 @@ __global__ void init_f_kernel(Layout L, typename StoreT<S>::T* b0, typename Stor
   const int64_t b = L.idx(0, i, j, k);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    const auto val = encode<S>(feq_of<q, R, EXACT>(uu, vv, ww, tp3, udu15), q, enc);
+    constexpr int cls = D3Q27::wclass[q];
+    R fq = feq_of<q, R, EXACT>(uu, vv, ww, tp3, udu15);
+    if constexpr (S == Store::F16 || S == Store::BF16)
+      fq -= wgt<R>(cls) * R(enc.br_ref[q]);  // deviation from the reference flow (0 unless set)
+    const auto val = encode<S>(fq, q, enc);
     b0[b + q * L.sq] = val;
     if (b1) b1[b + q * L.sq] = val;
   });
@@ -215,7 +219,8 @@ __global__ void __launch_bounds__(256) drag_links_kernel(const StepArgs a) {
         float d;
         if constexpr (S == Store::F16) d = __fmul_rn(__half2float(raw), a.enc.inv_scale[qb]);
         else d = __fmul_rn(__bfloat162float(raw), a.enc.inv_scale[qb]);
-        const double f = static_cast<double>(d) + 3.0 * wgt<double>(cls) * a.p_shift;
+        const double f = static_cast<double>(d) +
+                         wgt<double>(cls) * (3.0 * a.p_shift + static_cast<double>(a.enc.br_ref[qb]));
         if constexpr (ex != 0) acc[0] -= 2.0 * f * ex;
         if constexpr (ey != 0) acc[1] -= 2.0 * f * ey;
         if constexpr (ez != 0) acc[2] -= 2.0 * f * ez;

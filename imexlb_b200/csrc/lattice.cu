@@ -73,6 +73,17 @@ struct DevArray {
 namespace imx {
 int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 
+void set_reference_flow(Encoding& enc, double u, double omega) {
+  enc.u_ref[0] = static_cast<float>(u);
+  enc.u_ref[1] = enc.u_ref[2] = 0.f;
+  const float om_u = static_cast<float>(omega) * enc.unit;  // as the kernels form it
+  for (int q = 0; q < Q; ++q) {
+    const double e = D3Q27::ex[q] * u;
+    enc.br_ref[q] = static_cast<float>(3.0 * e + 4.5 * e * e - 1.5 * u * u);
+    enc.kref[q] = -(om_u * enc.br_ref[q]);
+  }
+}
+
 Layout make_layout(int nx, int ny, int nz, int g, int elem) {
   Layout L;
   L.nx = nx;
@@ -484,12 +495,19 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       h->drag_blocks = step_grid_blocks(h->cfg, P.nx, P.ny, P.nz);
       IMX_CUDA(h->drag_part.alloc(3 * static_cast<size_t>(h->drag_blocks)));
       IMX_CUDA(cudaMemset(h->drag_part.p, 0, h->drag_part.n * sizeof(double)));
-      // equilibrium populations of the inlet (deviation form)
+      // 2-byte x-pair formats store deviations from the inflow's equilibrium
       const double ui = P.inlet_u;
+      const bool ref_flow = (P.storage == IMEXLB_F16 || P.storage == IMEXLB_BF16) && P.nx % 2 == 0;
+      if (ref_flow) {
+        set_reference_flow(h->enc, ui, 1.0 / (P.tau0 + 0.5));
+        a.enc = h->enc;
+      }
+      // equilibrium populations of the inlet (deviation form)
       for (int q = 0; q < Q; ++q) {
         const double t = weight_of_class(D3Q27::wclass[q]);
         const double e = D3Q27::ex[q] * ui;
-        a.feq_in[q] = t * (3.0 * (0.0 - h->p_shift) + 3.0 * e + 4.5 * e * e - 1.5 * ui * ui);
+        const double br = 3.0 * e + 4.5 * e * e - 1.5 * ui * ui;
+        a.feq_in[q] = t * (3.0 * (0.0 - h->p_shift) + (ref_flow ? 0.0 : br));
       }
     }
   }

@@ -49,11 +49,22 @@ Layout make_layout(int nx, int ny, int nz, int g, int elem);
 // deviation f_q - 3 w_q p_shift.
 // For the 2-byte formats scale[q] = unit / w_q, unit = 2^14 for FP16 (keeps
 // small deviations out of the subnormals) and 1 for BF16; FP32 stores d_q.
+// The standard sphere channel in the 2-byte x-pair formats measures the
+// deviations from the equilibrium of the inflow instead of the rest state:
+// d_q = f_q - w_q (3 p_shift + br_ref[q]), br_ref[q] = 3 c.u_ref + 4.5
+// (c.u_ref)^2 - 1.5 |u_ref|^2 with u_ref the inlet velocity, so most of the
+// channel stores small numbers; elsewhere u_ref = 0 and br_ref = 0.
 struct Encoding {
   float scale[Q];
   float inv_scale[Q];
   float unit = 1.f;
+  float u_ref[3] = {0.f, 0.f, 0.f};
+  float br_ref[Q] = {};
+  float kref[Q] = {};  // -omega unit br_ref[q], the collision's share of it
 };
+// Set u_ref, br_ref and kref of `enc` for the reference velocity (u, 0, 0)
+// and the relaxation rate omega.
+void set_reference_flow(Encoding& enc, double u, double omega);
 
 struct StepArgs {
   // Fields up to `src` are all that the shared-memory staged kernels read;

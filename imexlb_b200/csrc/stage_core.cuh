@@ -240,6 +240,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
 
   const int32_t bself = a.base32 + k * a.sz32 + j * a.pitch32 + x;
   bool live0 = true, live1 = true;
+  uint32_t links0 = 0, links1 = 0;  // sphere: solid-link bits of the two cells
   if constexpr (RULE == CaseRule::CavityStd && EDGE) {
     uint32_t out_bits = 0;  // bit (3 dz + dy): source row outside the box
 #pragma unroll
@@ -272,7 +273,8 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
                       x + 1 >= a.near_lo[0] && x <= a.near_hi[0];
     if (near) {
       const int64_t cell = x + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
-      const uint32_t links0 = a.links[cell], links1 = a.links[cell + 1];
+      links0 = a.links[cell];
+      links1 = a.links[cell + 1];
       live0 = a.usr[cell] != 0;
       live1 = a.usr[cell + 1] != 0;
       if (links0 | links1) {
@@ -289,7 +291,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
     }
   }
   const bool lid = RULE == CaseRule::CavityStd && k == a.nz - 1;
-  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store);
+  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store, links0, links1);
 }
 
 // The cells of tile (j0, k) from stage `st`, shared by the block's threads.

@@ -402,10 +402,38 @@ __device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, con
   });
 }
 
-// Two cells at once in FP32 with Blackwell's paired FP32 instructions
-// (__fadd2_rn, __fmul2_rn, __ffma2_rn): every operation of the collision
-// acts on the same quantity of both cells, so the pair costs about the
-// instructions of one.  Same arithmetic as compute_cell's FP32 path.
+// Two cells at once in FP32 with Blackwell's paired FP32 instructions: every
+// operation of the collision acts on the same quantity of both cells, so the
+// pair costs about the instructions of one.  Same arithmetic as
+// compute_cell's FP32 path.  The operations are written as PTX
+// add/mul/fma.rn.f32x2: an explicit rounding mode forbids the code generator
+// to fuse a multiply into a later add, so every kernel that inlines this code
+// rounds the same way and their results agree bit for bit (the x-pair
+// register kernels, the staged kernels and the engine's).
+__device__ __forceinline__ float2 add2rn(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " add.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 mul2rn(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " mul.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 fma2rn(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " mov.b64 rc, {%6, %7};\n fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
 
@@ -420,14 +448,14 @@ __device__ __forceinline__ float2 edu2(float2 u, float2 v, float2 w) {
   }
   if constexpr (b != 0) {
     if (have)
-      t = b > 0 ? __fadd2_rn(t, v) : __fadd2_rn(t, f2(-v.x, -v.y));
+      t = b > 0 ? add2rn(t, v) : add2rn(t, f2(-v.x, -v.y));
     else
       t = b > 0 ? v : f2(-v.x, -v.y);
     have = true;
   }
   if constexpr (c != 0) {
     if (have)
-      t = c > 0 ? __fadd2_rn(t, w) : __fadd2_rn(t, f2(-w.x, -w.y));
+      t = c > 0 ? add2rn(t, w) : add2rn(t, f2(-w.x, -w.y));
     else
       t = c > 0 ? w : f2(-w.x, -w.y);
   }
@@ -446,15 +474,15 @@ __device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, con
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     const float2 x = f2(f0[q], f1[q]);
-    s = __fadd2_rn(s, x);
-    if constexpr (D3Q27::ex[q] == 1) u = __fadd2_rn(u, x);
-    if constexpr (D3Q27::ex[q] == -1) u = __fadd2_rn(u, f2(-x.x, -x.y));
-    if constexpr (D3Q27::ey[q] == 1) v = __fadd2_rn(v, x);
-    if constexpr (D3Q27::ey[q] == -1) v = __fadd2_rn(v, f2(-x.x, -x.y));
-    if constexpr (D3Q27::ez[q] == 1) w = __fadd2_rn(w, x);
-    if constexpr (D3Q27::ez[q] == -1) w = __fadd2_rn(w, f2(-x.x, -x.y));
+    s = add2rn(s, x);
+    if constexpr (D3Q27::ex[q] == 1) u = add2rn(u, x);
+    if constexpr (D3Q27::ex[q] == -1) u = add2rn(u, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ey[q] == 1) v = add2rn(v, x);
+    if constexpr (D3Q27::ey[q] == -1) v = add2rn(v, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ez[q] == 1) w = add2rn(w, x);
+    if constexpr (D3Q27::ez[q] == -1) w = add2rn(w, f2(-x.x, -x.y));
   });
-  float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
+  float2 p = mul2rn(s, f2s(1.0f / 3.0f));
   case_rules<RULE>(a, i, k, c0, u.x, v.x, w.x, p.x);
   case_rules<RULE>(a, i, k, c1, u.y, v.y, w.y, p.y);
   if (a.store) {
@@ -467,20 +495,20 @@ __device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, con
     a.mw[c1] = w.y;
     a.mp[c1] = static_cast<double>(p.y) + a.p_shift;
   }
-  const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+  const float2 udu15 = mul2rn(f2s(1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
   float2 tp3[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) tp3[c] = __fmul2_rn(p, f2s(3.0f * wgt<float>(c)));
+  for (int c = 0; c < 4; ++c) tp3[c] = mul2rn(p, f2s(3.0f * wgt<float>(c)));
   const float2 om = f2s(-static_cast<float>(a.omega));
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     constexpr int cls = D3Q27::wclass[q];
     const float2 e = edu2<q>(u, v, w);
     // t (3e + 4.5 e^2 - 1.5 u.u) + 3 t p, with e (3 + 4.5 e) for the bracket
-    const float2 br = __fadd2_rn(__fmul2_rn(e, __ffma2_rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
-    const float2 feq = __ffma2_rn(f2s(wgt<float>(cls)), br, tp3[cls]);
+    const float2 br = add2rn(mul2rn(e, fma2rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
+    const float2 feq = fma2rn(f2s(wgt<float>(cls)), br, tp3[cls]);
     const float2 x = f2(f0[q], f1[q]);
-    const float2 fs = __ffma2_rn(om, __fadd2_rn(x, f2(-feq.x, -feq.y)), x);
+    const float2 fs = fma2rn(om, add2rn(x, f2(-feq.x, -feq.y)), x);
     pl.store(q, b0, encode<S>(fs.x, q, a.enc));
     pl.store(q, b1, encode<S>(fs.y, q, a.enc));
   });
@@ -577,12 +605,16 @@ __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { retu
 //   g_q' = (1 - omega) g_q + omega unit (3 p~ + e(3 + 4.5 e) - 1.5 u.u),
 // e = c_q . u and p~ = sum d_q / 3 = p - p_shift, since the shift's own
 // equilibrium cancels (sum w_q = 1, sum w_q c_q = 0).  The moments take
-// d_q = g_q w_q / unit.  live0 / live1: the cell is fluid (a solid cell's
-// values are left as they are); store: write the moments.
+// d_q = g_q w_q / unit.  For the sphere channel the deviations are from the
+// inflow's equilibrium (Encoding::br_ref): u gains u_ref, the collision
+// subtracts omega unit br_ref[q] (Encoding::kref) and populations bounced off
+// the solid (links0 / links1, bit q) are corrected.  live0 / live1: the cell is fluid (a solid
+// cell's values are left as they are); store: write the moments.
 template <Store S, CaseRule RULE, class P>
 __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
-                                                const bool live0, const bool live1, const bool store) {
+                                                const bool live0, const bool live1, const bool store,
+                                                const uint32_t links0 = 0, const uint32_t links1 = 0) {
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
   [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
@@ -592,24 +624,48 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     float2 x = Pack2<S>::to_f2(raw[q]);
     if constexpr (RULE == CaseRule::CavityStd && ex != 0 && ez < 0) {
       // moving lid: + 6 rho_w w_q (c_q . u_w), in stored units
-      if (lid) x = __fadd2_rn(x, f2s(ex > 0 ? lid_g : -lid_g));
+      if (lid) x = add2rn(x, f2s(ex > 0 ? lid_g : -lid_g));
     }
     if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
       if (left_edge) x.x = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
     }
-    const float2 d = __fmul2_rn(x, f2s(a.enc.inv_scale[q]));
-    s = __fadd2_rn(s, d);
-    if constexpr (ex == 1) u = __fadd2_rn(u, d);
-    if constexpr (ex == -1) u = __fadd2_rn(u, f2(-d.x, -d.y));
-    if constexpr (ey == 1) v = __fadd2_rn(v, d);
-    if constexpr (ey == -1) v = __fadd2_rn(v, f2(-d.x, -d.y));
-    if constexpr (ez == 1) w = __fadd2_rn(w, d);
-    if constexpr (ez == -1) w = __fadd2_rn(w, f2(-d.x, -d.y));
+    const float2 d = mul2rn(x, f2s(a.enc.inv_scale[q]));
+    s = add2rn(s, d);
+    if constexpr (ex == 1) u = add2rn(u, d);
+    if constexpr (ex == -1) u = add2rn(u, f2(-d.x, -d.y));
+    if constexpr (ey == 1) v = add2rn(v, d);
+    if constexpr (ey == -1) v = add2rn(v, f2(-d.x, -d.y));
+    if constexpr (ez == 1) w = add2rn(w, d);
+    if constexpr (ez == -1) w = add2rn(w, f2(-d.x, -d.y));
     g[q] = x;
   });
+  if constexpr (RULE == CaseRule::SphereStd) {
+    if (links0 | links1) {
+      // A population bounced off the solid came back as the cell's own
+      // bb(q) value; against the inflow's equilibrium its deviation gains
+      // unit (br_ref[bb(q)] - br_ref[q]) = -6 unit c_q.u_ref (e_x != 0
+      // only), added here with its share of the moments.
+      static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+        if constexpr (ex != 0) {
+          const float c = -6.f * static_cast<float>(ex) * a.enc.u_ref[0] * a.enc.unit;
+          const float2 dg = f2(((links0 >> q) & 1u) ? c : 0.f, ((links1 >> q) & 1u) ? c : 0.f);
+          g[q] = add2rn(g[q], dg);
+          const float2 dd = mul2rn(dg, f2s(a.enc.inv_scale[q]));
+          s = add2rn(s, dd);
+          u = ex > 0 ? add2rn(u, dd) : add2rn(u, f2(-dd.x, -dd.y));
+          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : add2rn(v, f2(-dd.x, -dd.y));
+          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : add2rn(w, f2(-dd.x, -dd.y));
+        }
+      });
+    }
+    // deviations are from the inflow's equilibrium: its velocity adds back
+    u = add2rn(u, f2s(a.enc.u_ref[0]));
+  }
   const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + x0;
   const int64_t c0 = x0 + static_cast<int64_t>(a.nx) * (j + static_cast<int64_t>(a.ny) * k);
-  float2 p = __fmul2_rn(s, f2s(1.0f / 3.0f));
+  float2 p = mul2rn(s, f2s(1.0f / 3.0f));
   case_rules<RULE>(a, x0, k, c0, u.x, v.x, w.x, p.x);
   case_rules<RULE>(a, x0 + 1, k, c0 + 1, u.y, v.y, w.y, p.y);
   if (store) {
@@ -625,19 +681,24 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   const float om = static_cast<float>(a.omega);
   const float om_u = om * a.enc.unit;
   const float2 keep = f2s(1.0f - om);
-  const float2 udu15 = __fmul2_rn(f2s(1.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+  const float2 udu15 = mul2rn(f2s(1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
   // omega unit (3 p~ - 1.5 u.u)
-  const float2 K = __fmul2_rn(f2s(om_u), __ffma2_rn(p, f2s(3.0f), f2(-udu15.x, -udu15.y)));
+  const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), f2(-udu15.x, -udu15.y)));
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
+    float2 Kq = K;
+    if constexpr (RULE == CaseRule::SphereStd) {
+      // minus the reference flow's equilibrium, omega unit br_ref[q]
+      Kq = add2rn(K, f2s(a.enc.kref[q]));
+    }
     float2 gn;
     if constexpr (q == 0) {
-      gn = __ffma2_rn(g[q], keep, K);
+      gn = fma2rn(g[q], keep, Kq);
     } else {
       const float2 e = edu2<q>(u, v, w);
-      const float2 t = __ffma2_rn(e, f2s(4.5f), f2s(3.0f));
-      const float2 h = __fmul2_rn(e, f2s(om_u));
-      gn = __ffma2_rn(h, t, __ffma2_rn(g[q], keep, K));
+      const float2 t = fma2rn(e, f2s(4.5f), f2s(3.0f));
+      const float2 h = mul2rn(e, f2s(om_u));
+      gn = fma2rn(h, t, fma2rn(g[q], keep, Kq));
     }
     if (live0 && live1) {
       pl.store_pair(q, b, Pack2<S>::from_f2(gn));
@@ -659,6 +720,7 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
   bool act[RY];
   uint32_t row_out_bits[RY];  // cavity: bit (3 dz + dy) = source row outside the box
   uint32_t lid_mask = 0;      // cavity: rows whose cells sit under the lid
+  uint32_t lk[RY][2];         // sphere: per-cell solid-link bits
   int32_t bself[RY];
 
   // Every population of both rows arrives as aligned 4-byte pairs issued
@@ -703,6 +765,8 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       links0 = near ? a.links[cell] : 0u;
       links1 = near ? a.links[cell + 1] : 0u;
     }
+    lk[r][0] = links0;
+    lk[r][1] = links1;
     if constexpr (RULE == CaseRule::CavityStd) {
       if (k == a.nz - 1) lid_mask |= 1u << r;
     }
@@ -766,7 +830,8 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       live0 = a.usr[c0] != 0;
       live1 = a.usr[c0 + 1] != 0;
     }
-    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store);
+    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store,
+                             lk[r][0], lk[r][1]);
   }
 }
 
