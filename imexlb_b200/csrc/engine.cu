@@ -685,7 +685,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   const int elem = e->storage == IMEXLB_F64 ? 8 : (e->storage == IMEXLB_F32 ? 4 : 2);
   Slot sl;
   sl.d = *d;
-  sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem);
+  sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem, cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, e->storage));
   if (static_cast<double>(sl.L.sq) * Q >= 2147483647.0) return efail(IMEXLB_E_ARG, "instance too large for the engine");
   sl.ncell = static_cast<int64_t>(d->nx) * d->ny * d->nz;
   const size_t fbytes = (sl.L.bytes() + 511) & ~static_cast<size_t>(511);
@@ -834,6 +834,8 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
                 e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
+  if (cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, e->storage) && d->nx % 2 == 0)
+    IMX_ECUDA(launch_cavity_pad_init(sl.L, buf0, buf1, e->stream));
   std::memcpy(up + off_inst, &in, sizeof(EngInst));
   IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + s, up + off_inst, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
   // no wait: the uploads follow the work already queued on the stream, and
@@ -954,7 +956,7 @@ int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st) {
 int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes) {
   if (!d || !bytes) return efail(IMEXLB_E_ARG, "null argument");
   const int elem = storage == IMEXLB_F64 ? 8 : (storage == IMEXLB_F32 ? 4 : 2);
-  const Layout L = make_layout(d->nx, d->ny, d->nz, 0, elem);
+  const Layout L = make_layout(d->nx, d->ny, d->nz, 0, elem, cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, storage));
   const int64_t n = static_cast<int64_t>(d->nx) * d->ny * d->nz;
   auto r = [](size_t x) { return (x + 511) & ~static_cast<size_t>(511); };
   const size_t mask = static_cast<size_t>((n + 255) & ~int64_t(255));

@@ -187,6 +187,30 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   if (threadIdx.x == 0 && abort_flag) atomicOr(a.err, 1);
 }
 
+// 2-byte standard cavity: the padding after each stored row carries the
+// bounce-back values of its x walls (stage_core.cuh).  For the row (jj, kk)
+// of population q with e_x = +1, element pitch - 1 holds f(bb(q)) of the
+// cell (0, jj + e_y, kk + e_z), whose pull along e_q starts at x = -1; with
+// e_x = -1, element nx holds f(bb(q)) of the cell (nx - 1, jj + e_y, kk + e_z).
+// This fills them for the initial state; the step kernels refresh them.
+__global__ void cavity_pad_init_kernel(const Layout L, uint16_t* b0, uint16_t* b1) {
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, kk = blockIdx.y;
+  if (jj >= L.ny) return;
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q], qb = D3Q27::bb[q];
+    if constexpr (ex != 0) {
+      const int j = jj + ey, k = kk + ez;
+      if (j >= 0 && j < L.ny && k >= 0 && k < L.nz) {
+        const int64_t from = L.idx(qb, ex > 0 ? 0 : L.nx - 1, j, k);
+        const int64_t to = L.idx(q, ex > 0 ? static_cast<int>(L.pitch - L.xoff) - 1 : L.nx, jj, kk);
+        b0[to] = b0[from];
+        b1[to] = b1[from];
+      }
+    }
+  });
+}
+
 // Momentum-exchange drag of the 2-byte sphere channel, from the buffer a
 // step reads: every fluid cell c with a solid link along -e_q takes back
 // f*(bb(q), c), so the body receives -2 (f*(bb(q), c)) e_q.  Its own kernel
@@ -443,6 +467,12 @@ int64_t step_grid_blocks(const LaunchCfg& c, int nx, int ny, int nz) {
   const int cpt = c.store == Store::F64 ? 1 : CellsPerThread<Store::F32>::value;
   const int rows = b.y * cpt;
   return static_cast<int64_t>((nx + b.x - 1) / b.x) * ((ny + rows - 1) / rows) * nz;
+}
+
+cudaError_t launch_cavity_pad_init(const Layout& L, void* buf0, void* buf1, cudaStream_t s) {
+  const dim3 block(64, 1, 1), grid((L.ny + 63) / 64, L.nz, 1);
+  cavity_pad_init_kernel<<<grid, block, 0, s>>>(L, static_cast<uint16_t*>(buf0), static_cast<uint16_t*>(buf1));
+  return cudaGetLastError();
 }
 
 cudaError_t launch_drag_sum(const double* part, int64_t nblk, double* out, cudaStream_t s) {

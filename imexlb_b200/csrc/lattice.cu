@@ -84,7 +84,12 @@ void set_reference_flow(Encoding& enc, double u, double omega) {
   }
 }
 
-Layout make_layout(int nx, int ny, int nz, int g, int elem) {
+int cavity_x_pad(int kase, int bc, int storage) {
+  return kase == IMEXLB_CAVITY && bc == IMEXLB_BC_STANDARD && (storage == IMEXLB_F16 || storage == IMEXLB_BF16) ? 2
+                                                                                                              : 0;
+}
+
+Layout make_layout(int nx, int ny, int nz, int g, int elem, int xpad) {
   Layout L;
   L.nx = nx;
   L.ny = ny;
@@ -100,7 +105,7 @@ Layout make_layout(int nx, int ny, int nz, int g, int elem) {
   // staged kernels copy several rows with one bulk copy.
   const int64_t line = (elem == 2 && g == 0) ? 16 : 128 / elem;
   L.xoff = (line - (g % line)) % line;
-  L.pitch = ((L.xoff + L.ex + line - 1) / line) * line;
+  L.pitch = ((L.xoff + L.ex + xpad + line - 1) / line) * line;
   L.sz = L.pitch * L.ey;
   L.sq = L.sz * L.ez;
   return L;
@@ -285,6 +290,8 @@ int upload_case(imexlb_lattice* h) {
   IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
   IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, tmp.p, tmp.p + n, tmp.p + 2 * n, tmp.p + 3 * n,
                          h->p_shift, h->enc, h->stream));
+  if (cavity_x_pad(h->P.kase, h->P.bc, h->P.storage) && h->L.nx % 2 == 0)
+    IMX_CUDA(launch_cavity_pad_init(L, h->buf[0].p, h->buf[1].p, h->stream));
   // the views after Initialize: interior moments
   std::vector<double> mom(4 * static_cast<size_t>(h->ncell));
   for (int k = 0; k < L.nz; ++k)
@@ -396,7 +403,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   else
     h->cfg.rule = ghost ? CaseRule::SphereRef : CaseRule::SphereStd;
   const int elem = P.storage == IMEXLB_F64 ? 8 : (P.storage == IMEXLB_F32 ? 4 : 2);
-  h->L = make_layout(P.nx, P.ny, P.nz, ghost ? GHOST : 0, elem);
+  h->L = make_layout(P.nx, P.ny, P.nz, ghost ? GHOST : 0, elem, cavity_x_pad(P.kase, P.bc, P.storage));
   const Layout& L = h->L;
   h->ncell = static_cast<int64_t>(P.nx) * P.ny * P.nz;
 

@@ -42,7 +42,12 @@ struct Layout {
   IMX_HD int64_t interior(int q, int i, int j, int k) const { return idx(q, i + g, j + g, k + g); }
   size_t bytes() const { return static_cast<size_t>(sq) * Q * elem; }
 };
-Layout make_layout(int nx, int ny, int nz, int g, int elem);
+// xpad: stored elements kept free after the last stored x of each row (the
+// 2-byte standard cavity keeps 2 for the bounce-back of its x walls, see
+// cavity_x_pad and stage_core.cuh).
+Layout make_layout(int nx, int ny, int nz, int g, int elem, int xpad = 0);
+// Row padding of a lattice of this case, boundary and storage.
+int cavity_x_pad(int kase, int bc, int storage);
 
 // Per-population scaling of reduced-precision storage:
 // stored = d_q * scale[q], d_q = stored * inv_scale[q], where d_q is the
@@ -161,6 +166,9 @@ struct LaunchCfg {
   bool exact;
 };
 
+// 2-byte standard cavity: fill each row's x-wall padding of both buffers
+// with the bounce-back values of the initial state (stage_core.cuh).
+cudaError_t launch_cavity_pad_init(const Layout& L, void* buf0, void* buf1, cudaStream_t s);
 cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void* buf1, const double* u,
                           const double* v, const double* w, const double* p, double p_shift, const Encoding& enc,
                           cudaStream_t s);

@@ -25,9 +25,11 @@
 // counts the tile's bytes.  Every warp waits on "full", updates its cells
 // and releases the stage.  Each thread updates x-pairs of cells with the
 // same arithmetic as the register-staged x-pair kernels (finish_pair_row).
-// Halfway bounce-back and solid links read the cell's own opposite
-// population from global memory, in a second pass that only boundary pairs
-// take.
+// The cavity's x-wall bounce-back values travel in the padding after each
+// row (a cell at an x wall also writes its opposite populations there, see
+// finish_pair_row), so its x walls cost nothing here; the y / z walls and a
+// sphere's solid links read the cell's own opposite population from global
+// memory, in a second pass that only boundary pairs take.
 //
 // Every wait on an mbarrier gives up after about a second of wall-clock time
 // (%globaltimer), records the failure in the step's error word and leaves
@@ -215,8 +217,16 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
   const int row = (r * g.P) >> 1;  // word offset of tile row r in a slot
   const int pw = row + (x >> 1);
   const bool left_edge = EDGE && x == 0, right_edge = EDGE && x + 2 >= a.nx;
-  const int lw = row + ((left_edge ? a.nx - 2 : x - 2) >> 1);  // holds x - 1 (wrapped)
-  const int rw = row + ((right_edge ? 0 : x + 2) >> 1);       // holds x + 2 (wrapped)
+  int lw, rw;  // the pairs holding x - 1 and x + 2
+  if constexpr (RULE == CaseRule::CavityStd) {
+    // the row's padding holds the x walls' bounce-back values: x = -1 is
+    // element P - 1, x = nx element nx
+    lw = row + ((x == 0 ? g.P - 2 : x - 2) >> 1);
+    rw = row + ((x + 2) >> 1);
+  } else {
+    lw = row + ((x == 0 ? a.nx - 2 : x - 2) >> 1);  // wrapped inside the row
+    rw = row + ((x + 2 >= a.nx ? 0 : x + 2) >> 1);
+  }
   const int slotw = g.cap >> 1;
 
   uint32_t raw[Q];
@@ -250,20 +260,15 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
         const int jj = j + dy - 1, kk = k + dz - 1;
         if (jj < 0 || jj >= a.ny || kk < 0 || kk >= a.nz) out_bits |= 1u << (3 * dz + dy);
       }
-    if (out_bits || left_edge || right_edge) {
-      // halfway bounce-back: a link leaving the box returns the cell's own
-      // opposite population
+    if (out_bits) {
+      // halfway bounce-back at the y and z walls: a link leaving the box
+      // returns the cell's own opposite population (the x walls' values
+      // come with the staged row's padding)
       static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+        constexpr int ey = D3Q27::ey[q], ez = D3Q27::ez[q];
         constexpr int qb = D3Q27::bb[q];
-        const bool out_row = (out_bits >> (3 * (1 - ez) + (1 - ey))) & 1u;
-        const bool out0 = out_row || (ex == 1 && left_edge);
-        const bool out1 = out_row || (ex == -1 && right_edge);
-        if (out0 || out1) {
-          const uint32_t bbp = pl.load_pair(qb, bself);
-          raw[q] = pair_of(out0 ? bbp : raw[q], out1 ? (bbp >> 16) : (raw[q] >> 16));
-        }
+        if ((out_bits >> (3 * (1 - ez) + (1 - ey))) & 1u) raw[q] = pl.load_pair(qb, bself);
       });
     }
   } else if constexpr (RULE == CaseRule::SphereStd) {
@@ -295,35 +300,28 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
 }
 
 // The cells of tile (j0, k) from stage `st`, shared by the block's threads.
-// For the cavity, pairs next to a wall take the checked path, and the pairs
-// at the x walls go last, to as few warps as possible: their bounce-back
-// reads global memory, and a warp waits for its slowest lane.
+// Cavity pairs in a wall row or plane take the checked path (y / z
+// bounce-back; a warp holds pairs of one or two rows, so the choice is
+// nearly uniform across it); the others need no check, since the x walls'
+// values come with the staged rows' padding.
 template <Store S, Bc B, CaseRule RULE, class P>
 __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                              const int j0, const int k, const bool store) {
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
+  const int half = g.P >> 1;
+  const int npairs = g.R * half;
   if constexpr (RULE == CaseRule::CavityStd) {
-    const int nx2 = a.nx >> 1;
-    const int ni = nx2 > 2 ? nx2 - 2 : 0;  // interior pairs per row
-    const int ne = nx2 < 2 ? nx2 : 2;      // edge pairs per row
-    const int n_int = rv * ni, n_all = n_int + rv * ne;
     const bool wall_plane = k == 0 || k == a.nz - 1;
-    for (int p = threadIdx.x; p < n_all; p += THREADS) {
-      if (p < n_int) {
-        const int r = p / ni, x = 2 + 2 * (p - r * ni);
-        const int j = j0 + r;
-        if (wall_plane || j == 0 || j == a.ny - 1)
-          pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
-        else
-          pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store);
-      } else {
-        const int e = p - n_int, r = e / ne, x = (e - r * ne) == 0 ? 0 : a.nx - 2;
+    for (int p = threadIdx.x; p < npairs; p += THREADS) {
+      const int r = p / half, x = 2 * (p - r * half);
+      if (r >= rv || x >= a.nx) continue;
+      const int j = j0 + r;
+      if (wall_plane || j == 0 || j == a.ny - 1)
         pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
-      }
+      else
+        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store);
     }
   } else {
-    const int half = g.P >> 1;
-    const int npairs = g.R * half;
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
       const int r = p / half, x = 2 * (p - r * half);
       if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);

@@ -706,6 +706,24 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
       if (live0) pl.store_half(q, b, Pack2<S>::from_f(gn.x));
       if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(gn.y));
     }
+    if constexpr (RULE == CaseRule::CavityStd) {
+      // x walls: the next step's pull of bb(q) at this cell starts outside
+      // the box and must return this value (halfway bounce-back); it goes to
+      // the padding of the row that pull reads (x = -1 -> element pitch - 1,
+      // x = nx -> element nx), inside the box's y and z range only
+      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q], qq = D3Q27::bb[q];
+      if constexpr (ex != 0) {
+        const bool at_wall = ex < 0 ? x0 == 0 : x0 + 2 >= a.nx;
+        const int jj = j + ey, kk = k + ez;  // the row of bb(q)'s pull source
+        if (at_wall && jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) {
+          const int32_t row = a.base32 + kk * a.sz32 + jj * a.pitch32;
+          if (ex < 0)
+            pl.store_half(qq, row + a.pitch32 - 1, Pack2<S>::from_f(gn.x));
+          else
+            pl.store_half(qq, row + a.nx, Pack2<S>::from_f(gn.y));
+        }
+      }
+    }
   });
 }
 
