@@ -684,6 +684,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   const float2 udu15 = mul2rn(f2s(1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
   // omega unit (3 p~ - 1.5 u.u)
   const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), f2(-udu15.x, -udu15.y)));
+  // cavity: the pair holds a cell at an x wall (padding stores below)
+  [[maybe_unused]] const bool xwall_lo = RULE == CaseRule::CavityStd && x0 == 0;
+  [[maybe_unused]] const bool xwall_hi = RULE == CaseRule::CavityStd && x0 + 2 >= a.nx;
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     float2 Kq = K;
@@ -713,14 +716,15 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
       // x = nx -> element nx), inside the box's y and z range only
       constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q], qq = D3Q27::bb[q];
       if constexpr (ex != 0) {
-        const bool at_wall = ex < 0 ? x0 == 0 : x0 + 2 >= a.nx;
-        const int jj = j + ey, kk = k + ez;  // the row of bb(q)'s pull source
-        if (at_wall && jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) {
-          const int32_t row = a.base32 + kk * a.sz32 + jj * a.pitch32;
-          if (ex < 0)
-            pl.store_half(qq, row + a.pitch32 - 1, Pack2<S>::from_f(gn.x));
-          else
-            pl.store_half(qq, row + a.nx, Pack2<S>::from_f(gn.y));
+        if (ex < 0 ? xwall_lo : xwall_hi) {
+          const int jj = j + ey, kk = k + ez;  // the row of bb(q)'s pull source
+          if (jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) {
+            const int32_t row = a.base32 + kk * a.sz32 + jj * a.pitch32;
+            if (ex < 0)
+              pl.store_half(qq, row + a.pitch32 - 1, Pack2<S>::from_f(gn.x));
+            else
+              pl.store_half(qq, row + a.nx, Pack2<S>::from_f(gn.y));
+          }
         }
       }
     }
