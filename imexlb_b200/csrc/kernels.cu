@@ -54,7 +54,7 @@ __global__ void init_f_kernel(Layout L, typename StoreT<S>::T* b0, typename Stor
   const int64_t b = L.idx(0, i, j, k);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    constexpr int cls = D3Q27::wclass[q];
+    [[maybe_unused]] constexpr int cls = D3Q27::wclass[q];
     R fq = feq_of<q, R, EXACT>(uu, vv, ww, tp3, udu15);
     if constexpr (S == Store::F16 || S == Store::BF16)
       fq -= wgt<R>(cls) * R(enc.br_ref[q]);  // deviation from the reference flow (0 unless set)

@@ -145,38 +145,64 @@ __device__ __forceinline__ int ez_of(int q) { return static_cast<int>((EZ_BITS >
 // The copies of population q for a tile: the source rows of tile rows
 // [0, rv) as at most two contiguous runs, the second one a wrapped row
 // (bytes 0 = no copy).
+// the opposite population of q in the D3Q27 ordering (pairs 1-2, 3-4, ...)
+__host__ __device__ constexpr int bb_of(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+constexpr bool bb_matches() {
+  for (int q = 0; q < Q; ++q)
+    if (bb_of(q) != D3Q27::bb[q]) return false;
+  return true;
+}
+static_assert(bb_matches(), "bb_of follows the opposite table");
+
 struct Run {
-  int32_t src;  // element index within plane q
+  int32_t src;  // element index within plane `pop`
   int32_t dst;  // element offset within the stage
   uint32_t bytes;
+  int32_t pop;  // population whose plane the run reads
 };
 
+// Source rows that lie outside a periodic axis wrap around.  On a wall
+// (WRAP_YZ false: the cavity) the halfway bounce-back returns the cell's own
+// opposite population instead, so slot q's rows whose source is outside the
+// box receive the tile's own rows of bb(q) (plane k, rows j0 + r), which the
+// consumer reads unshifted.
 template <bool WRAP_YZ>
 __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q, int j0, int k, int rv, int elem,
                                           Run& main, Run& wrap) {
   main.bytes = 0;
   wrap.bytes = 0;
+  main.pop = wrap.pop = q;
+  const int32_t slot = q * g.cap;
   int kk = k - ez_of(q);
   if (kk < 0 || kk >= a.nz) {
-    if (!WRAP_YZ) return;
+    if (!WRAP_YZ) {
+      // every row of the tile bounces: bb(q)'s own rows
+      main.pop = bb_of(q);
+      main.src = a.base32 + k * a.sz32 + j0 * a.pitch32;
+      main.dst = slot;
+      main.bytes = static_cast<uint32_t>(rv * g.P * elem);
+      return;
+    }
     kk = kk < 0 ? kk + a.nz : kk - a.nz;
   }
   const int y0 = j0 - ey_of(q);  // source row of tile row 0
   const int32_t plane = a.base32 + kk * a.sz32;
-  const int32_t slot = q * g.cap;
   const int r_lo = y0 < 0 ? -y0 : 0;
   const int r_hi = y0 + rv > a.ny ? a.ny - y0 : rv;
   main.src = plane + (y0 + r_lo) * a.pitch32;
   main.dst = slot + r_lo * g.P;
   main.bytes = r_hi > r_lo ? static_cast<uint32_t>((r_hi - r_lo) * g.P * elem) : 0u;
+  // tile row 0 pulls from y = -1, or the last tile row from y = ny; |e_y| <= 1
+  // allows one of them at most
+  const bool first = r_lo > 0, last = r_hi < rv;
   if (WRAP_YZ) {
-    // tile row 0 pulls from y = -1 (the last row), or the last tile row
-    // from y = ny (the first row); |e_y| <= 1 allows one of them at most
-    const bool first = r_lo > 0, last = r_hi < rv;
-    wrap.src = plane + (first ? (a.ny - 1) * a.pitch32 : 0);
-    wrap.dst = slot + (first ? 0 : (rv - 1) * g.P);
-    wrap.bytes = (first || last) ? static_cast<uint32_t>(g.P * elem) : 0u;
+    wrap.src = plane + (first ? (a.ny - 1) * a.pitch32 : 0);  // the wrapped row
+  } else {
+    wrap.pop = bb_of(q);  // the tile's own row of bb(q)
+    wrap.src = a.base32 + k * a.sz32 + (first ? j0 : j0 + rv - 1) * a.pitch32;
   }
+  wrap.dst = slot + (first ? 0 : (rv - 1) * g.P);
+  wrap.bytes = (first || last) ? static_cast<uint32_t>(g.P * elem) : 0u;
 }
 
 // Issue the copies of tile (j0, k) into stage `st` (called by a whole warp;
@@ -196,9 +222,8 @@ __device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, cons
   for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
   if (lane == 0) bar_arrive_expect(bar, total);
   __syncwarp();
-  const T* plane = src + static_cast<int64_t>(lane) * a.sq;
-  if (m.bytes) bulk_g2s(st + m.dst, plane + m.src, m.bytes, bar);
-  if (w.bytes) bulk_g2s(st + w.dst, plane + w.src, w.bytes, bar);
+  if (m.bytes) bulk_g2s(st + m.dst, src + static_cast<int64_t>(m.pop) * a.sq + m.src, m.bytes, bar);
+  if (w.bytes) bulk_g2s(st + w.dst, src + static_cast<int64_t>(w.pop) * a.sq + w.src, w.bytes, bar);
   if (lane == 31 && xbytes) bulk_g2s(xdst, xsrc, xbytes, bar);
 }
 
@@ -262,13 +287,13 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
       }
     if (out_bits) {
       // halfway bounce-back at the y and z walls: a link leaving the box
-      // returns the cell's own opposite population (the x walls' values
-      // come with the staged row's padding)
+      // returns the cell's own opposite population, which the producer put
+      // in slot q in place of the missing source row (tile_runs); the x
+      // walls' values come with the staged rows' padding
       static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         constexpr int ey = D3Q27::ey[q], ez = D3Q27::ez[q];
-        constexpr int qb = D3Q27::bb[q];
-        if ((out_bits >> (3 * (1 - ez) + (1 - ey))) & 1u) raw[q] = pl.load_pair(qb, bself);
+        if ((out_bits >> (3 * (1 - ez) + (1 - ey))) & 1u) raw[q] = st[q * slotw + pw];
       });
     }
   } else if constexpr (RULE == CaseRule::SphereStd) {
