@@ -51,6 +51,7 @@ struct __align__(16) EngInst {
   int staged;    // 2-byte format, rows staged in shared memory (stage_core.cuh)
   int tw, th;    // cells of a tile along x and y
   stage::Geo geo;
+  uint16_t* rec[2];  // wall records of buf[0], buf[1] (staged 2-byte cavity), else null
 };
 
 struct Tile {
@@ -97,7 +98,10 @@ template <Store S, bool EXACT, Bc B, CaseRule RULE, bool X2>
 __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, const int t0, const int t1) {
   using T = typename StoreT<S>::T;
   constexpr int CPT = CellsPerThread<S>::value;
-  __shared__ EngInst sh;
+  // raw storage: EngInst has default member initialisers, which a
+  // __shared__ variable cannot run; every field is copied in below
+  __shared__ __align__(16) unsigned char sh_raw[sizeof(EngInst)];
+  EngInst& sh = *reinterpret_cast<EngInst*>(sh_raw);
   int loaded = -1;  // same tile sequence in every thread: a block-uniform value
   for (int t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
     const Tile tile = ea.tiles[t];
@@ -137,13 +141,16 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   using T = typename StoreT<S>::T;
   using namespace stage;
   constexpr bool WRAP = B == Bc::Periodic || RULE == CaseRule::SphereStd;
+  constexpr bool REC = RULE == CaseRule::CavityStd;  // wall records staged with the rows
   constexpr int NS = MAX_STAGES;
   constexpr int stage_elems = Q * (SLOT_UNITS / MAX_STAGES);
   extern __shared__ __align__(128) unsigned char smem[];
   T* stages = reinterpret_cast<T*>(smem);
   unsigned char* args = smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T);
-  uint64_t* full = reinterpret_cast<uint64_t*>(args + NS * STAGED_ARGS_BYTES);
+  unsigned char* recs = args + NS * STAGED_ARGS_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(recs + (REC ? NS * REC_STAGE_BYTES : 0));
   uint64_t* empty = full + NS;
+  auto rec_stage = [&](int sn) { return reinterpret_cast<uint16_t*>(recs + sn * REC_STAGE_BYTES); };
   __shared__ int abort_flag;
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) {
@@ -164,8 +171,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
     const EngInst* in = ea.inst + tile.slot;
     const int cur = (ea.parity ^ in->parity0) & 1;
     issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
-                        stages + sn * stage_elems, &full[sn], args + sn * STAGED_ARGS_BYTES, &in->a,
-                        static_cast<uint32_t>(STAGED_ARGS_BYTES));
+                        stages + sn * stage_elems, &full[sn], REC ? in->rec[cur] : nullptr, rec_stage(sn),
+                        args + sn * STAGED_ARGS_BYTES, &in->a, static_cast<uint32_t>(STAGED_ARGS_BYTES));
   };
   int issued = 0;
   if (warp == 0) {
@@ -201,7 +208,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
                            static_cast<int32_t>(a.sq)};
     const Geo g = in->geo;
     consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), tile.j0, tile.k,
-                             ea.store != 0);
+                             ea.store != 0, rec_stage(s), REC ? in->rec[1 - cur] : nullptr);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
@@ -213,9 +220,9 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   if (threadIdx.x == 0 && abort_flag) atomicOr(ea.err, 1);
 }
 
-inline size_t engine_staged_smem() {
+inline size_t engine_staged_smem(bool records) {
   return static_cast<size_t>(Q) * stage::SLOT_UNITS * 2 + stage::MAX_STAGES * STAGED_ARGS_BYTES +
-         16 * stage::MAX_STAGES;
+         (records ? stage::MAX_STAGES * stage::REC_STAGE_BYTES : 0) + 16 * stage::MAX_STAGES;
 }
 
 // Residual partial sums per tile: sum |u - u_prev|^2 and sum |u|^2 over the
@@ -551,11 +558,11 @@ int rebuild_tiles(imexlb_engine* e) {
 
 template <Store S>
 void set_staged_smem() {
-  const int smem = static_cast<int>(engine_staged_smem());
+  const int smem = static_cast<int>(engine_staged_smem(false));
   cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Periodic, CaseRule::None>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Standard, CaseRule::CavityStd>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(engine_staged_smem(true)));
   cudaFuncSetAttribute(engine_staged_kernel<S, Bc::Standard, CaseRule::SphereStd>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -569,7 +576,7 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
     if constexpr (S == Store::F16 || S == Store::BF16) {
       if (mode == 2) {
         const int grid = std::min(e->staged_resident, t1 - t0);
-        const size_t smem = engine_staged_smem();
+        const size_t smem = engine_staged_smem(rule == 1);
         if (rule == 0)
           engine_staged_kernel<S, Bc::Periodic, CaseRule::None><<<grid, stage::THREADS, smem, e->stream>>>(ea, t0, t1);
         else if (rule == 1)
@@ -658,15 +665,33 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
     if (storage == IMEXLB_F16)
       IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
           &per_sm, engine_staged_kernel<Store::F16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
-          engine_staged_smem()));
+          engine_staged_smem(true)));
     else
       IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
           &per_sm, engine_staged_kernel<Store::BF16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
-          engine_staged_smem()));
+          engine_staged_smem(true)));
     e->staged_resident = std::max(per_sm, 1) * sms;
   }
   *out = e.release();
   return IMEXLB_OK;
+}
+
+static CaseRule rule_of_case(int kase) {
+  return kase == IMEXLB_TGV ? CaseRule::None : (kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd);
+}
+
+// Rows of the instance staged in shared memory (2-byte formats, nx even,
+// rows that fit a stage and no register-staged tile width asked for).
+static bool instance_staged(int storage, const imexlb_instance_desc* d, const Layout& L, stage::Geo* g) {
+  const bool x2 = (storage == IMEXLB_F16 || storage == IMEXLB_BF16) && d->nx % 2 == 0;
+  return x2 && d->tile_bx <= 0 && stage::staged_layout(rule_of_case(d->kase), d->nx, d->ny, L.pitch, g);
+}
+
+// Bytes of one wall-record buffer of the instance (a staged cavity), else 0.
+static size_t record_bytes(int storage, const imexlb_instance_desc* d, const Layout& L) {
+  stage::Geo g;
+  if (d->kase != IMEXLB_CAVITY || !instance_staged(storage, d, L, &g)) return 0;
+  return (static_cast<size_t>(d->ny) * d->nz * WallRecord::BYTES + 511) & ~static_cast<size_t>(511);
 }
 
 int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot_out) {
@@ -685,7 +710,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   const int elem = e->storage == IMEXLB_F64 ? 8 : (e->storage == IMEXLB_F32 ? 4 : 2);
   Slot sl;
   sl.d = *d;
-  sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem, cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, e->storage));
+  sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem);
   if (static_cast<double>(sl.L.sq) * Q >= 2147483647.0) return efail(IMEXLB_E_ARG, "instance too large for the engine");
   sl.ncell = static_cast<int64_t>(d->nx) * d->ny * d->nz;
   const size_t fbytes = (sl.L.bytes() + 511) & ~static_cast<size_t>(511);
@@ -693,7 +718,8 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   const size_t pbytes = ((3 * sl.ncell * 8) + 511) & ~static_cast<size_t>(511);
   const size_t mask_bytes = static_cast<size_t>((sl.ncell + 255) & ~int64_t(255));
   const size_t sbytes = d->kase == IMEXLB_SPHERE ? ((mask_bytes + 4 * sl.ncell + 511) & ~static_cast<size_t>(511)) : 0;
-  sl.bytes = 2 * fbytes + mbytes + pbytes + sbytes;
+  const size_t rbytes = record_bytes(e->storage, d, sl.L);
+  sl.bytes = 2 * fbytes + mbytes + pbytes + sbytes + 2 * rbytes;
   if (!e->arena.alloc(sl.bytes, &sl.off))
     return efail(IMEXLB_E_NOMEM, "instance does not fit the engine's memory budget");
   char* b = e->arena.base + sl.off;
@@ -703,6 +729,8 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   double* prev = reinterpret_cast<double*>(b + 2 * fbytes + mbytes);
   uint8_t* usr = d->kase == IMEXLB_SPHERE ? reinterpret_cast<uint8_t*>(b + 2 * fbytes + mbytes + pbytes) : nullptr;
   uint32_t* links = usr ? reinterpret_cast<uint32_t*>(usr + mask_bytes) : nullptr;
+  uint16_t* rec0 = rbytes ? reinterpret_cast<uint16_t*>(b + 2 * fbytes + mbytes + pbytes + sbytes) : nullptr;
+  uint16_t* rec1 = rbytes ? reinterpret_cast<uint16_t*>(b + 2 * fbytes + mbytes + pbytes + sbytes + rbytes) : nullptr;
 
   // initial fields (the same set-up as a single lattice)
   imexlb_params P;
@@ -815,6 +843,8 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   }
   in.buf[0] = buf0;
   in.buf[1] = buf1;
+  in.rec[0] = rec0;
+  in.rec[1] = rec1;
   in.prev = prev;
   sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
   in.bx_log2 = sl.bx_log2;
@@ -822,7 +852,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   in.x2 = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
   // rows staged in shared memory where they fit a stage (and tile_bx asks
   // for no register-staged tile width)
-  in.staged = in.x2 && d->tile_bx <= 0 && stage::make_geo(d->ny, sl.L.pitch, &in.geo) ? 1 : 0;
+  in.staged = instance_staged(e->storage, d, sl.L, &in.geo) ? 1 : 0;
   if (in.staged) {
     in.tw = d->nx;
     in.th = in.geo.R;
@@ -834,8 +864,10 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
                 e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
-  if (cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, e->storage) && d->nx % 2 == 0)
-    IMX_ECUDA(launch_cavity_pad_init(sl.L, buf0, buf1, e->stream));
+  if (rec0) {
+    IMX_ECUDA(launch_cavity_records(sl.L, buf0, rec0, e->stream));
+    IMX_ECUDA(launch_cavity_records(sl.L, buf1, rec1, e->stream));
+  }
   std::memcpy(up + off_inst, &in, sizeof(EngInst));
   IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + s, up + off_inst, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
   // no wait: the uploads follow the work already queued on the stream, and
@@ -956,11 +988,12 @@ int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st) {
 int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes) {
   if (!d || !bytes) return efail(IMEXLB_E_ARG, "null argument");
   const int elem = storage == IMEXLB_F64 ? 8 : (storage == IMEXLB_F32 ? 4 : 2);
-  const Layout L = make_layout(d->nx, d->ny, d->nz, 0, elem, cavity_x_pad(d->kase, IMEXLB_BC_STANDARD, storage));
+  const Layout L = make_layout(d->nx, d->ny, d->nz, 0, elem);
   const int64_t n = static_cast<int64_t>(d->nx) * d->ny * d->nz;
   auto r = [](size_t x) { return (x + 511) & ~static_cast<size_t>(511); };
   const size_t mask = static_cast<size_t>((n + 255) & ~int64_t(255));
-  *bytes = 2 * r(L.bytes()) + r(4 * n * 8) + r(3 * n * 8) + (d->kase == IMEXLB_SPHERE ? r(mask + 4 * n) : 0);
+  *bytes = 2 * r(L.bytes()) + r(4 * n * 8) + r(3 * n * 8) + (d->kase == IMEXLB_SPHERE ? r(mask + 4 * n) : 0) +
+           2 * record_bytes(storage, d, L);
   return IMEXLB_OK;
 }
 
@@ -1033,6 +1066,7 @@ int imexlb_engine_restore(imexlb_engine* e, const imexlb_instance_desc* d, const
   // at admission the next step reads buf[0] (parity0 = engine step parity)
   const char* p = static_cast<const char*>(host) + sizeof c;
   IMX_ECUDA(cudaMemcpyAsync(in.buf[0], p, c.buf_bytes, cudaMemcpyHostToDevice, e->stream));
+  if (in.rec[0]) IMX_ECUDA(launch_cavity_records(sl.L, in.buf[0], in.rec[0], e->stream));
   p += c.buf_bytes;
   IMX_ECUDA(cudaMemcpyAsync(in.a.mu, p, c.mom_bytes, cudaMemcpyHostToDevice, e->stream));
   IMX_ECUDA(cudaStreamSynchronize(e->stream));

@@ -120,10 +120,13 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   using T = typename StoreT<S>::T;
   using namespace stage;
   constexpr bool WRAP = B == Bc::Periodic || RULE == CaseRule::SphereStd;
+  constexpr bool REC = RULE == CaseRule::CavityStd;  // wall records staged with the rows
   extern __shared__ __align__(128) unsigned char smem[];
   T* stages = reinterpret_cast<T*>(smem);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T));
+  unsigned char* recs = smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T);
+  uint64_t* full = reinterpret_cast<uint64_t*>(recs + (REC ? MAX_STAGES * REC_STAGE_BYTES : 0));
   uint64_t* empty = full + MAX_STAGES;
+  auto rec_stage = [&](int sn) { return reinterpret_cast<uint16_t*>(recs + sn * REC_STAGE_BYTES); };
   __shared__ int abort_flag;
   const int NS = g.stages;
   const int stage_elems = Q * g.cap;
@@ -149,7 +152,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
     for (; issued < NS - 1; ++issued) {
       const int t = blockIdx.x + issued * grid;
       if (t >= ntiles) break;
-      issue_tile<T, WRAP>(a, g, src, (t % g.nty) * g.R, t / g.nty, stages + issued * stage_elems, &full[issued]);
+      issue_tile<T, WRAP>(a, g, src, (t % g.nty) * g.R, t / g.nty, stages + issued * stage_elems, &full[issued],
+                          REC ? a.rec_src : nullptr, rec_stage(issued));
     }
   }
   int i = 0;
@@ -165,7 +169,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
           break;
         }
         const int sn = (i + NS - 1) % NS;
-        issue_tile<T, WRAP>(a, g, src, (tn % g.nty) * g.R, tn / g.nty, stages + sn * stage_elems, &full[sn]);
+        issue_tile<T, WRAP>(a, g, src, (tn % g.nty) * g.R, tn / g.nty, stages + sn * stage_elems, &full[sn],
+                            REC ? a.rec_src : nullptr, rec_stage(sn));
         ++issued;
       }
     }
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       break;
     }
     const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
-    consume_tile<S, B, RULE>(a, pl, g, st, (t % g.nty) * g.R, t / g.nty, a.store != 0);
+    consume_tile<S, B, RULE>(a, pl, g, st, (t % g.nty) * g.R, t / g.nty, a.store != 0, rec_stage(s), a.rec_dst);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
@@ -187,28 +192,23 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   if (threadIdx.x == 0 && abort_flag) atomicOr(a.err, 1);
 }
 
-// 2-byte standard cavity: the padding after each stored row carries the
-// bounce-back values of its x walls (stage_core.cuh).  For the row (jj, kk)
-// of population q with e_x = +1, element pitch - 1 holds f(bb(q)) of the
-// cell (0, jj + e_y, kk + e_z), whose pull along e_q starts at x = -1; with
-// e_x = -1, element nx holds f(bb(q)) of the cell (nx - 1, jj + e_y, kk + e_z).
-// This fills them for the initial state; the step kernels refresh them.
-__global__ void cavity_pad_init_kernel(const Layout L, uint16_t* b0, uint16_t* b1) {
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x, kk = blockIdx.y;
-  if (jj >= L.ny) return;
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q], qb = D3Q27::bb[q];
-    if constexpr (ex != 0) {
-      const int j = jj + ey, k = kk + ez;
-      if (j >= 0 && j < L.ny && k >= 0 && k < L.nz) {
-        const int64_t from = L.idx(qb, ex > 0 ? 0 : L.nx - 1, j, k);
-        const int64_t to = L.idx(q, ex > 0 ? static_cast<int>(L.pitch - L.xoff) - 1 : L.nx, jj, kk);
-        b0[to] = b0[from];
-        b1[to] = b1[from];
-      }
-    }
-  });
+// 2-byte standard cavity: the wall records (WallRecord) of buffer `buf`,
+// gathered from its x-wall cells: the state a step leaves them in, for the
+// initial state and a loaded checkpoint.  One thread per row (j, k).
+__global__ void cavity_records_kernel(const Layout L, const uint16_t* buf, uint16_t* rec) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (j >= L.ny) return;
+  uint32_t w[WallRecord::WORDS / 2] = {};
+#pragma unroll
+  for (int m = 0; m < WallRecord::SLOTS; ++m) {
+    const int p = WallRecord::pos(m);
+    const uint32_t lo = buf[L.idx(p + 1, 0, j, k)], hi = buf[L.idx(p, L.nx - 1, j, k)];
+    w[m >> 1] |= lo << (16 * (m & 1));
+    w[(WallRecord::HI + m) >> 1] |= hi << (16 * (m & 1));
+  }
+  uint4* out = reinterpret_cast<uint4*>(rec + (static_cast<int64_t>(k) * L.ny + j) * WallRecord::WORDS);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) out[c] = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
 }
 
 // Momentum-exchange drag of the 2-byte sphere channel, from the buffer a
@@ -406,7 +406,12 @@ static bool use_x2(Store s, int nx) { return (s == Store::F16 || s == Store::BF1
 static bool staged_geo(const LaunchCfg& c, int nx, int ny, int64_t pitch, stage::Geo* g) {
   if (!use_x2(c.store, nx)) return false;
   if (c.bc != Bc::Standard && c.bc != Bc::Periodic) return false;
-  return stage::make_geo(ny, pitch, g);
+  return stage::staged_layout(c.rule, nx, ny, pitch, g);
+}
+
+bool uses_wall_records(const LaunchCfg& c, int nx, int ny, int64_t pitch) {
+  stage::Geo g;
+  return c.rule == CaseRule::CavityStd && staged_geo(c, nx, ny, pitch, &g);
 }
 
 // Blocks of the persistent staged grid: as many as fit on the device at
@@ -426,7 +431,7 @@ template <Store S, Bc B, CaseRule R>
 static int staged_blocks(const stage::Geo& g, int nz) {
   static int resident = 0;  // blocks of this kernel resident on the device
   if (resident == 0) {
-    const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)));
+    const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)), R == CaseRule::CavityStd);
     cudaFuncSetAttribute(staged_kernel<S, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_kernel<S, B, R>, stage::THREADS, smem);
@@ -438,7 +443,8 @@ static int staged_blocks(const stage::Geo& g, int nz) {
 
 template <Store S, Bc B, CaseRule R>
 static cudaError_t launch_staged(const StepArgs& a, const stage::Geo& g, cudaStream_t s) {
-  const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)));
+  const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)), R == CaseRule::CavityStd);
+  if (R == CaseRule::CavityStd && (!a.rec_src || !a.rec_dst)) return cudaErrorInvalidValue;
   const int blocks = staged_blocks<S, B, R>(g, a.nz);
   staged_kernel<S, B, R><<<blocks, stage::THREADS, smem, s>>>(a, g);
   return cudaGetLastError();
@@ -469,9 +475,73 @@ int64_t step_grid_blocks(const LaunchCfg& c, int nx, int ny, int nz) {
   return static_cast<int64_t>((nx + b.x - 1) / b.x) * ((ny + rows - 1) / rows) * nz;
 }
 
-cudaError_t launch_cavity_pad_init(const Layout& L, void* buf0, void* buf1, cudaStream_t s) {
+// The staged kernels' copy plan of one 2-byte lattice, from the same
+// tile_runs the kernels run (see imexlb_debug_stage_plan).
+int64_t stage_plan(int nx, int ny, int nz, bool wrap_yz, int32_t* geo, int32_t* runs, int64_t max_runs) {
+  const Layout L = make_layout(nx, ny, nz, 0, 2);
+  stage::Geo g;
+  const CaseRule rule = wrap_yz ? CaseRule::None : CaseRule::CavityStd;
+  if (!stage::staged_layout(rule, nx, ny, L.pitch, &g)) return -1;
+  StepArgs a;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.base32 = static_cast<int32_t>(L.idx(0, 0, 0, 0));
+  a.sz32 = static_cast<int32_t>(L.sz);
+  a.pitch32 = static_cast<int32_t>(L.pitch);
+  if (geo) {
+    const int32_t v[8] = {g.P, g.R, g.cap, g.nty, static_cast<int32_t>(L.sq), a.sz32, a.pitch32, a.base32};
+    for (int i = 0; i < 8; ++i) geo[i] = v[i];
+  }
+  int64_t n = 0;
+  for (int t = 0; t < g.nty * nz; ++t) {
+    const int j0 = (t % g.nty) * g.R, k = t / g.nty;
+    const int rv = ny - j0 < g.R ? ny - j0 : g.R;
+    for (int q = 0; q < Q; ++q) {
+      stage::Run m{0, 0, 0u, q}, w{0, 0, 0u, q};
+      if (wrap_yz)
+        stage::tile_runs<true>(a, g, q, j0, k, rv, 2, m, w);
+      else
+        stage::tile_runs<false>(a, g, q, j0, k, rv, 2, m, w);
+      for (const stage::Run* r : {&m, &w}) {
+        if (!r->bytes) continue;
+        if (runs && n < max_runs) {
+          int32_t* o = runs + 6 * n;
+          o[0] = t;
+          o[1] = q;
+          o[2] = r->pop;
+          o[3] = r->src;
+          o[4] = r->dst;
+          o[5] = static_cast<int32_t>(r->bytes);
+        }
+        ++n;
+      }
+    }
+    if (rule == CaseRule::CavityStd) {
+      // the wall records: "population" Q, element offsets into the record
+      // buffer and the stage's record area
+      int64_t rsrc = 0;
+      uint32_t rbytes = 0;
+      stage::tile_records(a, j0, k, rv, rsrc, rbytes);
+      if (runs && n < max_runs) {
+        int32_t* o = runs + 6 * n;
+        o[0] = t;
+        o[1] = Q;
+        o[2] = -1;
+        o[3] = static_cast<int32_t>(rsrc);
+        o[4] = 0;
+        o[5] = static_cast<int32_t>(rbytes);
+      }
+      ++n;
+    }
+  }
+  return n;
+}
+
+cudaError_t launch_cavity_records(const Layout& L, const void* buf, uint16_t* rec, cudaStream_t s) {
+  if (L.elem != 2 || L.g != 0) return cudaErrorInvalidValue;
   const dim3 block(64, 1, 1), grid((L.ny + 63) / 64, L.nz, 1);
-  cavity_pad_init_kernel<<<grid, block, 0, s>>>(L, static_cast<uint16_t*>(buf0), static_cast<uint16_t*>(buf1));
+  cavity_records_kernel<<<grid, block, 0, s>>>(L, static_cast<const uint16_t*>(buf), rec);
   return cudaGetLastError();
 }
 

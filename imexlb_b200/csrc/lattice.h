@@ -42,12 +42,7 @@ struct Layout {
   IMX_HD int64_t interior(int q, int i, int j, int k) const { return idx(q, i + g, j + g, k + g); }
   size_t bytes() const { return static_cast<size_t>(sq) * Q * elem; }
 };
-// xpad: stored elements kept free after the last stored x of each row (the
-// 2-byte standard cavity keeps 2 for the bounce-back of its x walls, see
-// cavity_x_pad and stage_core.cuh).
-Layout make_layout(int nx, int ny, int nz, int g, int elem, int xpad = 0);
-// Row padding of a lattice of this case, boundary and storage.
-int cavity_x_pad(int kase, int bc, int storage);
+Layout make_layout(int nx, int ny, int nz, int g, int elem);
 
 // Per-population scaling of reduced-precision storage:
 // stored = d_q * scale[q], d_q = stored * inv_scale[q], where d_q is the
@@ -110,6 +105,10 @@ struct StepArgs {
   double inlet_u = 0;     // standard sphere inlet velocity
   double* drag_part = nullptr;  // standard sphere: per-block momentum-exchange partials (3 per block), or null
   int* err = nullptr;  // set non-zero by a kernel that gave up waiting (staged steps)
+  // 2-byte standard cavity, staged kernels: the wall records of the buffer
+  // read and of the buffer written (WallRecord)
+  const uint16_t* rec_src = nullptr;
+  uint16_t* rec_dst = nullptr;
 };
 // Bytes of the StepArgs prefix the staged kernels read, rounded to 16.
 constexpr size_t STAGED_ARGS_BYTES = (offsetof(StepArgs, src) + 15) & ~static_cast<size_t>(15);
@@ -166,9 +165,20 @@ struct LaunchCfg {
   bool exact;
 };
 
-// 2-byte standard cavity: fill each row's x-wall padding of both buffers
-// with the bounce-back values of the initial state (stage_core.cuh).
-cudaError_t launch_cavity_pad_init(const Layout& L, void* buf0, void* buf1, cudaStream_t s);
+// The staged kernels of this configuration keep wall records (WallRecord,
+// one per row (j, k), ny * nz * WallRecord::BYTES bytes a buffer parity).
+bool uses_wall_records(const LaunchCfg& c, int nx, int ny, int64_t pitch);
+// Fill the wall records of distribution buffer `buf` (a 2-byte layout),
+// after the buffer was written other than by a step.
+cudaError_t launch_cavity_records(const Layout& L, const void* buf, uint16_t* rec, cudaStream_t s);
+// Copy plan of the shared-memory staged kernels for a 2-byte lattice of
+// nx x ny x nz with y / z wrapping (periodic, sphere) or walls (cavity).
+// geo (8 values): P, R, cap, nty, then the layout's sq, sz, pitch and base.
+// runs: up to max_runs records (tile, q, population read, source element,
+// stage element, bytes); the cavity's wall-record copy of a tile has q = Q,
+// population -1 and its element offset in the record buffer.  Returns the
+// number of copies, or -1 when the lattice is not staged.
+int64_t stage_plan(int nx, int ny, int nz, bool wrap_yz, int32_t* geo, int32_t* runs, int64_t max_runs);
 cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void* buf1, const double* u,
                           const double* v, const double* w, const double* p, double p_shift, const Encoding& enc,
                           cudaStream_t s);

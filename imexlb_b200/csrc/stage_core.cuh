@@ -10,12 +10,13 @@
 //
 // A tile is R whole rows [j0, j0 + R) of plane k.  Population q of those
 // cells pulls from rows j0 - e_y .. j0 + R - 1 - e_y of plane k - e_z,
-// shifted by e_x along x.  The 2-byte layouts pad rows to 16 elements only,
+// shifted by e_x along x.  The 2-byte layouts pad rows to 8 elements only,
 // so those R source rows are one contiguous run of memory and a tile needs
-// one bulk copy per population (two where a periodic y wraps).  Whole rows
-// also hold the x wrap of a periodic lattice.  A source plane outside the
-// box is not copied: the cavity's walls replace those values (halfway
-// bounce-back), and a periodic axis copies the wrapped plane.  Each copy
+// one bulk copy per population (two where a y wall or a periodic y cuts
+// the run).  Whole rows also hold the x wrap of a periodic lattice.  A
+// periodic y or z copies the wrapped rows; beyond a cavity wall the halfway
+// bounce-back returns the cell's own opposite population, so the producer
+// copies the tile's own rows of bb(q) into those slot rows.  Each copy
 // costs the copy engine about the same whatever its size, so few large
 // copies per tile are what keep DRAM busy.
 //
@@ -25,11 +26,12 @@
 // counts the tile's bytes.  Every warp waits on "full", updates its cells
 // and releases the stage.  Each thread updates x-pairs of cells with the
 // same arithmetic as the register-staged x-pair kernels (finish_pair_row).
-// The cavity's x-wall bounce-back values travel in the padding after each
-// row (a cell at an x wall also writes its opposite populations there, see
-// finish_pair_row), so its x walls cost nothing here; the y / z walls and a
-// sphere's solid links read the cell's own opposite population from global
-// memory, in a second pass that only boundary pairs take.
+// The cavity's x-wall bounce-back values travel in wall records, one per
+// row (WallRecord): the x-wall cells of a step write them (finish_pair_row),
+// and the next step's tile copies the records of its rows with one more
+// bulk copy, so no wall reads global memory here; only a sphere's solid
+// links read the cell's own opposite population from global memory, in a
+// second pass that only linked pairs take.
 //
 // Every wait on an mbarrier gives up after about a second of wall-clock time
 // (%globaltimer), records the failure in the step's error word and leaves
@@ -57,23 +59,45 @@ struct Geo {
   int nty;     // tiles along y
 };
 
-// Whole-row tiles for rows of `pitch` elements (a multiple of 16, at most
-// 1024): population slots of 1024 elements in 2 stages.  Fewer, larger
-// copies beat deeper pipelines here (2 KB copies in 2 stages measured
-// faster than 1 KB copies in 4 stages of the same shared memory).
-inline bool make_geo(int ny, int64_t pitch, Geo* g) {
-  if (pitch % 16 != 0 || pitch > 1024) return false;
+// The 2-byte cavity's tiles also stage the wall records of their rows
+// (WallRecord, 64 bytes a row) in an area of REC_ROWS records per stage.
+constexpr int REC_ROWS = 16;
+constexpr int REC_STAGE_BYTES = REC_ROWS * WallRecord::BYTES;
+
+// Whole-row tiles for rows of `pitch` elements (a multiple of 8, so that
+// every row starts on a 16-byte boundary; at most 1024): population slots
+// of 1024 elements in 2 stages, at most `max_rows` rows a tile.  Fewer,
+// larger copies beat deeper pipelines here (2 KB copies in 2 stages
+// measured faster than 1 KB copies in 4 stages of the same shared memory).
+inline bool make_geo(int ny, int64_t pitch, Geo* g, int max_rows = 1024) {
+  if (pitch % 8 != 0 || pitch > 1024) return false;
   g->P = static_cast<int>(pitch);
   g->cap = 1024;
   g->stages = SLOT_UNITS / g->cap;
   g->R = g->cap / g->P;
+  if (g->R > max_rows) g->R = max_rows;
   if (g->R > ny) g->R = ny;
   g->nty = (ny + g->R - 1) / g->R;
   return true;
 }
 
-// stages of 27 population slots, then the full and empty mbarriers
-inline size_t smem_bytes(int elem) { return static_cast<size_t>(27) * SLOT_UNITS * elem + 16 * MAX_STAGES; }
+// Tile geometry of the staged kernels for a lattice of nx x ny cells with
+// rows of `pitch` elements, or false when it is not staged: nx even (the
+// x-pairs); the cavity (wall records) at most REC_ROWS rows a tile and
+// nx >= 4, so that a pair holds at most one x-wall cell.
+inline bool staged_layout(CaseRule rule, int nx, int ny, int64_t pitch, Geo* g) {
+  if (nx % 2 != 0) return false;
+  const bool rec = rule == CaseRule::CavityStd;
+  if (rec && nx < 4) return false;
+  return make_geo(ny, pitch, g, rec ? REC_ROWS : 1024);
+}
+
+// stages of 27 population slots, the wall-record areas (cavity), then the
+// full and empty mbarriers
+inline size_t smem_bytes(int elem, bool records) {
+  return static_cast<size_t>(27) * SLOT_UNITS * elem + (records ? MAX_STAGES * REC_STAGE_BYTES : 0) +
+         16 * MAX_STAGES;
+}
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -139,8 +163,8 @@ constexpr uint64_t pack_axis(int axis) {
   return v;
 }
 constexpr uint64_t EY_BITS = pack_axis(1), EZ_BITS = pack_axis(2);
-__device__ __forceinline__ int ey_of(int q) { return static_cast<int>((EY_BITS >> (2 * q)) & 3u) - 1; }
-__device__ __forceinline__ int ez_of(int q) { return static_cast<int>((EZ_BITS >> (2 * q)) & 3u) - 1; }
+__host__ __device__ __forceinline__ int ey_of(int q) { return static_cast<int>((EY_BITS >> (2 * q)) & 3u) - 1; }
+__host__ __device__ __forceinline__ int ez_of(int q) { return static_cast<int>((EZ_BITS >> (2 * q)) & 3u) - 1; }
 
 // The copies of population q for a tile: the source rows of tile rows
 // [0, rv) as at most two contiguous runs, the second one a wrapped row
@@ -165,9 +189,10 @@ struct Run {
 // (WRAP_YZ false: the cavity) the halfway bounce-back returns the cell's own
 // opposite population instead, so slot q's rows whose source is outside the
 // box receive the tile's own rows of bb(q) (plane k, rows j0 + r), which the
-// consumer reads unshifted.
+// consumer reads unshifted.  Also compiled for the host, where
+// imexlb_debug_stage_plan lists the copies for checks on the CPU.
 template <bool WRAP_YZ>
-__device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q, int j0, int k, int rv, int elem,
+__host__ __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q, int j0, int k, int rv, int elem,
                                           Run& main, Run& wrap) {
   main.bytes = 0;
   wrap.bytes = 0;
@@ -205,49 +230,65 @@ __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q
   wrap.bytes = (first || last) ? static_cast<uint32_t>(g.P * elem) : 0u;
 }
 
+// The wall records of tile rows [j0, j0 + rv) of plane k: one contiguous
+// run (element offset into the record buffer, bytes).
+__host__ __device__ __forceinline__ void tile_records(const StepArgs& a, int j0, int k, int rv, int64_t& src,
+                                                      uint32_t& bytes) {
+  src = (static_cast<int64_t>(k) * a.ny + j0) * WallRecord::WORDS;
+  bytes = static_cast<uint32_t>(rv * WallRecord::BYTES);
+}
+
 // Issue the copies of tile (j0, k) into stage `st` (called by a whole warp;
 // lane q < 27 copies population q).  `src` is the buffer being read,
-// population q at q * a.sq.  Lane 31 also copies `xbytes` (a multiple of
-// 16, 0 for none) from `xsrc` to `xdst` on the same mbarrier.
+// population q at q * a.sq.  Lane 30 copies the tile's wall records from
+// `rec_src` (a 2-byte cavity; null for none) to `rec_st`; lane 31 copies
+// `xbytes` (a multiple of 16, 0 for none) from `xsrc` to `xdst`; all on the
+// same mbarrier.
 template <class T, bool WRAP_YZ>
 __device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, const T* src, int j0, int k, T* st,
-                                           uint64_t* bar, void* xdst = nullptr, const void* xsrc = nullptr,
-                                           uint32_t xbytes = 0) {
+                                           uint64_t* bar, const uint16_t* rec_src = nullptr,
+                                           uint16_t* rec_st = nullptr, void* xdst = nullptr,
+                                           const void* xsrc = nullptr, uint32_t xbytes = 0) {
   const int lane = threadIdx.x & 31;
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   Run m{0, 0, 0u}, w{0, 0, 0u};
   if (lane < Q) tile_runs<WRAP_YZ>(a, g, lane, j0, k, rv, static_cast<int>(sizeof(T)), m, w);
-  uint32_t total = m.bytes + w.bytes + (lane == 31 ? xbytes : 0u);
+  int64_t rsrc = 0;
+  uint32_t rbytes = 0;
+  if (lane == 30 && rec_src) tile_records(a, j0, k, rv, rsrc, rbytes);
+  uint32_t total = m.bytes + w.bytes + rbytes + (lane == 31 ? xbytes : 0u);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
   if (lane == 0) bar_arrive_expect(bar, total);
   __syncwarp();
   if (m.bytes) bulk_g2s(st + m.dst, src + static_cast<int64_t>(m.pop) * a.sq + m.src, m.bytes, bar);
   if (w.bytes) bulk_g2s(st + w.dst, src + static_cast<int64_t>(w.pop) * a.sq + w.src, w.bytes, bar);
+  if (rbytes) bulk_g2s(rec_st, rec_src + rsrc, rbytes, bar);
   if (lane == 31 && xbytes) bulk_g2s(xdst, xsrc, xbytes, bar);
 }
 
 // The x-pair (x, x + 1) in tile row r of tile (j0, k), read from the staged
-// rows.  `st` is the stage as 4-byte words.  Boundary values (halfway
-// bounce-back at the cavity's walls, solid links of the sphere) are put in
-// place by a second pass that only boundary pairs take.  Reads only the
-// fields of `a` before StepArgs::src.  EDGE = false
-// promises that no boundary rule of the box applies to the pair:
-// 2 <= x < nx - 2 and, for the cavity, no wall row or plane around it.
+// rows.  `st` is the stage as 4-byte words.  Reads only the fields of `a`
+// before StepArgs::src.  EDGE = false promises that no boundary rule of the
+// box applies to the pair but the cavity's x walls: for the cavity, no wall
+// row or plane around it.  Cavity: `rec` is the stage's wall records (tile
+// row r at r * WallRecord::WORDS), `rec_row` the pair's row in the record
+// buffer this step writes.
 template <Store S, Bc B, CaseRule RULE, bool EDGE, class P>
 __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                                 const int x, const int r, const int j0, const int k,
-                                                const bool store) {
+                                                const bool store, const uint16_t* rec = nullptr,
+                                                uint16_t* rec_row = nullptr) {
   const int j = j0 + r;
   const int row = (r * g.P) >> 1;  // word offset of tile row r in a slot
   const int pw = row + (x >> 1);
   const bool left_edge = EDGE && x == 0, right_edge = EDGE && x + 2 >= a.nx;
   int lw, rw;  // the pairs holding x - 1 and x + 2
   if constexpr (RULE == CaseRule::CavityStd) {
-    // the row's padding holds the x walls' bounce-back values: x = -1 is
-    // element P - 1, x = nx element nx
-    lw = row + ((x == 0 ? g.P - 2 : x - 2) >> 1);
-    rw = row + ((x + 2) >> 1);
+    // at an x wall the value comes from the wall record below; read the
+    // pair's own word there, inside the row
+    lw = row + ((x == 0 ? x : x - 2) >> 1);
+    rw = row + ((x + 2 >= a.nx ? x : x + 2) >> 1);
   } else {
     lw = row + ((x == 0 ? a.nx - 2 : x - 2) >> 1);  // wrapped inside the row
     rw = row + ((x + 2 >= a.nx ? 0 : x + 2) >> 1);
@@ -276,6 +317,28 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
   const int32_t bself = a.base32 + k * a.sz32 + j * a.pitch32 + x;
   bool live0 = true, live1 = true;
   uint32_t links0 = 0, links1 = 0;  // sphere: solid-link bits of the two cells
+  if constexpr (RULE == CaseRule::CavityStd) {
+    // halfway bounce-back at the x walls: the cell's own opposite population
+    // of the last step, from the row's wall record (x = 0: the lo side, for
+    // e_x = +1; x = nx - 1: the hi side, for e_x = -1).  A y / z wall
+    // crossed by the same link overrides it below with the same value.
+    if (x == 0 || x + 2 >= a.nx) {
+      const uint16_t* rr = rec + r * WallRecord::WORDS;
+      const bool lo = x == 0;
+      static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int ex = D3Q27::ex[q];
+        if constexpr (ex != 0) {
+          constexpr int m = WallRecord::slot(q);
+          if constexpr (ex > 0) {
+            if (lo) raw[q] = (raw[q] & 0xffff0000u) | rr[m];
+          } else {
+            if (!lo) raw[q] = (raw[q] & 0xffffu) | (static_cast<uint32_t>(rr[WallRecord::HI + m]) << 16);
+          }
+        }
+      });
+    }
+  }
   if constexpr (RULE == CaseRule::CavityStd && EDGE) {
     uint32_t out_bits = 0;  // bit (3 dz + dy): source row outside the box
 #pragma unroll
@@ -288,8 +351,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
     if (out_bits) {
       // halfway bounce-back at the y and z walls: a link leaving the box
       // returns the cell's own opposite population, which the producer put
-      // in slot q in place of the missing source row (tile_runs); the x
-      // walls' values come with the staged rows' padding
+      // in slot q in place of the missing source row (tile_runs)
       static_for<0, Q>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         constexpr int ey = D3Q27::ey[q], ez = D3Q27::ez[q];
@@ -320,31 +382,40 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
       }
     }
   }
-  const bool lid = RULE == CaseRule::CavityStd && k == a.nz - 1;
-  finish_pair_row<S, RULE>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store, links0, links1);
+  // the lid plane is a wall plane: only EDGE pairs can sit under it
+  const bool lid = RULE == CaseRule::CavityStd && EDGE && k == a.nz - 1;
+  finish_pair_row<S, RULE, RULE == CaseRule::CavityStd>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store,
+                                                        links0, links1, rec_row);
 }
 
-// The cells of tile (j0, k) from stage `st`, shared by the block's threads.
+// The cells of tile (j0, k) from stage `st`, shared by the block's threads:
+// thread slot p is the pair at x = 2 (p mod P/2) of tile row p div P/2, so
+// a warp's pairs, and its stores, follow the rows' alignment in memory
+// (mapping only the pairs inside the box, so that warps start mid-row,
+// spread each warp's stores over more sectors and measured slower).
 // Cavity pairs in a wall row or plane take the checked path (y / z
 // bounce-back; a warp holds pairs of one or two rows, so the choice is
-// nearly uniform across it); the others need no check, since the x walls'
-// values come with the staged rows' padding.
+// nearly uniform across it).  Cavity: `rec` is the stage's wall records,
+// `rec_out` the record buffer this step writes.
 template <Store S, Bc B, CaseRule RULE, class P>
 __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
-                                             const int j0, const int k, const bool store) {
+                                             const int j0, const int k, const bool store,
+                                             const uint16_t* rec = nullptr, uint16_t* rec_out = nullptr) {
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   const int half = g.P >> 1;
   const int npairs = g.R * half;
   if constexpr (RULE == CaseRule::CavityStd) {
     const bool wall_plane = k == 0 || k == a.nz - 1;
+    uint16_t* const rec_tile = rec_out + (static_cast<int64_t>(k) * a.ny + j0) * WallRecord::WORDS;
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
       const int r = p / half, x = 2 * (p - r * half);
       if (r >= rv || x >= a.nx) continue;
       const int j = j0 + r;
+      uint16_t* const rec_row = rec_tile + r * WallRecord::WORDS;
       if (wall_plane || j == 0 || j == a.ny - 1)
-        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
       else
-        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store);
+        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
     }
   } else {
     for (int p = threadIdx.x; p < npairs; p += THREADS) {

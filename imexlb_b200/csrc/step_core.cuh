@@ -434,8 +434,64 @@ __device__ __forceinline__ float2 fma2rn(float2 a, float2 b, float2 c) {
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
   return d;
 }
+__device__ __forceinline__ float2 sub2rn(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+// e = c_q . u of a pair without negations.  Round-to-nearest is symmetric
+// in sign, so (-x) + y rounds to y - x and (-x) + (-y) to -(x + y): the
+// value equals the left-to-right sum of the signed components (edu2), or
+// its negation when edu_neg<q>() is true; callers fold that sign into the
+// constants the value is multiplied by.
+template <int q>
+constexpr bool edu_neg() {
+  constexpr int s[3] = {D3Q27::ex[q], D3Q27::ey[q], D3Q27::ez[q]};
+  int sg[3] = {0, 0, 0}, n = 0;
+  for (int i = 0; i < 3; ++i)
+    if (s[i] != 0) sg[n++] = s[i];
+  if (n == 1) return sg[0] < 0;
+  if (n == 2) return sg[0] < 0 && sg[1] < 0;
+  return n == 3 && sg[0] < 0 && sg[1] < 0 && sg[2] < 0;
+}
+
+// s1 x + s2 y for signs s1, s2 = +-1, negated when both are negative
+template <int s1, int s2>
+__device__ __forceinline__ float2 signed_sum2(float2 x, float2 y) {
+  if constexpr (s1 > 0 && s2 > 0) return add2rn(x, y);
+  else if constexpr (s1 > 0) return sub2rn(x, y);
+  else if constexpr (s2 > 0) return sub2rn(y, x);
+  else return add2rn(x, y);
+}
+
+template <int q>
+__device__ __forceinline__ float2 edu2f(float2 u, float2 v, float2 w) {
+  constexpr int a = D3Q27::ex[q], b = D3Q27::ey[q], c = D3Q27::ez[q];
+  if constexpr (a != 0 && b != 0 && c != 0) {
+    const float2 t = signed_sum2<a, b>(u, v);
+    constexpr bool tneg = a < 0 && b < 0;
+    if constexpr (!tneg) return c > 0 ? add2rn(t, w) : sub2rn(t, w);
+    else return c > 0 ? sub2rn(w, t) : add2rn(t, w);
+  } else if constexpr (a != 0 && b != 0) {
+    return signed_sum2<a, b>(u, v);
+  } else if constexpr (a != 0 && c != 0) {
+    return signed_sum2<a, c>(u, w);
+  } else if constexpr (b != 0 && c != 0) {
+    return signed_sum2<b, c>(v, w);
+  } else if constexpr (a != 0) {
+    return u;
+  } else if constexpr (b != 0) {
+    return v;
+  } else {
+    return w;
+  }
+}
 
 template <int q>
 __device__ __forceinline__ float2 edu2(float2 u, float2 v, float2 w) {
@@ -476,11 +532,11 @@ __device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, con
     const float2 x = f2(f0[q], f1[q]);
     s = add2rn(s, x);
     if constexpr (D3Q27::ex[q] == 1) u = add2rn(u, x);
-    if constexpr (D3Q27::ex[q] == -1) u = add2rn(u, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ex[q] == -1) u = sub2rn(u, x);
     if constexpr (D3Q27::ey[q] == 1) v = add2rn(v, x);
-    if constexpr (D3Q27::ey[q] == -1) v = add2rn(v, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ey[q] == -1) v = sub2rn(v, x);
     if constexpr (D3Q27::ez[q] == 1) w = add2rn(w, x);
-    if constexpr (D3Q27::ez[q] == -1) w = add2rn(w, f2(-x.x, -x.y));
+    if constexpr (D3Q27::ez[q] == -1) w = sub2rn(w, x);
   });
   float2 p = mul2rn(s, f2s(1.0f / 3.0f));
   case_rules<RULE>(a, i, k, c0, u.x, v.x, w.x, p.x);
@@ -505,10 +561,10 @@ __device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, con
     constexpr int cls = D3Q27::wclass[q];
     const float2 e = edu2<q>(u, v, w);
     // t (3e + 4.5 e^2 - 1.5 u.u) + 3 t p, with e (3 + 4.5 e) for the bracket
-    const float2 br = add2rn(mul2rn(e, fma2rn(e, f2s(4.5f), f2s(3.0f))), f2(-udu15.x, -udu15.y));
+    const float2 br = sub2rn(mul2rn(e, fma2rn(e, f2s(4.5f), f2s(3.0f))), udu15);
     const float2 feq = fma2rn(f2s(wgt<float>(cls)), br, tp3[cls]);
     const float2 x = f2(f0[q], f1[q]);
-    const float2 fs = fma2rn(om, add2rn(x, f2(-feq.x, -feq.y)), x);
+    const float2 fs = fma2rn(om, sub2rn(x, feq), x);
     pl.store(q, b0, encode<S>(fs.x, q, a.enc));
     pl.store(q, b1, encode<S>(fs.y, q, a.enc));
   });
@@ -610,11 +666,18 @@ __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { retu
 // subtracts omega unit br_ref[q] (Encoding::kref) and populations bounced off
 // the solid (links0 / links1, bit q) are corrected.  live0 / live1: the cell is fluid (a solid
 // cell's values are left as they are); store: write the moments.
-template <Store S, CaseRule RULE, class P>
+//
+// REC (2-byte cavity, staged kernels): an x-wall cell also writes its
+// row's wall record (`rec_row`, WallRecord layout): the post-collision
+// values the halfway bounce-back returns to it next step, 32 bytes per wall
+// side in three aligned stores, so that the next step's tile finds them in
+// one bulk copy instead of nine scattered rows.
+template <Store S, CaseRule RULE, bool REC = false, class P>
 __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
                                                 const bool live0, const bool live1, const bool store,
-                                                const uint32_t links0 = 0, const uint32_t links1 = 0) {
+                                                const uint32_t links0 = 0, const uint32_t links1 = 0,
+                                                uint16_t* rec_row = nullptr) {
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
   [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
@@ -632,11 +695,11 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     const float2 d = mul2rn(x, f2s(a.enc.inv_scale[q]));
     s = add2rn(s, d);
     if constexpr (ex == 1) u = add2rn(u, d);
-    if constexpr (ex == -1) u = add2rn(u, f2(-d.x, -d.y));
+    if constexpr (ex == -1) u = sub2rn(u, d);
     if constexpr (ey == 1) v = add2rn(v, d);
-    if constexpr (ey == -1) v = add2rn(v, f2(-d.x, -d.y));
+    if constexpr (ey == -1) v = sub2rn(v, d);
     if constexpr (ez == 1) w = add2rn(w, d);
-    if constexpr (ez == -1) w = add2rn(w, f2(-d.x, -d.y));
+    if constexpr (ez == -1) w = sub2rn(w, d);
     g[q] = x;
   });
   if constexpr (RULE == CaseRule::SphereStd) {
@@ -654,9 +717,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
           g[q] = add2rn(g[q], dg);
           const float2 dd = mul2rn(dg, f2s(a.enc.inv_scale[q]));
           s = add2rn(s, dd);
-          u = ex > 0 ? add2rn(u, dd) : add2rn(u, f2(-dd.x, -dd.y));
-          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : add2rn(v, f2(-dd.x, -dd.y));
-          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : add2rn(w, f2(-dd.x, -dd.y));
+          u = ex > 0 ? add2rn(u, dd) : sub2rn(u, dd);
+          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : sub2rn(v, dd);
+          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : sub2rn(w, dd);
         }
       });
     }
@@ -681,12 +744,19 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   const float om = static_cast<float>(a.omega);
   const float om_u = om * a.enc.unit;
   const float2 keep = f2s(1.0f - om);
-  const float2 udu15 = mul2rn(f2s(1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
+  // -1.5 u.u, rounded as 1.5 u.u then negated
+  const float2 mudu15 = mul2rn(f2s(-1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
   // omega unit (3 p~ - 1.5 u.u)
-  const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), f2(-udu15.x, -udu15.y)));
-  // cavity: the pair holds a cell at an x wall (padding stores below)
-  [[maybe_unused]] const bool xwall_lo = RULE == CaseRule::CavityStd && x0 == 0;
-  [[maybe_unused]] const bool xwall_hi = RULE == CaseRule::CavityStd && x0 + 2 >= a.nx;
+  const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), mudu15));
+  // wall record: the pair holds the x = 0 cell (lo) or the x = nx - 1 cell
+  // (hi; nx >= 4, so not both).  Each 16-bit value sits in the pair's packed
+  // store word of its population (low half: cell x0, high half: x0 + 1);
+  // rsel picks those halves of two words into one record word.
+  [[maybe_unused]] const bool rec_lo = REC && x0 == 0, rec_hi = REC && x0 + 2 >= a.nx;
+  [[maybe_unused]] const bool rec_any = rec_lo || rec_hi;
+  [[maybe_unused]] const uint32_t rsel = rec_lo ? 0x5410u : 0x7632u;
+  [[maybe_unused]] uint16_t* const rec_side = rec_row + (rec_hi ? WallRecord::HI : 0);
+  [[maybe_unused]] uint32_t held = 0, pend = 0, w01 = 0, w23 = 0;
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     float2 Kq = K;
@@ -698,35 +768,50 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     if constexpr (q == 0) {
       gn = fma2rn(g[q], keep, Kq);
     } else {
-      const float2 e = edu2<q>(u, v, w);
-      const float2 t = fma2rn(e, f2s(4.5f), f2s(3.0f));
-      const float2 h = mul2rn(e, f2s(om_u));
+      // with e negated, so are the factors 4.5 and omega unit: same values.
+      // The sphere's kernels keep the signed e, whose negations cost no
+      // register for -omega unit (their registers are at the limit).
+      constexpr bool en = RULE != CaseRule::SphereStd && edu_neg<q>();
+      const float2 e = RULE != CaseRule::SphereStd ? edu2f<q>(u, v, w) : edu2<q>(u, v, w);
+      const float2 t = fma2rn(e, f2s(en ? -4.5f : 4.5f), f2s(3.0f));
+      const float2 h = mul2rn(e, f2s(en ? -om_u : om_u));
       gn = fma2rn(h, t, fma2rn(g[q], keep, Kq));
     }
     if (live0 && live1) {
-      pl.store_pair(q, b, Pack2<S>::from_f2(gn));
-    } else {
-      if (live0) pl.store_half(q, b, Pack2<S>::from_f(gn.x));
-      if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(gn.y));
-    }
-    if constexpr (RULE == CaseRule::CavityStd) {
-      // x walls: the next step's pull of bb(q) at this cell starts outside
-      // the box and must return this value (halfway bounce-back); it goes to
-      // the padding of the row that pull reads (x = -1 -> element pitch - 1,
-      // x = nx -> element nx), inside the box's y and z range only
-      constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q], qq = D3Q27::bb[q];
-      if constexpr (ex != 0) {
-        if (ex < 0 ? xwall_lo : xwall_hi) {
-          const int jj = j + ey, kk = k + ez;  // the row of bb(q)'s pull source
-          if (jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) {
-            const int32_t row = a.base32 + kk * a.sz32 + jj * a.pitch32;
-            if (ex < 0)
-              pl.store_half(qq, row + a.pitch32 - 1, Pack2<S>::from_f(gn.x));
-            else
-              pl.store_half(qq, row + a.nx, Pack2<S>::from_f(gn.y));
+      const uint32_t word = Pack2<S>::from_f2(gn);
+      pl.store_pair(q, b, word);
+      if constexpr (REC) {
+        // slot m of a side holds the population of pair m that leaves the
+        // box through that wall: e_x = -1 (q = P_m + 1) at x = 0, e_x = +1
+        // (q = P_m) at x = nx - 1
+        constexpr int ex = D3Q27::ex[q];
+        if constexpr (ex > 0) {
+          held = word;
+        } else if constexpr (ex < 0) {
+          constexpr int m = WallRecord::slot(q);
+          const uint32_t wv = rec_lo ? word : held;
+          if constexpr (m % 2 == 0) {
+            pend = wv;
+          } else {
+            const uint32_t pk = __byte_perm(pend, wv, rsel);
+            if constexpr (m == 1) w01 = pk;
+            if constexpr (m == 3) {
+              if (rec_any) *reinterpret_cast<uint2*>(rec_side) = make_uint2(w01, pk);
+            }
+            if constexpr (m == 5) w23 = pk;
+            if constexpr (m == 7) {
+              if (rec_any) *reinterpret_cast<uint2*>(rec_side + 4) = make_uint2(w23, pk);
+            }
+          }
+          if constexpr (m == 8) {
+            // the side's last 16 bytes: slot 8, then zeros
+            if (rec_any) *reinterpret_cast<uint4*>(rec_side + 8) = make_uint4(__byte_perm(wv, 0u, rsel), 0u, 0u, 0u);
           }
         }
       }
+    } else {
+      if (live0) pl.store_half(q, b, Pack2<S>::from_f(gn.x));
+      if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(gn.y));
     }
   });
 }
