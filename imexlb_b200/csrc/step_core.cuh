@@ -445,6 +445,17 @@ __device__ __forceinline__ float2 sub2rn(float2 a, float2 b) {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
 
+// a - b, or with NEGADD as a + (-b), the same value.  The two forms only
+// steer register allocation: the sphere's staged kernels spill 24 bytes
+// with the subtract form and none with the other, the cavity's the reverse.
+template <bool NEGADD>
+__device__ __forceinline__ float2 minus2(float2 a, float2 b) {
+  if constexpr (NEGADD)
+    return add2rn(a, f2(-b.x, -b.y));
+  else
+    return sub2rn(a, b);
+}
+
 // e = c_q . u of a pair without negations.  Round-to-nearest is symmetric
 // in sign, so (-x) + y rounds to y - x and (-x) + (-y) to -(x + y): the
 // value equals the left-to-right sum of the signed components (edu2), or
@@ -678,6 +689,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
                                                 const bool live0, const bool live1, const bool store,
                                                 const uint32_t links0 = 0, const uint32_t links1 = 0,
                                                 uint16_t* rec_row = nullptr) {
+  constexpr bool NEGADD = RULE == CaseRule::SphereStd;  // see minus2
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
   [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
@@ -695,11 +707,11 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     const float2 d = mul2rn(x, f2s(a.enc.inv_scale[q]));
     s = add2rn(s, d);
     if constexpr (ex == 1) u = add2rn(u, d);
-    if constexpr (ex == -1) u = sub2rn(u, d);
+    if constexpr (ex == -1) u = minus2<NEGADD>(u, d);
     if constexpr (ey == 1) v = add2rn(v, d);
-    if constexpr (ey == -1) v = sub2rn(v, d);
+    if constexpr (ey == -1) v = minus2<NEGADD>(v, d);
     if constexpr (ez == 1) w = add2rn(w, d);
-    if constexpr (ez == -1) w = sub2rn(w, d);
+    if constexpr (ez == -1) w = minus2<NEGADD>(w, d);
     g[q] = x;
   });
   if constexpr (RULE == CaseRule::SphereStd) {
@@ -717,9 +729,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
           g[q] = add2rn(g[q], dg);
           const float2 dd = mul2rn(dg, f2s(a.enc.inv_scale[q]));
           s = add2rn(s, dd);
-          u = ex > 0 ? add2rn(u, dd) : sub2rn(u, dd);
-          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : sub2rn(v, dd);
-          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : sub2rn(w, dd);
+          u = ex > 0 ? add2rn(u, dd) : minus2<NEGADD>(u, dd);
+          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : minus2<NEGADD>(v, dd);
+          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : minus2<NEGADD>(w, dd);
         }
       });
     }
@@ -745,7 +757,14 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   const float om_u = om * a.enc.unit;
   const float2 keep = f2s(1.0f - om);
   // -1.5 u.u, rounded as 1.5 u.u then negated
-  const float2 mudu15 = mul2rn(f2s(-1.5f), fma2rn(w, w, fma2rn(v, v, mul2rn(u, u))));
+  const float2 uu = fma2rn(w, w, fma2rn(v, v, mul2rn(u, u)));
+  float2 mudu15;
+  if constexpr (NEGADD) {
+    const float2 t15 = mul2rn(f2s(1.5f), uu);
+    mudu15 = f2(-t15.x, -t15.y);
+  } else {
+    mudu15 = mul2rn(f2s(-1.5f), uu);
+  }
   // omega unit (3 p~ - 1.5 u.u)
   const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), mudu15));
   // wall record: the pair holds the x = 0 cell (lo) or the x = nx - 1 cell
