@@ -11,8 +11,10 @@
 
 #if defined(__CUDACC__)
 #define IMX_HD __host__ __device__ __forceinline__
+#define IMX_HDC __host__ __device__ constexpr
 #else
 #define IMX_HD inline
+#define IMX_HDC constexpr
 #endif
 
 namespace imx {
@@ -31,7 +33,7 @@ struct D3Q27 {
 
 // The weights as the reference computes them: 8.0/27.0, 2.0/27.0, 1.0/54.0,
 // 1.0/216.0 (each a correctly rounded double quotient).
-IMX_HD double weight_of_class(int c) {
+IMX_HDC double weight_of_class(int c) {
   return c == 0 ? 8.0 / 27.0 : (c == 1 ? 2.0 / 27.0 : (c == 2 ? 1.0 / 54.0 : 1.0 / 216.0));
 }
 

@@ -807,12 +807,11 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   const double p_rest = d->kase == IMEXLB_TGV ? d->rho0 / 3.0 : 0.0;
   a.p_shift = e->storage == IMEXLB_F64 ? 0.0 : p_rest;
   for (int q = 0; q < Q; ++q) {
-    const double t = weight_of_class(D3Q27::wclass[q]);
-    const double sc = e->storage == IMEXLB_F16 ? 16384.0 / t : (e->storage == IMEXLB_BF16 ? 1.0 / t : 1.0);
+    const double sc = store_scale(static_cast<Store>(e->storage), D3Q27::wclass[q]);
     a.enc.scale[q] = static_cast<float>(sc);
     a.enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
-  a.enc.unit = e->storage == IMEXLB_F16 ? 16384.f : 1.f;
+  a.enc.unit = store_unit(static_cast<Store>(e->storage));
   in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {

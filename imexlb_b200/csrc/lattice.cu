@@ -408,12 +408,11 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   const double p_rest = P.kase == IMEXLB_TGV ? P.rho0 / 3.0 : 0.0;
   h->p_shift = is_float_store(P.storage) ? p_rest : 0.0;
   for (int q = 0; q < Q; ++q) {
-    const double t = weight_of_class(D3Q27::wclass[q]);
-    const double sc = P.storage == IMEXLB_F16 ? 16384.0 / t : (P.storage == IMEXLB_BF16 ? 1.0 / t : 1.0);
+    const double sc = store_scale(static_cast<Store>(P.storage), D3Q27::wclass[q]);
     h->enc.scale[q] = static_cast<float>(sc);
     h->enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
-  h->enc.unit = P.storage == IMEXLB_F16 ? 16384.f : 1.f;
+  h->enc.unit = store_unit(static_cast<Store>(P.storage));
 
   const size_t padded = static_cast<size_t>(L.ex) * L.ey * L.ez;
   if (P.kase == IMEXLB_SPHERE) {

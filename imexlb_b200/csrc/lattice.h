@@ -16,6 +16,15 @@ namespace imx {
 
 enum class Bc : int { Periodic = 0, Ghost = 1, Standard = 2 };
 enum class Store : int { F64 = 0, F32 = 1, F16 = 2, BF16 = 3 };
+// Scale of a stored population of weight class `cls` (Encoding::scale):
+// the FP16 format stores deviations times 2^14 / w_q, the BF16 format times
+// 1 / w_q, FP32 and FP64 unscaled; the unit of the 2-byte collision is 2^14
+// for FP16, else 1.  Compile-time values, so that the 2-byte step kernels
+// take them as constants rather than loads.
+IMX_HDC double store_scale(Store s, int cls) {
+  return s == Store::F16 ? 16384.0 / weight_of_class(cls) : (s == Store::BF16 ? 1.0 / weight_of_class(cls) : 1.0);
+}
+IMX_HDC float store_unit(Store s) { return s == Store::F16 ? 16384.f : 1.f; }
 // Which per-cell rules the step applies after the moments.
 enum class CaseRule : int {
   None = 0,         // TGV

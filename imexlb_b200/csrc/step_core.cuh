@@ -692,7 +692,10 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   constexpr bool NEGADD = RULE == CaseRule::SphereStd;  // see minus2
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
-  [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * a.enc.unit;
+  // the format's scales are compile-time values (store_scale; Encoding holds
+  // the same numbers for the host and the other kernels)
+  constexpr float UNIT = store_unit(S);
+  [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * UNIT;
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
@@ -704,7 +707,8 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
       if (left_edge) x.x = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
     }
-    const float2 d = mul2rn(x, f2s(a.enc.inv_scale[q]));
+    constexpr float isc = static_cast<float>(1.0 / store_scale(S, D3Q27::wclass[q]));
+    const float2 d = mul2rn(x, f2s(isc));
     s = add2rn(s, d);
     if constexpr (ex == 1) u = add2rn(u, d);
     if constexpr (ex == -1) u = minus2<NEGADD>(u, d);
@@ -724,10 +728,11 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
         constexpr int q = decltype(qc)::value;
         constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
         if constexpr (ex != 0) {
-          const float c = -6.f * static_cast<float>(ex) * a.enc.u_ref[0] * a.enc.unit;
+          const float c = -6.f * static_cast<float>(ex) * a.enc.u_ref[0] * UNIT;
           const float2 dg = f2(((links0 >> q) & 1u) ? c : 0.f, ((links1 >> q) & 1u) ? c : 0.f);
           g[q] = add2rn(g[q], dg);
-          const float2 dd = mul2rn(dg, f2s(a.enc.inv_scale[q]));
+          constexpr float isc = static_cast<float>(1.0 / store_scale(S, D3Q27::wclass[q]));
+          const float2 dd = mul2rn(dg, f2s(isc));
           s = add2rn(s, dd);
           u = ex > 0 ? add2rn(u, dd) : minus2<NEGADD>(u, dd);
           if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : minus2<NEGADD>(v, dd);
@@ -754,7 +759,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     a.mp[c0 + 1] = live1 ? static_cast<double>(p.y) + a.p_shift : a.p_shift;
   }
   const float om = static_cast<float>(a.omega);
-  const float om_u = om * a.enc.unit;
+  const float om_u = om * UNIT;
   const float2 keep = f2s(1.0f - om);
   // -1.5 u.u, rounded as 1.5 u.u then negated
   const float2 uu = fma2rn(w, w, fma2rn(v, v, mul2rn(u, u)));
