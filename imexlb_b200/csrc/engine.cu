@@ -67,6 +67,19 @@ struct EngArgs {
   int* err;  // set non-zero by a staged kernel that gave up waiting
 };
 
+// What the consumer warps of a staged engine kernel need of a tile beyond
+// its rows and its instance's StepArgs prefix: written to shared memory by
+// warp 0 with the tile's copies (the stage's full mbarrier publishes it),
+// so that no consumer waits on global loads of the tile list or instance.
+struct __align__(16) TileHdr {
+  const void* src;   // distribution buffer read
+  void* dst;         // distribution buffer written
+  uint16_t* rec;     // wall records written (staged cavity), else null
+  stage::Geo geo;
+  int j0, k;
+};
+constexpr size_t TILE_HDR_BYTES = (sizeof(TileHdr) + 15) & ~static_cast<size_t>(15);
+
 // Population planes of one instance: plane q starts q * sq elements into the
 // buffer (27 sq < 2^31 for every engine instance).
 template <class T>
@@ -148,7 +161,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   T* stages = reinterpret_cast<T*>(smem);
   unsigned char* args = smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T);
   unsigned char* recs = args + NS * STAGED_ARGS_BYTES;
-  uint64_t* full = reinterpret_cast<uint64_t*>(recs + (REC ? NS * REC_STAGE_BYTES : 0));
+  TileHdr* hdr = reinterpret_cast<TileHdr*>(recs + (REC ? NS * REC_STAGE_BYTES : 0));
+  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(hdr) + NS * TILE_HDR_BYTES);
   uint64_t* empty = full + NS;
   auto rec_stage = [&](int sn) { return reinterpret_cast<uint16_t*>(recs + sn * REC_STAGE_BYTES); };
   __shared__ int abort_flag;
@@ -170,6 +184,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
     const Tile tile = ea.tiles[t];
     const EngInst* in = ea.inst + tile.slot;
     const int cur = (ea.parity ^ in->parity0) & 1;
+    if (lane == 0) hdr[sn] = TileHdr{in->buf[cur], in->buf[1 - cur], REC ? in->rec[1 - cur] : nullptr, in->geo,
+                                     tile.j0, tile.k};
     issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
                         stages + sn * stage_elems, &full[sn], REC ? in->rec[cur] : nullptr, rec_stage(sn),
                         args + sn * STAGED_ARGS_BYTES, &in->a, static_cast<uint32_t>(STAGED_ARGS_BYTES));
@@ -200,15 +216,12 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       *abort_v = 1;
       break;
     }
-    const Tile tile = ea.tiles[t];
-    const EngInst* in = ea.inst + tile.slot;
-    const int cur = (ea.parity ^ in->parity0) & 1;
+    const TileHdr& h = hdr[s];
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
-    const FlatPlanes<T> pl{static_cast<const T*>(in->buf[cur]), static_cast<T*>(in->buf[1 - cur]),
-                           static_cast<int32_t>(a.sq)};
-    const Geo g = in->geo;
-    consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), tile.j0, tile.k,
-                             ea.store != 0, rec_stage(s), REC ? in->rec[1 - cur] : nullptr);
+    const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
+    const Geo g = h.geo;
+    consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k,
+                             ea.store != 0, rec_stage(s), h.rec);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
@@ -222,7 +235,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
 
 inline size_t engine_staged_smem(bool records) {
   return static_cast<size_t>(Q) * stage::SLOT_UNITS * 2 + stage::MAX_STAGES * STAGED_ARGS_BYTES +
-         (records ? stage::MAX_STAGES * stage::REC_STAGE_BYTES : 0) + 16 * stage::MAX_STAGES;
+         (records ? stage::MAX_STAGES * stage::REC_STAGE_BYTES : 0) + stage::MAX_STAGES * TILE_HDR_BYTES +
+         16 * stage::MAX_STAGES;
 }
 
 // Residual partial sums per tile: sum |u - u_prev|^2 and sum |u|^2 over the
