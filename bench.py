@@ -16,7 +16,8 @@ Metric: MLUPS (million lattice-cell updates per second), whole job.
 * e2e       the same solve through the public C ABI from host memory: create
             (host set-up + upload), K steps with the u, v, w, p fields read
             into pinned host buffers every K/10 steps (the reference driver's
-            output cadence, Time/inter = 10), host wall clock.
+            output cadence, Time/inter = 10; imexlb_get_fields_async, each
+            copy overlapping the next steps), destroy, host wall clock.
 * roofline  the fused step kernel: 432 algorithmic bytes per cell update
             (27 FP64 loads + 27 FP64 stores) x cells / mean launch duration
             (per-launch CUDA events on the launching stream), against the
@@ -421,7 +422,10 @@ def main(argv=None) -> int:
     # ---- end to end through the public API, host memory in and out
     outputs = 10
     chunk = max(1, args.steps // outputs)
-    pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
+    # two pinned sets: each output is copied while the next chunk's steps
+    # run (imexlb_get_fields_async), into the set the host is not holding
+    pinned = [{k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
+              for _ in range(2)]
     barrier()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
@@ -432,8 +436,9 @@ def main(argv=None) -> int:
             s = min(chunk, args.steps - done)
             lbm2.step(s)
             done += s
-            lbm2.fields(out=pinned)
+            lbm2.fields(out=pinned[nout % 2], wait=False)
             nout += 1
+        lbm2.synchronize()  # every output is in host memory
         lbm2.close()
     e2e_s = time.perf_counter() - t0
     _, _, e2e, e2e_s = replica_throughput(elapsed_ms, e2e_s, cells, args.steps, dist)

@@ -76,7 +76,7 @@ class EngineStats(ctypes.Structure):
 
 # Every symbol include/imexlb.h declares (tests check the library exports them).
 EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imexlb_initialize", "imexlb_step",
-           "imexlb_get_fields", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
+           "imexlb_get_fields", "imexlb_get_fields_async", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
            "imexlb_reduce_fields_noalloc", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
            "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
@@ -104,6 +104,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_initialize.argtypes = [vp]
     lib.imexlb_step.argtypes = [vp, i]
     lib.imexlb_get_fields.argtypes = [vp, vp, vp, vp, vp]
+    lib.imexlb_get_fields_async.argtypes = [vp, vp, vp, vp, vp]
     lib.imexlb_get_mask.argtypes = [vp, vp]
     lib.imexlb_write_tecplot.argtypes = [vp, ctypes.c_char_p, i]
     lib.imexlb_reduce.argtypes = [vp, i, ctypes.POINTER(d)]
@@ -224,12 +225,16 @@ class LBM:
     def synchronize(self):
         _check(self.lib.imexlb_synchronize(self.h))
 
-    def fields(self, out: dict | None = None) -> dict:
-        """ua, va, wa, p after the last step, each shaped (nz, ny, nx)."""
+    def fields(self, out: dict | None = None, wait: bool = True) -> dict:
+        """ua, va, wa, p after the last step, each shaped (nz, ny, nx).  With
+        wait=False the copy is only enqueued (imexlb_get_fields_async): `out`
+        (pinned memory overlaps the copy with later steps) holds the fields
+        after the next synchronize() or synchronous call."""
         nx, ny, nz = self.n
         if out is None:
             out = {k: np.empty((nz, ny, nx)) for k in ("u", "v", "w", "p")}
-        _check(self.lib.imexlb_get_fields(self.h, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]), _ptr(out["p"])))
+        fn = self.lib.imexlb_get_fields if wait else self.lib.imexlb_get_fields_async
+        _check(fn(self.h, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]), _ptr(out["p"])))
         return out
 
     def mask(self) -> np.ndarray:

@@ -178,7 +178,18 @@ struct imexlb_lattice {
   };
   std::vector<Timed> timed;
   std::vector<cudaEvent_t> event_pool;
+  // asynchronous field reads (imexlb_get_fields_async): copies on their own
+  // stream after `mom_ready`; the next moment-writing step waits `copy_done`
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t mom_ready = nullptr, copy_done = nullptr;
+  bool copy_pending = false;
   ~imexlb_lattice() {
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+    }
+    if (mom_ready) cudaEventDestroy(mom_ready);
+    if (copy_done) cudaEventDestroy(copy_done);
     std::vector<cudaEvent_t> all(event_pool);
     for (auto& t : timed) {
       if (std::find(all.begin(), all.end(), t.a) == all.end()) all.push_back(t.a);
@@ -278,30 +289,38 @@ int upload_case(imexlb_lattice* h) {
   std::vector<double> U, V, W, Pf;
   init_fields(h, U, V, W, Pf);
   const size_t n = U.size();
+  // Without ghosts the stored box is the interior: the fields go straight to
+  // the moment views, which init_f reads.  With ghosts they go to a scratch
+  // copy of the padded box and the interior is gathered on the host.
+  const bool interior = L.g == 0;
   DevArray<double> tmp;
-  IMX_CUDA(tmp.alloc(4 * n));
-  IMX_CUDA(cudaMemcpyAsync(tmp.p, U.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(tmp.p + n, V.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(tmp.p + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(tmp.p + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  if (!interior) IMX_CUDA(tmp.alloc(4 * n));
+  double* src = interior ? h->mom.p : tmp.p;
+  IMX_CUDA(cudaMemcpyAsync(src, U.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(src + n, V.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(src + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(src + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
   IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
   IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
-  IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, tmp.p, tmp.p + n, tmp.p + 2 * n, tmp.p + 3 * n,
-                         h->p_shift, h->enc, h->stream));
+  IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, src, src + n, src + 2 * n, src + 3 * n, h->p_shift,
+                         h->enc, h->stream));
   for (int b = 0; b < 2 && h->rec[b].p; ++b) IMX_CUDA(launch_cavity_records(L, h->buf[b].p, h->rec[b].p, h->stream));
-  // the views after Initialize: interior moments
-  std::vector<double> mom(4 * static_cast<size_t>(h->ncell));
-  for (int k = 0; k < L.nz; ++k)
-    for (int j = 0; j < L.ny; ++j)
-      for (int i = 0; i < L.nx; ++i) {
-        const size_t d = i + static_cast<size_t>(L.nx) * (j + static_cast<size_t>(L.ny) * k);
-        const size_t c = (i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g));
-        mom[d] = U[c];
-        mom[h->ncell + d] = V[c];
-        mom[2 * h->ncell + d] = W[c];
-        mom[3 * h->ncell + d] = Pf[c];
-      }
-  IMX_CUDA(cudaMemcpyAsync(h->mom.p, mom.data(), mom.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  if (!interior) {
+    // the views after Initialize: interior moments
+    std::vector<double> mom(4 * static_cast<size_t>(h->ncell));
+    for (int k = 0; k < L.nz; ++k)
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i) {
+          const size_t d = i + static_cast<size_t>(L.nx) * (j + static_cast<size_t>(L.ny) * k);
+          const size_t c = (i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g));
+          mom[d] = U[c];
+          mom[h->ncell + d] = V[c];
+          mom[2 * h->ncell + d] = W[c];
+          mom[3 * h->ncell + d] = Pf[c];
+        }
+    IMX_CUDA(cudaMemcpyAsync(h->mom.p, mom.data(), mom.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    IMX_CUDA(cudaStreamSynchronize(h->stream));  // before the host vector goes
+  }
   // reference boundaries: the first step's passes act on the initial state
   if (h->gn)
     IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[0].p, h->buf[1].p, h->gtgt.p, h->gsrc.p, h->gn, L.sq, h->enc,
@@ -552,8 +571,12 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   return IMEXLB_OK;
 }
 
+static int sync_checked(imexlb_lattice* h);
+
 int imexlb_initialize(imexlb_lattice* h) {
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (h->copy_pending)
+    if (const int rc = sync_checked(h)) return rc;  // a field read still copies the moments
   return upload_case(h);
 }
 
@@ -571,6 +594,9 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
       a.dstq[q] = h->buf[1 - h->cur].p + static_cast<size_t>(q) * h->L.sq * h->L.elem;
     }
     a.store = s == nsteps - 1;
+    // the moments an asynchronous read is still copying are overwritten by
+    // this call's last step only
+    if (a.store && h->copy_pending) IMX_CUDA(cudaStreamWaitEvent(h->stream, h->copy_done, 0));
     const bool drag = a.store && h->drag_part.p;
     const bool drag_own = drag && drag_in_own_kernel(h->cfg.store);
     a.drag_part = (drag && !drag_own) ? h->drag_part.p : nullptr;
@@ -611,6 +637,10 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
 // Wait for the lattice's stream and report a step kernel that gave up
 // waiting for its staged copies (its error word is then cleared).
 static int sync_checked(imexlb_lattice* h) {
+  if (h->copy_pending) {
+    IMX_CUDA(cudaStreamSynchronize(h->copy_stream));
+    h->copy_pending = false;
+  }
   int word = 0;
   IMX_CUDA(cudaMemcpyAsync(&word, h->err.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   IMX_CUDA(cudaStreamSynchronize(h->stream));
@@ -629,6 +659,25 @@ int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double
       IMX_CUDA(cudaMemcpyAsync(dst[c], h->mom.p + c * h->ncell, h->ncell * sizeof(double), cudaMemcpyDeviceToHost,
                                h->stream));
   return sync_checked(h);
+}
+
+int imexlb_get_fields_async(imexlb_lattice* h, double* u, double* v, double* w, double* p) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (!h->copy_stream) {
+    IMX_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    IMX_CUDA(cudaEventCreateWithFlags(&h->mom_ready, cudaEventDisableTiming));
+    IMX_CUDA(cudaEventCreateWithFlags(&h->copy_done, cudaEventDisableTiming));
+  }
+  IMX_CUDA(cudaEventRecord(h->mom_ready, h->stream));
+  IMX_CUDA(cudaStreamWaitEvent(h->copy_stream, h->mom_ready, 0));
+  double* dst[4] = {u, v, w, p};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c])
+      IMX_CUDA(cudaMemcpyAsync(dst[c], h->mom.p + c * h->ncell, h->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->copy_stream));
+  IMX_CUDA(cudaEventRecord(h->copy_done, h->copy_stream));
+  h->copy_pending = true;
+  return IMEXLB_OK;
 }
 
 int imexlb_get_mask(imexlb_lattice* h, int32_t* usr) {

@@ -707,15 +707,12 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
       if (left_edge) x.x = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
     }
+    // d_q = g_q w_q / unit enters each moment as one fused multiply-add
     constexpr float isc = static_cast<float>(1.0 / store_scale(S, D3Q27::wclass[q]));
-    const float2 d = mul2rn(x, f2s(isc));
-    s = add2rn(s, d);
-    if constexpr (ex == 1) u = add2rn(u, d);
-    if constexpr (ex == -1) u = minus2<NEGADD>(u, d);
-    if constexpr (ey == 1) v = add2rn(v, d);
-    if constexpr (ey == -1) v = minus2<NEGADD>(v, d);
-    if constexpr (ez == 1) w = add2rn(w, d);
-    if constexpr (ez == -1) w = minus2<NEGADD>(w, d);
+    s = fma2rn(x, f2s(isc), s);
+    if constexpr (ex != 0) u = fma2rn(x, f2s(ex > 0 ? isc : -isc), u);
+    if constexpr (ey != 0) v = fma2rn(x, f2s(ey > 0 ? isc : -isc), v);
+    if constexpr (ez != 0) w = fma2rn(x, f2s(ez > 0 ? isc : -isc), w);
     g[q] = x;
   });
   if constexpr (RULE == CaseRule::SphereStd) {

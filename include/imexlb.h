@@ -125,6 +125,14 @@ int imexlb_step(imexlb_lattice* h, int nsteps);
  * pointer may be NULL).  Synchronises the lattice's stream. */
 int imexlb_get_fields(imexlb_lattice* h, double* u, double* v, double* w, double* p);
 
+/* The same views, asynchronously: enqueues their copy into the host
+ * buffers (pinned memory lets it overlap the following steps) and returns.
+ * The buffers hold the fields, and must stay allocated, until the next
+ * synchronising call (imexlb_synchronize, imexlb_get_fields, ...).  The
+ * next imexlb_step call's last step, which rewrites the views, waits for
+ * the copy; the steps before it run meanwhile. */
+int imexlb_get_fields_async(imexlb_lattice* h, double* u, double* v, double* w, double* p);
+
 /* The usr view (sphere solid mask, 1 = fluid; interior, x fastest). */
 int imexlb_get_mask(imexlb_lattice* h, int32_t* usr);
 
