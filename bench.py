@@ -94,7 +94,7 @@ DEFAULT_WORKLOAD = "cavity128-f64"
 
 # DRAM bytes (read + write) of one step launch from one ncu capture of the
 # workload (the summaries in profiles/ give the commands)
-TRAFFIC = {"cavity128-f64": 857.3e6, "cavity128-f16": 214.0e6}
+TRAFFIC = {"cavity128-f64": 857.3e6, "cavity128-f16": 178.5e6}
 
 
 def tau_of(w) -> float:
