@@ -445,17 +445,6 @@ __device__ __forceinline__ float2 sub2rn(float2 a, float2 b) {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
 
-// a - b, or with NEGADD as a + (-b), the same value.  The two forms only
-// steer register allocation: the sphere's staged kernels spill 24 bytes
-// with the subtract form and none with the other, the cavity's the reverse.
-template <bool NEGADD>
-__device__ __forceinline__ float2 minus2(float2 a, float2 b) {
-  if constexpr (NEGADD)
-    return add2rn(a, f2(-b.x, -b.y));
-  else
-    return sub2rn(a, b);
-}
-
 // e = c_q . u of a pair without negations.  Round-to-nearest is symmetric
 // in sign, so (-x) + y rounds to y - x and (-x) + (-y) to -(x + y): the
 // value equals the left-to-right sum of the signed components (edu2), or
@@ -689,7 +678,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
                                                 const bool live0, const bool live1, const bool store,
                                                 const uint32_t links0 = 0, const uint32_t links1 = 0,
                                                 uint16_t* rec_row = nullptr) {
-  constexpr bool NEGADD = RULE == CaseRule::SphereStd;  // see minus2
+  // -1.5 u.u below is formed two ways of the same value: the sphere's
+  // staged kernels spill 24 bytes with one and none with the other
+  constexpr bool NEGADD = RULE == CaseRule::SphereStd;
   float2 g[Q];
   float2 s = f2s(0.f), u = f2s(0.f), v = f2s(0.f), w = f2s(0.f);
   // the format's scales are compile-time values (store_scale; Encoding holds
@@ -731,9 +722,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
           constexpr float isc = static_cast<float>(1.0 / store_scale(S, D3Q27::wclass[q]));
           const float2 dd = mul2rn(dg, f2s(isc));
           s = add2rn(s, dd);
-          u = ex > 0 ? add2rn(u, dd) : minus2<NEGADD>(u, dd);
-          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : minus2<NEGADD>(v, dd);
-          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : minus2<NEGADD>(w, dd);
+          u = ex > 0 ? add2rn(u, dd) : add2rn(u, f2(-dd.x, -dd.y));
+          if constexpr (ey != 0) v = ey > 0 ? add2rn(v, dd) : add2rn(v, f2(-dd.x, -dd.y));
+          if constexpr (ez != 0) w = ez > 0 ? add2rn(w, dd) : add2rn(w, f2(-dd.x, -dd.y));
         }
       });
     }
