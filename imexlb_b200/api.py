@@ -81,7 +81,7 @@ EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imex
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
            "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
            "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_remove",
-           "imexlb_engine_step", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
+           "imexlb_engine_step", "imexlb_engine_limit", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
            "imexlb_engine_instance_bytes", "imexlb_engine_checkpoint_size", "imexlb_engine_checkpoint_save",
            "imexlb_engine_restore", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
 
@@ -130,6 +130,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_engine_add.argtypes = [vp, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_int)]
     lib.imexlb_engine_remove.argtypes = [vp, i]
     lib.imexlb_engine_step.argtypes = [vp, i]
+    lib.imexlb_engine_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.imexlb_engine_fields.argtypes = [vp, i, vp, vp, vp, vp]
     lib.imexlb_engine_residuals.argtypes = [vp, vp, i]
     lib.imexlb_engine_info.argtypes = [vp, ctypes.POINTER(EngineStats)]
@@ -372,6 +373,12 @@ class Engine:
 
     def step(self, n: int = 1):
         _check(self.lib.imexlb_engine_step(self.h, n))
+
+    def limit(self, slot: int, steps: int | None):
+        """The instance takes at most `steps` more steps (None: no limit), then
+        stays as it is while the others go on; its fields are written at its
+        last step (imexlb_engine_limit)."""
+        _check(self.lib.imexlb_engine_limit(self.h, slot, -1 if steps is None else int(steps)))
 
     def synchronize(self):
         _check(self.lib.imexlb_engine_synchronize(self.h))

@@ -72,6 +72,7 @@ struct __align__(128) StagedTile {
   int parity0;
   int j0, k;
   stage::Geo geo;
+  int slot;
 };
 static_assert(sizeof(StagedTile) == 128, "one 4-byte word per lane");
 
@@ -86,6 +87,7 @@ struct EngArgs {
   const EngInst* inst;
   const Tile* tiles;
   const StagedTile* stiles;  // staged groups: per-tile descriptors (index as tiles)
+  const int* left;           // per slot: steps the instance still takes (ENG_NO_LIMIT: no limit)
   int ntiles;
   int parity;
   int store;
@@ -102,8 +104,24 @@ struct __align__(16) TileHdr {
   uint16_t* rec;     // wall records written (staged cavity), else null
   stage::Geo geo;
   int j0, k;
+  int skip;          // the instance has taken its steps: no copies, no update
+  int store;         // write the moments (the call's last step or the instance's)
 };
 constexpr size_t TILE_HDR_BYTES = (sizeof(TileHdr) + 15) & ~static_cast<size_t>(15);
+
+// Steps left of an instance without a step limit (imexlb_engine_limit).
+constexpr int ENG_NO_LIMIT = 0x7fffffff;
+
+// Before each step a tile reads its instance's steps left: 0 skips the tile,
+// 1 (the instance's last step) also writes the moments.  engine_tick counts
+// them down after the step.
+__global__ void engine_tick(int* left, int n) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    const int l = left[s];
+    if (l > 0 && l != ENG_NO_LIMIT) left[s] = l - 1;
+  }
+}
 
 // Population planes of one instance: plane q starts q * sq elements into the
 // buffer (27 sq < 2^31 for every engine instance).
@@ -143,13 +161,15 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
   int loaded = -1;  // same tile sequence in every thread: a block-uniform value
   for (int t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
     const Tile tile = ea.tiles[t];
+    const int left = ea.left[tile.slot];  // block-uniform
+    if (left == 0) continue;              // the instance has taken its steps
     if (tile.slot != loaded) {
       __syncthreads();
       const int4* from = reinterpret_cast<const int4*>(ea.inst + tile.slot);
       int4* to = reinterpret_cast<int4*>(&sh);
       for (int w = threadIdx.x; w < static_cast<int>(sizeof(EngInst) / 16); w += blockDim.x) to[w] = from[w];
       __syncthreads();
-      if (threadIdx.x == 0) sh.a.store = ea.store;
+      if (threadIdx.x == 0) sh.a.store = ea.store || left == 1;
       __syncthreads();
       loaded = tile.slot;
     }
@@ -227,23 +247,32 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       const StagedTile& d = dslot[issued & 1];
       const int cur = (ea.parity ^ d.parity0) & 1;
       const void* src_buf = d.buf[cur];
+      const int left = ea.left[d.slot];
       if (lane == 0)
         hdr[sn] = TileHdr{src_buf, const_cast<void*>(d.buf[1 - cur]), REC ? d.rec[1 - cur] : nullptr, d.geo, d.j0,
-                          d.k};
-      issue_tile<T, WRAP>(d, d.geo, static_cast<const T*>(src_buf), d.j0, d.k, stages + sn * stage_elems, &full[sn],
-                          REC ? d.rec[cur] : nullptr, rec_stage(sn), args + sn * STAGED_ARGS_BYTES, d.args,
-                          static_cast<uint32_t>(STAGED_ARGS_BYTES));
+                          d.k, left == 0, ea.store || left == 1};
+      if (left == 0)
+        issue_skip(&full[sn]);
+      else
+        issue_tile<T, WRAP>(d, d.geo, static_cast<const T*>(src_buf), d.j0, d.k, stages + sn * stage_elems,
+                            &full[sn], REC ? d.rec[cur] : nullptr, rec_stage(sn), args + sn * STAGED_ARGS_BYTES,
+                            d.args, static_cast<uint32_t>(STAGED_ARGS_BYTES));
       __syncwarp();  // every lane has read the slot before the fetch after next refills it
       fetch(tf, issued + 1);
     } else {
       const Tile tile = ea.tiles[tf - grid];
       const EngInst* in = ea.inst + tile.slot;
       const int cur = (ea.parity ^ in->parity0) & 1;
+      const int left = ea.left[tile.slot];
       if (lane == 0)
-        hdr[sn] = TileHdr{in->buf[cur], in->buf[1 - cur], REC ? in->rec[1 - cur] : nullptr, in->geo, tile.j0, tile.k};
-      issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
-                          stages + sn * stage_elems, &full[sn], REC ? in->rec[cur] : nullptr, rec_stage(sn),
-                          args + sn * STAGED_ARGS_BYTES, &in->a, static_cast<uint32_t>(STAGED_ARGS_BYTES));
+        hdr[sn] = TileHdr{in->buf[cur], in->buf[1 - cur], REC ? in->rec[1 - cur] : nullptr, in->geo, tile.j0, tile.k,
+                          left == 0, ea.store || left == 1};
+      if (left == 0)
+        issue_skip(&full[sn]);
+      else
+        issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
+                            stages + sn * stage_elems, &full[sn], REC ? in->rec[cur] : nullptr, rec_stage(sn),
+                            args + sn * STAGED_ARGS_BYTES, &in->a, static_cast<uint32_t>(STAGED_ARGS_BYTES));
     }
   };
   if (PREFETCH && warp == 0) fetch(t0 + blockIdx.x, 0);
@@ -273,11 +302,13 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       break;
     }
     const TileHdr& h = hdr[s];
-    const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
-    const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
-    const Geo g = h.geo;
-    consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k,
-                             ea.store != 0, rec_stage(s), h.rec);
+    if (!h.skip) {
+      const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
+      const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
+      const Geo g = h.geo;
+      consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k,
+                               h.store != 0, rec_stage(s), h.rec);
+    }
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
@@ -437,6 +468,7 @@ struct Slot {
   size_t off = 0, bytes = 0;
   int64_t ncell = 0;
   int64_t steps = 0;
+  int64_t run = 0;  // steps taken since admission (its buffer parity)
   bool have_prev = false;
   int bx_log2 = 5;
   int seg = -1;  // index into the segment table of the current work list
@@ -520,6 +552,8 @@ struct imexlb_engine {
   std::vector<Tile> h_tiles;
   DevBuf<StagedTile> d_stiles;
   std::vector<StagedTile> h_stiles;
+  DevBuf<int> d_left;       // per slot: steps left (ENG_NO_LIMIT: no limit)
+  std::vector<int> h_left;  // host copy, counted down with the steps run
   DevBuf<double> d_part;
   DevBuf<int> d_seg;  // begin[nseg], end[nseg]
   DevBuf<double> d_res;
@@ -628,6 +662,7 @@ int rebuild_tiles(imexlb_engine* e) {
     d.j0 = tl.j0;
     d.k = tl.k;
     d.geo = in.geo;
+    d.slot = tl.slot;
   }
   if (nt) {
     IMX_ECUDA(e->d_tiles.reserve(nt));
@@ -709,16 +744,22 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
 }
 
 cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
-  EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, static_cast<int>(e->h_tiles.size()), parity, store,
-              e->d_err.p};
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, e->d_left.p, static_cast<int>(e->h_tiles.size()), parity,
+              store, e->d_err.p};
   if (ea.ntiles == 0) return cudaSuccess;
+  cudaError_t err = cudaErrorInvalidValue;
   switch (e->storage) {
-    case IMEXLB_F64: return e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
-    case IMEXLB_F32: return launch_groups<Store::F32, false>(e, ea);
-    case IMEXLB_F16: return launch_groups<Store::F16, false>(e, ea);
-    case IMEXLB_BF16: return launch_groups<Store::BF16, false>(e, ea);
+    case IMEXLB_F64:
+      err = e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
+      break;
+    case IMEXLB_F32: err = launch_groups<Store::F32, false>(e, ea); break;
+    case IMEXLB_F16: err = launch_groups<Store::F16, false>(e, ea); break;
+    case IMEXLB_BF16: err = launch_groups<Store::BF16, false>(e, ea); break;
   }
-  return cudaErrorInvalidValue;
+  if (err != cudaSuccess) return err;
+  const int n = static_cast<int>(e->h_left.size());
+  engine_tick<<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_left.p, n);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -749,6 +790,9 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
   e->slots.resize(max_instances);
   e->h_inst.resize(max_instances);
   IMX_ECUDA(e->d_inst.reserve(max_instances));
+  e->h_left.assign(max_instances, ENG_NO_LIMIT);
+  IMX_ECUDA(e->d_left.reserve(max_instances));
+  IMX_ECUDA(cudaMemcpy(e->d_left.p, e->h_left.data(), max_instances * sizeof(int), cudaMemcpyHostToDevice));
   int dev = 0, sms = 148;
   IMX_ECUDA(cudaGetDevice(&dev));
   IMX_ECUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -970,6 +1014,8 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   IMX_ECUDA(e->staging.release_after(sb, e->stream));
   sl.used = true;
   e->slots[s] = sl;
+  e->h_left[s] = ENG_NO_LIMIT;
+  IMX_ECUDA(cudaMemcpyAsync(e->d_left.p + s, &e->h_left[s], sizeof(int), cudaMemcpyHostToDevice, e->stream));
   e->dirty = true;
   *slot_out = s;
   return IMEXLB_OK;
@@ -983,6 +1029,25 @@ int imexlb_engine_remove(imexlb_engine* e, int slot) {
   e->arena.release(sl.off, sl.bytes);
   sl = Slot{};
   e->dirty = true;
+  return IMEXLB_OK;
+}
+
+int imexlb_engine_limit(imexlb_engine* e, int slot, int steps) {
+  if (!e || slot < 0 || slot >= static_cast<int>(e->slots.size()) || !e->slots[slot].used)
+    return efail(IMEXLB_E_ARG, "no such instance");
+  Slot& sl = e->slots[slot];
+  EngInst& in = e->h_inst[slot];
+  // an instance that stopped missed steps: realign its buffer parity with
+  // the engine's (the next step reads the buffer of its run's parity)
+  const int parity0 = static_cast<int>((e->gstep ^ sl.run) & 1);
+  if (parity0 != in.parity0) {
+    IMX_ECUDA(cudaStreamSynchronize(e->stream));  // no queued step reads the old value
+    in.parity0 = parity0;
+    IMX_ECUDA(cudaMemcpy(e->d_inst.p + slot, &in, sizeof(EngInst), cudaMemcpyHostToDevice));
+    e->dirty = true;  // the staged tiles' descriptors carry it too
+  }
+  e->h_left[slot] = steps < 0 ? ENG_NO_LIMIT : steps;
+  IMX_ECUDA(cudaMemcpyAsync(e->d_left.p + slot, &e->h_left[slot], sizeof(int), cudaMemcpyHostToDevice, e->stream));
   return IMEXLB_OK;
 }
 
@@ -1019,8 +1084,15 @@ int imexlb_engine_step(imexlb_engine* e, int nsteps) {
     ++e->gstep;
     --left;
   }
-  for (auto& sl : e->slots)
-    if (sl.used) sl.steps += nsteps;
+  for (size_t s = 0; s < e->slots.size(); ++s) {
+    Slot& sl = e->slots[s];
+    if (!sl.used) continue;
+    int& left = e->h_left[s];
+    const int done = left == ENG_NO_LIMIT ? nsteps : std::min(nsteps, left);
+    if (left != ENG_NO_LIMIT) left -= done;
+    sl.steps += done;
+    sl.run += done;
+  }
   return IMEXLB_OK;
 }
 
@@ -1043,7 +1115,8 @@ int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
   if (rc) return rc;
   for (int s = 0; s < n_out; ++s) out[s] = NAN;
   if (e->h_tiles.empty()) return IMEXLB_OK;
-  EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, static_cast<int>(e->h_tiles.size()), 0, 0, e->d_err.p};
+  EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, e->d_left.p, static_cast<int>(e->h_tiles.size()), 0, 0,
+              e->d_err.p};
   const int grid = std::min(e->grid * 2, ea.ntiles);
   engine_resid_kernel<<<grid, 256, 0, e->stream>>>(ea, e->d_part.p);
   const int ns = static_cast<int>(e->seg_slots.size());
@@ -1126,7 +1199,7 @@ int imexlb_engine_checkpoint_save(imexlb_engine* e, int slot, void* host, size_t
   if (const int rc = sync_checked(e)) return rc;
   const Slot& sl = e->slots[slot];
   const EngInst& in = e->h_inst[slot];
-  const int cur = static_cast<int>((e->gstep & 1) ^ in.parity0) & 1;  // the buffer the next step reads
+  const int cur = static_cast<int>(sl.run & 1);  // the buffer the next step reads
   const CheckpointHeader c = instance_header(e, sl);
   char* p = static_cast<char*>(host);
   std::memcpy(p, &c, sizeof c);

@@ -269,6 +269,13 @@ __device__ __forceinline__ void issue_tile(const A& a, const Geo& g, const T* sr
   if (lane == 31 && xbytes) bulk_g2s(xdst, xsrc, xbytes, bar);
 }
 
+// A stage that receives no copies: completes its full mbarrier at once
+// (called by a whole warp, like issue_tile).
+__device__ __forceinline__ void issue_skip(uint64_t* bar) {
+  if ((threadIdx.x & 31) == 0) bar_arrive(bar);  // the phase's one arrival, no transactions
+  __syncwarp();
+}
+
 // The x-pair (x, x + 1) in tile row r of tile (j0, k), read from the staged
 // rows.  `st` is the stage as 4-byte words.  Reads only the fields of `a`
 // before StepArgs::src.  EDGE = false promises that no boundary rule of the

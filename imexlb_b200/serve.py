@@ -11,9 +11,11 @@ falls below a tolerance.  The loop does continuous batching:
   of one engine while they fit its HBM budget (cells x bytes per cell, the
   engine's arena refuses what does not fit) and the active cells stay under
   a cap that already fills the GPU; the lattices stay resident in HBM;
-* stepping: all admitted instances advance together, `chunk` steps per call
-  (fewer when an instance is closer to its step count), as persistent
-  launches replayed from CUDA graphs;
+* stepping: all admitted instances advance together, `chunk` steps per call,
+  as persistent launches replayed from CUDA graphs; each instance carries
+  its request's step count as an engine step limit (imexlb_engine_limit),
+  so it stops at exactly that step, with its fields written there, while
+  the others go on;
 * retirement: after each call the residuals are read; an instance that
   reached its step count or the tolerance is retired, its u, v, w, p are
   read back to the host (the request's answer) and its memory is freed for
@@ -132,6 +134,7 @@ class Server:
         slot = self.eng.try_add(req.desc(self._tile(req)))
         if slot is None:
             return False
+        self.eng.limit(slot, req.max_steps)
         self.active[slot] = (req, 0)
         return True
 
@@ -140,7 +143,7 @@ class Server:
         once; the steps run while the host admits more requests."""
         if not self.active:
             return 0
-        n = min(self.chunk, min(r.max_steps - done for r, done in self.active.values()))
+        n = min(self.chunk, max(r.max_steps - done for r, done in self.active.values()))
         self.eng.step(n)
         self.steps_run += n
         self._stepped = (n, set(self.active))
@@ -160,7 +163,7 @@ class Server:
             if slot not in stepped:
                 continue
             req, done = self.active[slot]
-            done += n
+            done += min(n, req.max_steps - done)  # the engine stops it at its step count
             self.active[slot] = (req, done)
             r = float(res[slot])
             # retire at the step count, at the tolerance, or when the lattice

@@ -262,6 +262,11 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
 int imexlb_engine_remove(imexlb_engine* e, int slot);
 /* Every active instance advances nsteps steps; the moments of the last are stored. */
 int imexlb_engine_step(imexlb_engine* e, int nsteps);
+/* Step limit of one instance: it takes at most `steps` more steps (< 0: no
+ * limit, the default at admission), then stays as it is while the others go
+ * on; its u, v, w, p views are written at its last step.  A serving loop can
+ * so run fixed-length step calls over requests of any step count. */
+int imexlb_engine_limit(imexlb_engine* e, int slot, int steps);
 /* u, v, w, p of one instance after the last step (host arrays, x fastest). */
 int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, double* w, double* p);
 /* Velocity residual per slot, sqrt(sum|u - u_prev|^2 / sum|u|^2) between this

@@ -141,3 +141,27 @@ def test_first_residual_after_admission_is_infinite(api):
         eng.step(5)
         r = eng.residuals()
         assert 0.0 < r[b] < 1.0
+
+
+@pytest.mark.parametrize("storage,arith", [("f64", "exact"), ("f16", "fast"), ("bf16", "fast")])
+def test_step_limits_stop_instances_at_their_own_count(api, storage, arith):
+    # an instance with a limit stops at exactly that step, with its fields
+    # written there, while the others go on; raising the limit resumes it
+    with api.Engine(storage=storage, arith=arith, budget_bytes=1 << 30, max_instances=8) as eng:
+        slots = [eng.add(api.instance_desc(c, *n, tau, 1.0, u0, **kw)) for c, n, tau, u0, kw in MIX[:3]]
+        eng.limit(slots[0], 7)
+        eng.limit(slots[1], 0)  # stopped before it starts
+        eng.step(12)
+        got = {s: eng.fields(s) for s in slots}
+        eng.limit(slots[0], None)  # resumes at its own buffer parity
+        eng.step(5)
+        resumed = eng.fields(slots[0])
+    expect = {slots[0]: 7, slots[1]: 0, slots[2]: 12}
+    for (c, n, tau, u0, kw), s in zip(MIX[:3], slots):
+        want = alone(api, c, n, tau, u0, kw, expect[s], storage, arith)
+        for k in "uvwp":
+            assert np.array_equal(got[s][k], want[k]), (c, expect[s], k)
+    c, n, tau, u0, kw = MIX[0]
+    want = alone(api, c, n, tau, u0, kw, 12, storage, arith)
+    for k in "uvwp":
+        assert np.array_equal(resumed[k], want[k]), k
