@@ -114,33 +114,97 @@ namespace imx {
 // Standard sphere channel: bit q of a fluid cell's word is set when its pull
 // along -e_q starts in a solid cell (y and z periodic; the x ends belong to
 // the inlet and outlet rules).  lo/hi: bounding box of cells with a set bit.
+// fn(k) for k in [0, nz), planes shared among host threads for large boxes
+// (every plane is computed the same way whichever thread takes it)
+template <class F>
+static void for_planes(int nz, size_t plane_cells, F&& fn) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = static_cast<int>(std::min<size_t>(std::min(hw ? hw : 1u, 32u), nz * plane_cells / (1u << 18) + 1));
+  if (nt <= 1) {
+    for (int k = 0; k < nz; ++k) fn(k);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int k = t; k < nz; k += nt) fn(k);
+    });
+  for (auto& th : pool) th.join();
+}
+
 void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]) {
-  links.assign(static_cast<size_t>(nx) * ny * nz, 0u);
+  const size_t plane = static_cast<size_t>(nx) * ny;
+  links.assign(plane * nz, 0u);
   lo[0] = nx;
   lo[1] = ny;
   lo[2] = nz;
   hi[0] = hi[1] = hi[2] = -1;
-  for (int k = 0; k < nz; ++k)
+  // the solid's box (per plane, then merged: each plane is one thread's)
+  std::vector<int> pb(static_cast<size_t>(nz) * 6);
+  for_planes(nz, plane, [&](int k) {
+    int b[6] = {nx, ny, nz, -1, -1, -1};
     for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
-        const size_t c = i + static_cast<size_t>(nx) * (j + static_cast<size_t>(ny) * k);
-        if (!fluid[c]) continue;
-        uint32_t bits = 0;
-        for (int q = 0; q < Q; ++q) {
-          const int si = i - D3Q27::ex[q];
-          if (si < 0 || si >= nx) continue;
-          const int sj = (j - D3Q27::ey[q] + ny) % ny, sk = (k - D3Q27::ez[q] + nz) % nz;
-          if (!fluid[si + static_cast<size_t>(nx) * (sj + static_cast<size_t>(ny) * sk)]) bits |= 1u << q;
+      for (int i = 0; i < nx; ++i)
+        if (!fluid[i + static_cast<size_t>(nx) * j + plane * k]) {
+          b[0] = std::min(b[0], i);
+          b[1] = std::min(b[1], j);
+          b[2] = std::min(b[2], k);
+          b[3] = std::max(b[3], i);
+          b[4] = std::max(b[4], j);
+          b[5] = std::max(b[5], k);
         }
-        links[c] = bits;
-        if (bits) {
-          const int x[3] = {i, j, k};
-          for (int d = 0; d < 3; ++d) {
-            lo[d] = std::min(lo[d], x[d]);
-            hi[d] = std::max(hi[d], x[d]);
+    std::copy(b, b + 6, pb.begin() + 6 * static_cast<size_t>(k));
+  });
+  int sb[6] = {nx, ny, nz, -1, -1, -1};
+  for (int k = 0; k < nz; ++k)
+    for (int d = 0; d < 3; ++d) {
+      sb[d] = std::min(sb[d], pb[6 * static_cast<size_t>(k) + d]);
+      sb[3 + d] = std::max(sb[3 + d], pb[6 * static_cast<size_t>(k) + 3 + d]);
+    }
+  if (sb[3] < 0) return;  // no solid
+  // Only cells within one cell of the solid can link into it: that box,
+  // or the whole axis where the solid reaches a periodic side (y, z) and
+  // its neighbours wrap around.
+  const int x0 = std::max(0, sb[0] - 1), x1 = std::min(nx - 1, sb[3] + 1);
+  const bool ywrap = sb[1] == 0 || sb[4] == ny - 1, zwrap = sb[2] == 0 || sb[5] == nz - 1;
+  const int y0 = ywrap ? 0 : sb[1] - 1, y1 = ywrap ? ny - 1 : sb[4] + 1;
+  const int z0 = zwrap ? 0 : sb[2] - 1, z1 = zwrap ? nz - 1 : sb[5] + 1;
+  std::vector<int> lb(static_cast<size_t>(nz) * 6);
+  for_planes(nz, plane, [&](int k) {
+    int b[6] = {nx, ny, nz, -1, -1, -1};
+    if (k >= z0 && k <= z1) {
+      const int ks[3] = {(k + 1) % nz, k, (k - 1 + nz) % nz};  // source plane for e_z = -1, 0, +1
+      for (int j = y0; j <= y1; ++j) {
+        const int js[3] = {(j + 1) % ny, j, (j - 1 + ny) % ny};
+        for (int i = x0; i <= x1; ++i) {
+          const size_t c = i + static_cast<size_t>(nx) * j + plane * k;
+          if (!fluid[c]) continue;
+          uint32_t bits = 0;
+          for (int q = 0; q < Q; ++q) {
+            const int si = i - D3Q27::ex[q];
+            if (si < 0 || si >= nx) continue;
+            const int sj = js[D3Q27::ey[q] + 1], sk = ks[D3Q27::ez[q] + 1];
+            if (!fluid[si + static_cast<size_t>(nx) * sj + plane * sk]) bits |= 1u << q;
+          }
+          links[c] = bits;
+          if (bits) {
+            b[0] = std::min(b[0], i);
+            b[1] = std::min(b[1], j);
+            b[2] = std::min(b[2], k);
+            b[3] = std::max(b[3], i);
+            b[4] = std::max(b[4], j);
+            b[5] = std::max(b[5], k);
           }
         }
       }
+    }
+    std::copy(b, b + 6, lb.begin() + 6 * static_cast<size_t>(k));
+  });
+  for (int k = 0; k < nz; ++k)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], lb[6 * static_cast<size_t>(k) + d]);
+      hi[d] = std::max(hi[d], lb[6 * static_cast<size_t>(k) + 3 + d]);
+    }
 }
 }  // namespace imx
 
@@ -223,24 +287,6 @@ void init_fields(imexlb_lattice* h, double* out) {
 }  // namespace
 
 namespace imx {
-// fn(k) for k in [0, nz), planes shared among host threads for large boxes
-// (every plane is computed the same way whichever thread takes it)
-template <class F>
-static void for_planes(int nz, size_t plane_cells, F&& fn) {
-  const unsigned hw = std::thread::hardware_concurrency();
-  const int nt = static_cast<int>(std::min<size_t>(std::min(hw ? hw : 1u, 32u), nz * plane_cells / (1u << 18) + 1));
-  if (nt <= 1) {
-    for (int k = 0; k < nz; ++k) fn(k);
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t)
-    pool.emplace_back([&, t] {
-      for (int k = t; k < nz; k += nt) fn(k);
-    });
-  for (auto& th : pool) th.join();
-}
-
 void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
                  double* out) {
   const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
@@ -1014,6 +1060,22 @@ void imexlb_destroy(imexlb_lattice* h) {
 const char* imexlb_last_error(void) { return g_last_error.c_str(); }
 
 const char* imexlb_version(void) { return "imexlb-b200 0.1 (sm_100a)"; }
+
+// Not part of include/imexlb.h: the standard sphere's solid-link table of a
+// fluid mask (x fastest), for checks on the CPU.  box: lo[3] then hi[3] of the
+// linked cells (hi < 0: none).
+int imexlb_debug_solid_links(int nx, int ny, int nz, const uint8_t* fluid, uint32_t* links, int32_t* box) {
+  if (nx < 1 || ny < 1 || nz < 1 || !fluid || !links || !box) return IMEXLB_E_ARG;
+  std::vector<uint32_t> l;
+  int lo[3], hi[3];
+  imx::solid_links(nx, ny, nz, fluid, l, lo, hi);
+  std::copy(l.begin(), l.end(), links);
+  for (int d = 0; d < 3; ++d) {
+    box[d] = lo[d];
+    box[3 + d] = hi[d];
+  }
+  return IMEXLB_OK;
+}
 
 // Not part of include/imexlb.h: lists the staged kernels' bulk copies so
 // that their alignment and bounds are checked on the CPU (tests).
