@@ -34,3 +34,71 @@ def test_fifo_one_at_a_time():
     # finishes at 1, 2, 3, 6 -> latencies 1, 1.5, 2.4, 1
     assert math.isclose(q["p50"], 1.25) and math.isclose(q["span"], 6.0)
     assert math.isclose(q["solves_per_s"], 4 / 6.0)
+
+
+class FakeEngine:
+    """The engine's step-limit semantics on the host: an instance with a
+    limit stops there; fields report the steps each instance took."""
+
+    def __init__(self, **kw):
+        self.taken, self.left, self.calls, self.res = {}, {}, [], {}
+        self.next = 0
+
+    def try_add(self, desc):
+        s = self.next
+        self.next += 1
+        self.taken[s], self.left[s], self.res[s] = 0, None, float("inf")
+        return s
+
+    def limit(self, slot, steps):
+        self.left[slot] = steps
+
+    def step(self, n):
+        self.calls.append(n)
+        for s in self.taken:
+            k = n if self.left[s] is None else min(n, self.left[s])
+            self.taken[s] += k
+            if self.left[s] is not None:
+                self.left[s] -= k
+            self.res[s] = 1.0 / (1 + self.taken[s])  # falls as the solve settles
+
+    def residuals(self):
+        return [self.res.get(s, float("inf")) for s in range(max(self.next, 1))]
+
+    def fields(self, slot):
+        return {"steps": self.taken[slot]}
+
+    def remove(self, slot):
+        del self.taken[slot], self.left[slot], self.res[slot]
+
+    def close(self):
+        pass
+
+
+def test_server_retires_each_request_at_its_own_step_count(monkeypatch):
+    monkeypatch.setattr(serve.api, "Engine", FakeEngine)
+    srv = serve.Server(chunk=100)
+    reqs = [serve.Request(i, 0.0, "tgv", (32, 32, 32), 100.0, m, tol=1e-9) for i, m in enumerate((30, 250, 100, 7))]
+    for r in reqs:
+        assert srv.try_admit(r)
+    retired = {}
+    while srv.active:
+        for req, f, steps, res in srv.advance():
+            retired[req.rid] = (f["steps"], steps)
+    # every answer is taken at exactly its request's step count
+    assert retired == {r.rid: (r.max_steps, r.max_steps) for r in reqs}
+    # fixed-length calls (the engine stops each instance at its own count),
+    # the last one only as long as the longest remaining request needs
+    assert srv.eng.calls == [100, 100, 50]
+
+
+def test_server_retires_on_the_residual_tolerance(monkeypatch):
+    monkeypatch.setattr(serve.api, "Engine", FakeEngine)
+    srv = serve.Server(chunk=100)
+    req = serve.Request(0, 0.0, "cavity", (32, 32, 32), 100.0, 10_000, tol=1.0 / 150)
+    assert srv.try_admit(req)
+    out = []
+    while srv.active:
+        out += srv.advance()
+    # residual 1 / (1 + steps) drops under the tolerance after 200 steps
+    assert [(r.rid, steps) for r, f, steps, res in out] == [(0, 200)]
