@@ -13,11 +13,13 @@ Metric: MLUPS (million lattice-cell updates per second), whole job.
             with CUDA events (barrier + synchronize on both sides, max over
             ranks); the two 470 MB distribution buffers exceed the 126 MB L2,
             so no flush is needed between steps.
-* e2e       the same solve through the public C ABI from host memory: create
-            (host set-up + upload), K steps with the u, v, w, p fields read
-            into pinned host buffers every K/10 steps (the reference driver's
-            output cadence, Time/inter = 10; imexlb_get_fields_async, each
-            copy overlapping the next steps), destroy, host wall clock.
+* e2e       the same solve through the public C ABI, host wall clock: create
+            (the cavity's initial state is built on the device; the vortex
+            uploads its initial fields), K steps in ten calls, each followed
+            by the velocity residual read into pinned host memory
+            (imexlb_reduce_async, the convergence check of a steady solve),
+            the u, v, w, p fields read into pinned host memory at the end,
+            destroy.
 * roofline  the fused step kernel: 432 algorithmic bytes per cell update
             (27 FP64 loads + 27 FP64 stores) x cells / its mean launch
             duration over the timed region (CUDA events on the launching
@@ -27,6 +29,11 @@ Metric: MLUPS (million lattice-cell updates per second), whole job.
             against the measured HBM copy bandwidth of MEASURED_PEAKS.json.
 * cpu_baseline  the reference's own solver (oracle/_ref) on the host cores,
             rank 0, a bounded sample of full-size steps (subprocess).
+* secondary the batched configuration (256 seeded instances, imexlb_b200.batch)
+            in FP16 storage and in plain FP64, each timed the same way over
+            K steps, with its own roofline and end-to-end figures, and the
+            ratio of the two aggregate MLUPS (one GPU only; --no-secondary
+            skips it).
 --impl reference runs only that CPU measurement (rank 0) and prints its line.
 With --gpus N (torchrun, one rank per GPU) every rank advances its own
 replica of the workload: the path has no exchange step ("replicas only").
@@ -197,6 +204,23 @@ def run_cpu_baseline(w, seconds: float, max_steps: int | None = None) -> dict:
                 seconds=res["seconds"])
 
 
+def create_upload_bytes(w) -> int:
+    """Host-to-device bytes imexlb_create copies for the workload's lattice:
+    the vortex's initial u, v, w, p (computed on the host with the
+    reference's expressions); the standard sphere's fluid mask and solid-link
+    table; the reference sphere's padded fields; nothing for the cavity, whose
+    initial state the device builds."""
+    nx, ny, nz = w["n"]
+    cells = nx * ny * nz
+    if w["case"] == "tgv":
+        return 4 * 8 * cells
+    if w["case"] == "sphere":
+        if w["bc"] == "standard":
+            return cells * (1 + 4)
+        return 4 * 8 * (nx + 6) * (ny + 6) * (nz + 6) + 4 * 8 * cells + cells
+    return 0
+
+
 def config_of(w, name, n_gpus) -> dict:
     nx, ny, nz = w["n"]
     return {"workload": name, "case": w["case"], "boundary": w["bc"], "storage": w["storage"],
@@ -244,42 +268,46 @@ def replica_throughput(elapsed_ms: float, seconds_e2e: float | None, cells: int,
     return value, max_ms, e2e, (max_e2e if seconds_e2e is not None else None)
 
 
-def bench_batch(args, w, name, cpu) -> int:
-    """The batched workload: all instances advance together in one engine
-    (persistent launches per kernel group, two steps per graph replay)."""
-    import numpy as np
+def measure_batch(storage: str, arith: str, steps: int, warmup: int, tune_cache=None, check_error=False,
+                  count: int = 256) -> dict:
+    """The batched configuration (imexlb_b200.batch): every instance advances
+    together in one engine (persistent launches per kernel group, two steps
+    per graph replay).  Device-timed aggregate MLUPS over `steps` steps after
+    `warmup`, and end to end from admission to every instance's u, v, w, p
+    in pinned host memory."""
     import torch
 
     from imexlb_b200 import api, batch, tune
 
-    specs = batch.batch_specs(w["count"])
+    specs = batch.batch_specs(count)
     cells = batch.total_cells(specs)
-    tiles = tune.tiles_for(specs, w["storage"], cache=args.tune_cache)
+    tiles = tune.tiles_for(specs, storage, cache=tune_cache)
     stream = torch.cuda.Stream()
-    budget = batch.budget_for(specs, w["storage"])
+    budget = batch.budget_for(specs, storage)
     with torch.cuda.stream(stream):
-        eng = api.Engine(storage=w["storage"], arith=w["arith"], budget_bytes=budget, max_instances=len(specs),
+        eng = api.Engine(storage=storage, arith=arith, budget_bytes=budget, max_instances=len(specs),
                          stream=stream.cuda_stream)
         slots = batch.add_all(eng, specs, tiles)
-        eng.step(args.warmup)
+        eng.step(warmup)
         torch.cuda.synchronize()
         sampler = ClockSampler(torch.cuda.current_device())
         sampler.start()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        eng.step(args.steps)
+        eng.step(steps)
         ev1.record(stream)
         ev1.synchronize()
         clocks = sampler.stop()
         ms = ev0.elapsed_time(ev1)
         stats = eng.stats()
-        fields = [eng.fields(s) for s in slots] if args.check_error else None
+        fields = [eng.fields(s) for s in slots] if check_error else None
         eng.close()
-    value = cells * args.steps / (ms * 1e-3) / 1e6
+    value = cells * steps / (ms * 1e-3) / 1e6
 
-    # end to end: admission from host (initial fields uploaded), the steps,
-    # every instance's u, v, w, p read back into pinned host memory (one
-    # pinned set per lattice shape, allocated beforehand as a caller would)
+    # end to end: admission from the host (the vortices' initial fields
+    # uploaded, the cavities' built on the device), the steps, every
+    # instance's u, v, w, p read back into pinned host memory (one pinned set
+    # per lattice shape, allocated beforehand as a caller would)
     pinned = {}
     for sp in specs:
         shp = (sp.edge,) * 3
@@ -288,54 +316,85 @@ def bench_batch(args, w, name, cpu) -> int:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
-        eng = api.Engine(storage=w["storage"], arith=w["arith"], budget_bytes=budget, max_instances=len(specs),
+        eng = api.Engine(storage=storage, arith=arith, budget_bytes=budget, max_instances=len(specs),
                          stream=stream.cuda_stream)
         slots = batch.add_all(eng, specs, tiles)
-        eng.step(args.steps)
-        for s, sp in zip(slots, specs):
-            eng.fields(s, out=pinned[(sp.edge,) * 3])
+        eng.step(steps)
+        for sl, sp in zip(slots, specs):
+            eng.fields(sl, out=pinned[(sp.edge,) * 3])
         eng.close()
     e2e_s = time.perf_counter() - t0
-    e2e = cells * args.steps / e2e_s / 1e6
+    e2e = cells * steps / e2e_s / 1e6
+    tgv_cells = sum(sp.cells for sp in specs if sp.case == "tgv")
 
     errs = None
-    if args.check_error:
+    if check_error:
         # the timed run took warm-up + timed steps: the FP64 run takes as many
-        ref = batch.run(specs, "f64", args.warmup + args.steps, fields=True)
+        ref = batch.run(specs, "f64", warmup + steps, fields=True)
         errs = batch.error_report(specs, fields, ref["fields"])
 
     peaks = load_peaks()
-    bpv = api.BYTES_PER_VALUE[w["storage"]]
-    step_ms = ms / args.steps
+    bpv = api.BYTES_PER_VALUE[storage]
+    step_ms = ms / steps
     achieved = 2 * 27 * bpv * cells / (step_ms * 1e-3) / 1e9
-    groups = len({(s.case, tiles.get(tune.key_of(w["storage"], s.case, (s.edge,) * 3), 0) == 0) for s in specs})
-    line = {
-        "metric": "D3Q27 MLUPS (aggregate over the batch)", "value": value, "unit": "MLUPS", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
-        "data": "synthetic: 256 seeded instances (analytic initial and boundary conditions)",
-        "config": {"workload": name, "instances": len(specs), "cells": cells, "storage": w["storage"],
-                   "mix": "TGV / lid-driven cavity 50/50, edge in {24..128}, Re log-uniform [50, 1000], U0 = 0.05",
-                   "seed": batch.BATCH_SEED, "tiles": "autotuned per (edge, case, storage)",
-                   "parallelism": "single GPU, one engine",
-                   "l2": f"inputs larger than L2 (distribution buffers {2 * 27 * bpv * cells / 1e9:.1f} GB)"},
+    groups = len({(sp.case, tiles.get(tune.key_of(storage, sp.case, (sp.edge,) * 3), 0) == 0) for sp in specs})
+    return {
+        "value": value, "unit": "MLUPS", "ms_per_step": step_ms, "steps": steps, "warmup": warmup,
+        "instances": len(specs), "cells": cells, "storage": storage, "seed": batch.BATCH_SEED,
         "roofline": {"bound": "hbm", "kernel": "engine step launches (all kernel groups of one step)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
                      "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
                      "bytes_per_cell_update": 2 * 27 * bpv},
-        "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * cells / args.steps,
-                "d2h_bytes_per_step": 4 * 8 * cells / args.steps, "seconds": e2e_s},
-        "gpu_launches": args.steps * groups,
-        "clocks": clocks,
+        "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * tgv_cells / steps,
+                "d2h_bytes_per_step": 4 * 8 * cells / steps, "seconds": e2e_s},
+        "gpu_launches": steps * groups, "clocks": clocks, "engine_tiles": stats["tiles"],
+        "per_instance_velocity_l2_vs_fp64": errs,
+    }
+
+
+def bench_batch(args, w, name, cpu) -> int:
+    """The batched workload's own bench line."""
+    from imexlb_b200 import batch
+
+    r = measure_batch(w["storage"], w["arith"], args.steps, args.warmup, args.tune_cache, args.check_error,
+                      w["count"])
+    cells, bpv = r["cells"], 2 if w["storage"] in ("f16", "bf16") else (4 if w["storage"] == "f32" else 8)
+    line = {
+        "metric": "D3Q27 MLUPS (aggregate over the batch)", "value": r["value"], "unit": "MLUPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
+        "data": "synthetic: 256 seeded instances (analytic initial and boundary conditions)",
+        "config": {"workload": name, "instances": r["instances"], "cells": cells, "storage": w["storage"],
+                   "mix": "TGV / lid-driven cavity 50/50, edge in {24..128}, Re log-uniform [50, 1000], U0 = 0.05",
+                   "seed": batch.BATCH_SEED, "tiles": "autotuned per (edge, case, storage)",
+                   "parallelism": "single GPU, one engine",
+                   "l2": f"inputs larger than L2 (distribution buffers {2 * 27 * bpv * cells / 1e9:.1f} GB)"},
+        "roofline": r["roofline"],
+        "e2e": r["e2e"],
+        "gpu_launches": r["gpu_launches"],
+        "clocks": r["clocks"],
         "cpu_baseline": ({"value": cpu["value"], "unit": "MLUPS", "cores": cpu["cores"], "kind": cpu["kind"],
                           "sample": cpu["sample"] + " (the batch's median-size cavity instance, 64^3)"}
                          if cpu else None),
-        "check": {"engine_tiles": stats["tiles"],
-                  "per_instance_velocity_l2_vs_fp64": errs},
+        "check": {"engine_tiles": r["engine_tiles"],
+                  "per_instance_velocity_l2_vs_fp64": r["per_instance_velocity_l2_vs_fp64"]},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def secondary_batches(args) -> dict:
+    """The batched configuration in FP16 storage and in plain FP64 at the
+    run's step counts, for the bench line of the default workload: the FP16
+    form's aggregate MLUPS against the FP64 form's on the same GPU."""
+    out = {}
+    for storage in ("f16", "f64"):
+        r = measure_batch(storage, "fast", args.steps, max(3, args.warmup), args.tune_cache)
+        r.pop("per_instance_velocity_l2_vs_fp64", None)
+        out[f"batched256_{storage}"] = r
+    out["f16_over_f64"] = out["batched256_f16"]["value"] / out["batched256_f64"]["value"]
+    return out
 
 
 def main(argv=None) -> int:
@@ -349,6 +408,8 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--check-error", action="store_true", help="batched workloads: per-instance error vs FP64")
     ap.add_argument("--tune-cache", default=None, help="batched workloads: autotuner cache (JSON)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="single-lattice workloads: skip the batched FP16 / FP64 measurements (secondary)")
     args = ap.parse_args(argv)
     w = WORKLOADS[args.workload]
     name = args.workload
@@ -431,31 +492,39 @@ def main(argv=None) -> int:
 
     value, max_ms, _, _ = replica_throughput(elapsed_ms, None, cells, args.steps, dist)
 
-    # ---- end to end through the public API, host memory in and out
-    outputs = 10
-    chunk = max(1, args.steps // outputs)
-    # two pinned sets: each output is copied while the next chunk's steps
-    # run (imexlb_get_fields_async), into the set the host is not holding
-    pinned = [{k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
-              for _ in range(2)]
+    # ---- end to end through the public API, host memory in and out: create
+    # the lattice, run the steps in ten calls with the velocity residual of
+    # each call read back (the convergence check of a steady solve), read
+    # the u, v, w, p fields once at the end, destroy
+    checks = 10
+    chunk = max(1, args.steps // checks)
+    pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
+    resid = torch.empty(checks + 1, dtype=torch.float64, pin_memory=True).numpy()
     barrier()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         lbm2 = api.LBM(w["case"], nx, ny, nz, tau, 1.0, w["u0"], stream=stream.cuda_stream, **kw)
         done = 0
-        nout = 0
+        nres = 0
         while done < args.steps:
             s = min(chunk, args.steps - done)
             lbm2.step(s)
             done += s
-            lbm2.fields(out=pinned[nout % 2], wait=False)
-            nout += 1
-        lbm2.synchronize()  # every output is in host memory
+            lbm2.reduce_async("residual", resid, min(nres, checks))
+            nres += 1
+        lbm2.fields(out=pinned, wait=False)
+        lbm2.synchronize()  # every residual and the fields are in host memory
         lbm2.close()
     e2e_s = time.perf_counter() - t0
     _, _, e2e, e2e_s = replica_throughput(elapsed_ms, e2e_s, cells, args.steps, dist)
-    h2d = 4 * 8 * cells / args.steps  # the initial u, v, w, p fields uploaded at create
-    d2h = nout * 4 * 8 * cells / args.steps
+    h2d = create_upload_bytes(w) / args.steps
+    d2h = (nres * 8 + 4 * 8 * cells) / args.steps
+
+    # the batched configuration in FP16 storage and FP64 beside the headline
+    # (one GPU; measured after the headline's timed regions)
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        secondary = secondary_batches(args)
 
     if rank == 0:
         peaks = load_peaks()
@@ -489,13 +558,19 @@ def main(argv=None) -> int:
                          "ghost_gather_ms_per_step": kt["ghost_ms"] / max(1, kt["ghost_launches"])
                          if kt["ghost_launches"] else 0.0},
             "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "seconds": e2e_s, "outputs": nout},
+                    "seconds": e2e_s, "residual_reads": nres, "field_reads": 1,
+                    "inputs": ("the case parameters: the cavity starts at rest (f = 0) and its initial state "
+                               "is built on the device, as the reference's Initialize builds it"
+                               if h2d == 0 else "initial fields and masks uploaded at create"),
+                    "final_residual": float(resid[min(nres, checks) - 1]) if nres else None},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": ({"value": cpu["value"], "unit": "MLUPS", "cores": cpu["cores"], "kind": cpu["kind"],
                               "sample": cpu["sample"]} if cpu else None),
             "check": {"max_speed_after_run": resid},
         }
+        if secondary is not None:
+            line["secondary"] = secondary
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

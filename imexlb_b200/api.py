@@ -77,7 +77,7 @@ class EngineStats(ctypes.Structure):
 # Every symbol include/imexlb.h declares (tests check the library exports them).
 EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imexlb_initialize", "imexlb_step",
            "imexlb_get_fields", "imexlb_get_fields_async", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
-           "imexlb_reduce_fields_noalloc", "imexlb_steps_taken",
+           "imexlb_reduce_async", "imexlb_reduce_fields_noalloc", "imexlb_release_cached_memory", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
            "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
            "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_remove",
@@ -108,6 +108,8 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_get_mask.argtypes = [vp, vp]
     lib.imexlb_write_tecplot.argtypes = [vp, ctypes.c_char_p, i]
     lib.imexlb_reduce.argtypes = [vp, i, ctypes.POINTER(d)]
+    lib.imexlb_reduce_async.argtypes = [vp, i, vp]
+    lib.imexlb_release_cached_memory.argtypes = []
     lib.imexlb_reduce_fields_noalloc.argtypes = [i, vp, vp, vp, vp, ctypes.c_int64, vp, vp]
     lib.imexlb_steps_taken.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.imexlb_footprint.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(d)]
@@ -255,6 +257,12 @@ class LBM:
         _check(self.lib.imexlb_reduce(self.h, REDUCE[kind], out))
         return out[0] if kind != "drag" else (out[0], out[1], out[2])
 
+    def reduce_async(self, kind: str, out: np.ndarray, index: int = 0):
+        """Queue a one-value reduction whose value lands in out[index] (an FP64
+        array, pinned for the copy to overlap) by the next synchronize()."""
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and 0 <= index < out.size
+        _check(self.lib.imexlb_reduce_async(self.h, REDUCE[kind], out.ctypes.data + 8 * index))
+
     def checkpoint(self) -> bytes:
         """The lattice's state (both buffers, moments, step count) as bytes."""
         n = ctypes.c_size_t()
@@ -287,6 +295,11 @@ class LBM:
         per = ctypes.c_double()
         _check(self.lib.imexlb_footprint(self.h, ctypes.byref(b), ctypes.byref(per)))
         return b.value, per.value
+
+
+def release_cached_memory():
+    """Return the lattice pool's reserved device memory of the current device."""
+    _check(load_library().imexlb_release_cached_memory())
 
 
 def instance_desc(case: str, nx: int, ny: int, nz: int, tau: float, rho0: float = 1.0, u0: float = 0.05, *,

@@ -155,26 +155,48 @@ def error_report(specs, fields, ref_fields, worst: int = 5) -> dict:
     }
 
 
+def per_instance(specs, fields, ref_fields) -> list[dict]:
+    """One record per instance: its parameters and its relative velocity L2
+    against the FP64 run (None where either run is not finite)."""
+    out = []
+    for s, g, w in zip(specs, fields, ref_fields):
+        ok_ref, ok_run = finite(w), finite(g)
+        out.append(dict(case=s.case, edge=s.edge, Re=s.Re, tau=s.tau0 + 0.5, fp64_finite=ok_ref, finite=ok_run,
+                        err=velocity_l2(g, w) if ok_ref and ok_run else None))
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--storage", default="f16", choices=sorted(api.STORAGES))
+    ap.add_argument("--storage", default="f16", help="storage format, or several separated by commas")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--check", action="store_true", help="also run FP64 and report per-instance errors")
+    ap.add_argument("--dump", default=None, help="with --check: write every instance's error to this JSON file")
     ap.add_argument("--tune-cache", default=None)
     args = ap.parse_args(argv)
     from . import tune
 
     specs = batch_specs(args.count)
-    tiles = tune.tiles_for(specs, args.storage, cache=args.tune_cache)
-    t0 = time.perf_counter()
-    res = run(specs, args.storage, args.steps, tiles=tiles, fields=args.check)
-    line = dict(storage=args.storage, instances=len(specs), cells=res["cells"], steps=args.steps,
-                mlups=res["mlups"], device_ms=res["ms"], wall_s=time.perf_counter() - t0)
-    if args.check:
-        ref = run(specs, "f64", args.steps, fields=True)
-        line.update(fp64_mlups=ref["mlups"], errors=error_report(specs, res["fields"], ref["fields"]))
-    print(json.dumps(line))
+    storages = args.storage.split(",")
+    for st in storages:
+        if st not in api.STORAGES:
+            raise SystemExit(f"unknown storage {st}")
+    ref = run(specs, "f64", args.steps, fields=True) if args.check else None
+    dump = {}
+    for st in storages:
+        tiles = tune.tiles_for(specs, st, cache=args.tune_cache)
+        t0 = time.perf_counter()
+        res = run(specs, st, args.steps, tiles=tiles, fields=args.check)
+        line = dict(storage=st, instances=len(specs), cells=res["cells"], steps=args.steps,
+                    mlups=res["mlups"], device_ms=res["ms"], wall_s=time.perf_counter() - t0)
+        if args.check:
+            line.update(fp64_mlups=ref["mlups"], errors=error_report(specs, res["fields"], ref["fields"]))
+            dump[st] = per_instance(specs, res["fields"], ref["fields"])
+        print(json.dumps(line), flush=True)
+    if args.dump and dump:
+        with open(args.dump, "w") as fh:
+            json.dump(dict(steps=args.steps, seed=BATCH_SEED, instances=dump), fh)
     return 0
 
 

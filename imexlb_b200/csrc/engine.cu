@@ -899,11 +899,12 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
     P.sphere_c[1] = d->ny / 2.0;
     P.sphere_c[2] = d->nz / 2.0;
   }
-  std::vector<int32_t> usr_pad(d->kase == IMEXLB_SPHERE ? static_cast<size_t>(sl.ncell) : 0, 1);
   const size_t n = static_cast<size_t>(sl.ncell);
-  // everything this admission uploads goes through one pinned buffer:
-  // moments, then (sphere) mask and links, then the instance descriptor
-  const size_t up_mom = 4 * n * 8, up_mask = d->kase == IMEXLB_SPHERE ? n : 0;
+  // everything this admission uploads goes through one pinned buffer: the
+  // vortex's initial moments (the cavity starts at rest and the sphere
+  // channel's fields follow from its mask, both set on the device), then
+  // (sphere) mask and links, then the instance descriptor
+  const size_t up_mom = d->kase == IMEXLB_TGV ? 4 * n * 8 : 0, up_mask = d->kase == IMEXLB_SPHERE ? n : 0;
   const size_t up_links = d->kase == IMEXLB_SPHERE ? 4 * n : 0;
   const size_t off_links = (up_mom + up_mask + 15) & ~static_cast<size_t>(15);
   const size_t off_inst = (off_links + up_links + 15) & ~static_cast<size_t>(15);
@@ -914,9 +915,14 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
     return efail(IMEXLB_E_NOMEM, std::string("pinned upload buffer: ") + cudaGetErrorString(serr));
   }
   char* up = e->staging.ptr(sb);
-  // the initial u, v, w, p straight into the pinned buffer
-  case_fields(P, sl.L, nullptr, &usr_pad, reinterpret_cast<double*>(up));
-  IMX_ECUDA(cudaMemcpyAsync(mom, up, up_mom, cudaMemcpyHostToDevice, e->stream));
+  if (d->kase == IMEXLB_TGV) {
+    // the initial u, v, w, p straight into the pinned buffer
+    std::vector<int32_t> no_mask;
+    case_fields(P, sl.L, nullptr, &no_mask, reinterpret_cast<double*>(up));
+    IMX_ECUDA(cudaMemcpyAsync(mom, up, up_mom, cudaMemcpyHostToDevice, e->stream));
+  } else if (d->kase == IMEXLB_CAVITY) {
+    IMX_ECUDA(cudaMemsetAsync(mom, 0, 4 * n * 8, e->stream));  // at rest: u = p = 0
+  }
 
   EngInst& in = e->h_inst[s];
   in = EngInst{};
@@ -956,13 +962,14 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {
     uint8_t* m = reinterpret_cast<uint8_t*>(up + up_mom);
-    for (size_t c = 0; c < n; ++c) m[c] = static_cast<uint8_t>(usr_pad[c]);
+    std_sphere_mask(P, m);
     std::vector<uint32_t> lk;
     int lo[3], hi[3];
     solid_links(d->nx, d->ny, d->nz, m, lk, lo, hi);
     std::memcpy(up + off_links, lk.data(), n * 4);
     IMX_ECUDA(cudaMemcpyAsync(usr, m, n, cudaMemcpyHostToDevice, e->stream));
     IMX_ECUDA(cudaMemcpyAsync(links, up + off_links, n * 4, cudaMemcpyHostToDevice, e->stream));
+    IMX_ECUDA(launch_sphere_fields(usr, sl.ncell, P.inlet_u, mom, e->stream));
     a.usr = usr;
     a.links = links;
     for (int c = 0; c < 3; ++c) {

@@ -18,6 +18,7 @@
 // the 18 populations with e_x != 0 are served from L1/L2.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <math_constants.h>
 
 #include <type_traits>
 #include <utility>
@@ -62,6 +63,19 @@ __global__ void init_f_kernel(Layout L, typename StoreT<S>::T* b0, typename Stor
     b0[b + q * L.sq] = val;
     if (b1) b1[b + q * L.sq] = val;
   });
+}
+
+// Initial fields of the standard sphere channel over the interior (x
+// fastest): the inflow velocity (ui, 0, 0) in the fluid, rest in the solid,
+// zero pressure deviation; out holds u, then v, w, p (n values each).
+__global__ void sphere_fields_kernel(const uint8_t* fluid, int64_t n, double ui, double* out) {
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < n;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[c] = fluid[c] ? ui : 0.0;
+    out[n + c] = 0.0;
+    out[2 * n + c] = 0.0;
+    out[3 * n + c] = 0.0;
+  }
 }
 
 // Programmatic dependent launch of consecutive steps (launch_pdl): a step
@@ -398,7 +412,27 @@ __global__ void reduce_pass2(RedKind kind, const double* part, int nparts, doubl
   }
 }
 
+// The velocity residual sqrt(num / den) from the two sums of the residual
+// reduction, as the synchronous path forms it on the host (INFINITY on the
+// first call, NaN when a sum is not finite).
+__global__ void residual_finish_kernel(const double* nd, int first, double* out) {
+  const double num = nd[0], den = nd[1];
+  double r;
+  if (first)
+    r = CUDART_INF;
+  else if (!isfinite(num) || !isfinite(den))
+    r = CUDART_NAN;
+  else
+    r = den > 0.0 ? sqrt(num / den) : (num > 0.0 ? CUDART_INF : 0.0);
+  *out = r;
+}
+
 }  // namespace
+
+cudaError_t launch_residual_finish(const double* nd, int first, double* out, cudaStream_t s) {
+  residual_finish_kernel<<<1, 1, 0, s>>>(nd, first, out);
+  return cudaGetLastError();
+}
 
 dim3 step_block(int nx) {
   if (nx >= 128) return dim3(128, 2, 1);
@@ -555,6 +589,12 @@ cudaError_t launch_cavity_records(const Layout& L, const void* buf, uint16_t* re
   if (L.elem != 2 || L.g != 0) return cudaErrorInvalidValue;
   const dim3 block(64, 1, 1), grid((L.ny + 63) / 64, L.nz, 1);
   cavity_records_kernel<<<grid, block, 0, s>>>(L, static_cast<const uint16_t*>(buf), rec);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sphere_fields(const uint8_t* fluid, int64_t n, double ui, double* out, cudaStream_t s) {
+  const int64_t want = (n + 255) / 256;
+  sphere_fields_kernel<<<static_cast<int>(want < 148 * 16 ? want : 148 * 16), 256, 0, s>>>(fluid, n, ui, out);
   return cudaGetLastError();
 }
 

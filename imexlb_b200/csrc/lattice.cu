@@ -15,6 +15,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -52,20 +53,65 @@ uint64_t splitmix64(uint64_t x) {
   return x ^ (x >> 31);
 }
 
+// Device memory of single lattices comes from one stream-ordered pool per
+// device that keeps freed memory reserved (up to POOL_KEEP_BYTES, or until
+// imexlb_release_cached_memory), so that creating a lattice after another was
+// destroyed neither maps new memory nor waits for the device, as cudaMalloc
+// and cudaFree of a few hundred MB do (tens of ms for a 128^3 FP64 lattice).
+constexpr uint64_t POOL_KEEP_BYTES = 16ull << 30;
+constexpr int POOL_MAX_DEVICES = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[POOL_MAX_DEVICES] = {};
+
+cudaError_t lattice_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= POOL_MAX_DEVICES) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+    uint64_t keep = POOL_KEEP_BYTES;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return cudaSuccess;
+}
+
+// A device array of a lattice, allocated from the lattice pool in the order
+// of the lattice's stream and returned to it the same way.  alloc() waits
+// for the stream once, so the memory is then usable from any stream and by
+// synchronous copies.
 template <class T>
 struct DevArray {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;
   ~DevArray() { reset(); }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     n = 0;
   }
-  cudaError_t alloc(size_t count) {
+  cudaError_t alloc(size_t count, cudaStream_t stream) {
     reset();
+    if (!count) return cudaSuccess;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = lattice_pool(&pool);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, stream)) != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
     n = count;
-    return count ? cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)) : cudaSuccess;
+    s = stream;
+    return cudaStreamSynchronize(stream);
   }
 };
 
@@ -340,8 +386,7 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
       for (int j = 0; j < L.ey; ++j)
         for (int i = 0; i < L.ex; ++i) {
           const size_t c = at(i, j, k);
-          const double dx = i - P.sphere_c[0], dy = j - P.sphere_c[1], dz = k - P.sphere_c[2];
-          const bool solid = dx * dx + dy * dy + dz * dz <= 0.25 * P.sphere_d * P.sphere_d;
+          const bool solid = std_sphere_solid(P, i, j, k);
           (*usr_padded)[c] = solid ? 0 : 1;
           U[c] = solid ? 0.0 : ui;
           V[c] = W[c] = Pf[c] = 0.0;
@@ -356,9 +401,64 @@ void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, st
 }
 }  // namespace imx
 
+namespace imx {
+bool std_sphere_solid(const imexlb_params& P, int i, int j, int k) {
+  const double dx = i - P.sphere_c[0], dy = j - P.sphere_c[1], dz = k - P.sphere_c[2];
+  return dx * dx + dy * dy + dz * dz <= 0.25 * P.sphere_d * P.sphere_d;
+}
+
+void std_sphere_mask(const imexlb_params& P, uint8_t* fluid) {
+  const size_t plane = static_cast<size_t>(P.nx) * P.ny;
+  for_planes(P.nz, plane, [&](int k) {
+    for (int j = 0; j < P.ny; ++j)
+      for (int i = 0; i < P.nx; ++i)
+        fluid[i + static_cast<size_t>(P.nx) * j + plane * k] = std_sphere_solid(P, i, j, k) ? 0 : 1;
+  });
+}
+}  // namespace imx
+
 namespace {
 
+// The cavity (at rest: u = p = 0, lid_driven_cavity/src/lbm.cpp:191-198, so
+// f = feq(0, 0) = +0 in every storage format) and the standard sphere channel
+// (inflow velocity in the fluid) have initial states the device builds from
+// the case parameters and the mask; the vortex's and the reference sphere's
+// initial fields are computed on the host with the reference's expressions
+// and libm (tgv/src/lbm.cpp:195-206, sphere/src/lbm.cpp:231-242).
+bool device_initial_state(const imexlb_params& P) {
+  return P.kase == IMEXLB_CAVITY || (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_STANDARD);
+}
+
+int upload_device_case(imexlb_lattice* h) {
+  const Layout& L = h->L;
+  if (h->P.kase == IMEXLB_CAVITY) {
+    IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
+    IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
+    IMX_CUDA(cudaMemsetAsync(h->mom.p, 0, h->mom.n * sizeof(double), h->stream));
+  } else {
+    // g = 0: the stored box is the interior, and init_f reads the moment views
+    IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
+    IMX_CUDA(cudaMemsetAsync(h->buf[1].p, 0, h->buf[1].n, h->stream));
+    IMX_CUDA(launch_sphere_fields(h->usr.p, h->ncell, h->P.inlet_u, h->mom.p, h->stream));
+    const double* src = h->mom.p;
+    const int64_t n = h->ncell;
+    IMX_CUDA(launch_init_f(h->cfg, L, h->buf[0].p, h->buf[1].p, src, src + n, src + 2 * n, src + 3 * n, h->p_shift,
+                           h->enc, h->stream));
+  }
+  for (int b = 0; b < 2 && h->rec[b].p; ++b) IMX_CUDA(launch_cavity_records(L, h->buf[b].p, h->rec[b].p, h->stream));
+  // reference boundaries: the first step's passes act on the initial state
+  if (h->gn)
+    IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[0].p, h->buf[1].p, h->gtgt.p, h->gsrc.p, h->gn, L.sq, h->enc,
+                                 h->stream));
+  IMX_CUDA(cudaStreamSynchronize(h->stream));
+  h->cur = 0;
+  h->steps = 0;
+  h->have_prev = false;
+  return IMEXLB_OK;
+}
+
 int upload_case(imexlb_lattice* h) {
+  if (device_initial_state(h->P)) return upload_device_case(h);
   const Layout& L = h->L;
   const size_t n = static_cast<size_t>(L.ex) * L.ey * L.ez;
   std::unique_ptr<double[]> host(new double[4 * n]);  // every element written below
@@ -372,7 +472,7 @@ int upload_case(imexlb_lattice* h) {
   // copy of the padded box and the interior is gathered on the host.
   const bool interior = L.g == 0;
   DevArray<double> tmp;
-  if (!interior) IMX_CUDA(tmp.alloc(4 * n));
+  if (!interior) IMX_CUDA(tmp.alloc(4 * n, h->stream));
   double* src = interior ? h->mom.p : tmp.p;
   IMX_CUDA(cudaMemcpyAsync(src, U, 4 * n * 8, cudaMemcpyHostToDevice, h->stream));
   IMX_CUDA(cudaMemsetAsync(h->buf[0].p, 0, h->buf[0].n, h->stream));
@@ -521,13 +621,13 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
     }
   }
 
-  IMX_CUDA(h->buf[0].alloc(L.bytes()));
-  IMX_CUDA(h->buf[1].alloc(L.bytes()));
+  IMX_CUDA(h->buf[0].alloc(L.bytes(), h->stream));
+  IMX_CUDA(h->buf[1].alloc(L.bytes(), h->stream));
   if (uses_wall_records(h->cfg, P.nx, P.ny, L.pitch))
-    for (int b = 0; b < 2; ++b) IMX_CUDA(h->rec[b].alloc(static_cast<size_t>(P.ny) * P.nz * WallRecord::WORDS));
-  IMX_CUDA(h->mom.alloc(4 * static_cast<size_t>(h->ncell)));
-  IMX_CUDA(h->red.alloc(reduce_blocks() + 8));
-  IMX_CUDA(h->err.alloc(1));
+    for (int b = 0; b < 2; ++b) IMX_CUDA(h->rec[b].alloc(static_cast<size_t>(P.ny) * P.nz * WallRecord::WORDS, h->stream));
+  IMX_CUDA(h->mom.alloc(4 * static_cast<size_t>(h->ncell), h->stream));
+  IMX_CUDA(h->red.alloc(reduce_blocks() + 8, h->stream));
+  IMX_CUDA(h->err.alloc(1, h->stream));
   IMX_CUDA(cudaMemset(h->err.p, 0, sizeof(int)));
 
   // base step arguments
@@ -559,17 +659,22 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   a.p_shift = h->p_shift;
   a.enc = h->enc;
 
-  // initial fields need usr_padded before the mask goes to the device
+  // the mask goes to the device before the initial state is set
   if (P.kase == IMEXLB_SPHERE) {
-    std::unique_ptr<double[]> fields(new double[4 * static_cast<size_t>(L.ex) * L.ey * L.ez]);
-    init_fields(h.get(), fields.get());  // fills usr_padded
     std::vector<uint8_t> m(static_cast<size_t>(h->ncell));
-    for (int k = 0; k < P.nz; ++k)
-      for (int j = 0; j < P.ny; ++j)
-        for (int i = 0; i < P.nx; ++i)
-          m[i + static_cast<size_t>(P.nx) * (j + static_cast<size_t>(P.ny) * k)] = static_cast<uint8_t>(
-              h->usr_padded[(i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g))]);
-    IMX_CUDA(h->usr.alloc(m.size()));
+    if (ref_sphere) {
+      std::unique_ptr<double[]> fields(new double[4 * static_cast<size_t>(L.ex) * L.ey * L.ez]);
+      init_fields(h.get(), fields.get());  // fills usr_padded
+      for (int k = 0; k < P.nz; ++k)
+        for (int j = 0; j < P.ny; ++j)
+          for (int i = 0; i < P.nx; ++i)
+            m[i + static_cast<size_t>(P.nx) * (j + static_cast<size_t>(P.ny) * k)] = static_cast<uint8_t>(
+                h->usr_padded[(i + L.g) + static_cast<size_t>(L.ex) * ((j + L.g) + static_cast<size_t>(L.ey) * (k + L.g))]);
+    } else {
+      std_sphere_mask(P, m.data());  // the stored box is the interior (g = 0)
+      for (size_t c = 0; c < m.size(); ++c) h->usr_padded[c] = m[c];
+    }
+    IMX_CUDA(h->usr.alloc(m.size(), h->stream));
     IMX_CUDA(cudaMemcpy(h->usr.p, m.data(), m.size(), cudaMemcpyHostToDevice));
     a.usr = h->usr.p;
     if (ref_sphere) {
@@ -577,14 +682,14 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       const int glz = P.nz;
       for (int k = 0; k < P.nz; ++k)  // sphere/src/lbm.cpp:405
         prof[k] = P.u0 * 4.0 * k * (glz - 1 - k) / std::pow(static_cast<double>(glz - 1), 2);
-      IMX_CUDA(h->inlet.alloc(prof.size()));
+      IMX_CUDA(h->inlet.alloc(prof.size(), h->stream));
       IMX_CUDA(cudaMemcpy(h->inlet.p, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
       a.inlet = h->inlet.p;
     } else {
       std::vector<uint32_t> links;
       int lo[3], hi[3];
       solid_links(P.nx, P.ny, P.nz, m.data(), links, lo, hi);
-      IMX_CUDA(h->links.alloc(links.size()));
+      IMX_CUDA(h->links.alloc(links.size(), h->stream));
       IMX_CUDA(cudaMemcpy(h->links.p, links.data(), links.size() * 4, cudaMemcpyHostToDevice));
       a.links = h->links.p;
       for (int d = 0; d < 3; ++d) {
@@ -592,7 +697,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
         a.near_hi[d] = hi[d];
       }
       h->drag_blocks = step_grid_blocks(h->cfg, P.nx, P.ny, P.nz);
-      IMX_CUDA(h->drag_part.alloc(3 * static_cast<size_t>(h->drag_blocks)));
+      IMX_CUDA(h->drag_part.alloc(3 * static_cast<size_t>(h->drag_blocks), h->stream));
       IMX_CUDA(cudaMemset(h->drag_part.p, 0, h->drag_part.n * sizeof(double)));
       // 2-byte x-pair formats store deviations from the inflow's equilibrium
       const double ui = P.inlet_u;
@@ -634,8 +739,8 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
     }
     h->gn = static_cast<int64_t>(t.size());
-    IMX_CUDA(h->gtgt.alloc(t.size()));
-    IMX_CUDA(h->gsrc.alloc(s.size()));
+    IMX_CUDA(h->gtgt.alloc(t.size(), h->stream));
+    IMX_CUDA(h->gsrc.alloc(s.size(), h->stream));
     IMX_CUDA(cudaMemcpy(h->gtgt.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
     IMX_CUDA(cudaMemcpy(h->gsrc.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice));
   }
@@ -870,7 +975,7 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
       IMX_CUDA(launch_reduce(RedKind::UMax, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
       break;
     case IMEXLB_REDUCE_RESIDUAL: {
-      if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N)));
+      if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N), h->stream));
       double num = 0, den = 0;
       if (h->have_prev) {
         IMX_CUDA(launch_reduce(RedKind::DiffSq, u, v, w, p, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N,
@@ -903,6 +1008,45 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
   IMX_CUDA(cudaMemcpyAsync(out, res, 8, cudaMemcpyDeviceToHost, h->stream));
   if (const int rc = sync_checked(h)) return rc;
   if (!std::isfinite(*out)) return fail(IMEXLB_E_STATE, "lattice is not finite (NaN/Inf in the moments)");
+  return IMEXLB_OK;
+}
+
+int imexlb_reduce_async(imexlb_lattice* h, int kind, double* out) {
+  if (!h || !out) return fail(IMEXLB_E_ARG, "null argument");
+  const int64_t N = h->ncell;
+  const double* u = h->mom.p;
+  const double* v = u + N;
+  const double* w = u + 2 * N;
+  const double* p = u + 3 * N;
+  double* part = h->red.p;
+  double* res = h->red.p + reduce_blocks();  // res[0..1]: sums, res[2]: the residual
+  double* val = res;
+  switch (kind) {
+    case IMEXLB_REDUCE_MASS:
+      IMX_CUDA(launch_reduce(RedKind::Mass, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_KINETIC:
+      IMX_CUDA(launch_reduce(RedKind::Kinetic, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_UMAX:
+      IMX_CUDA(launch_reduce(RedKind::UMax, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
+      break;
+    case IMEXLB_REDUCE_RESIDUAL:
+      if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N), h->stream));
+      if (h->have_prev) {
+        IMX_CUDA(launch_reduce(RedKind::DiffSq, u, v, w, p, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N,
+                               part, res, h->stream));
+        IMX_CUDA(launch_reduce(RedKind::NormSq, u, v, w, p, nullptr, nullptr, nullptr, N, part, res + 1, h->stream));
+      }
+      IMX_CUDA(launch_residual_finish(res, h->have_prev ? 0 : 1, res + 2, h->stream));
+      IMX_CUDA(cudaMemcpyAsync(h->prev_mom.p, u, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      h->have_prev = true;
+      val = res + 2;
+      break;
+    default:
+      return fail(IMEXLB_E_ARG, "unknown or unsupported asynchronous reduction");
+  }
+  IMX_CUDA(cudaMemcpyAsync(out, val, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   return IMEXLB_OK;
 }
 
@@ -1055,6 +1199,22 @@ void imexlb_destroy(imexlb_lattice* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
   delete h;
+}
+
+int imexlb_release_cached_memory(void) {
+  int dev = 0;
+  IMX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= POOL_MAX_DEVICES) return IMEXLB_OK;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    pool = g_pools[dev];
+  }
+  if (pool) {
+    IMX_CUDA(cudaDeviceSynchronize());
+    IMX_CUDA(cudaMemPoolTrimTo(pool, 0));
+  }
+  return IMEXLB_OK;
 }
 
 const char* imexlb_last_error(void) { return g_last_error.c_str(); }

@@ -148,6 +148,11 @@ bool build_ghost_plan_keys(int kase, int nx, int ny, int nz, const int32_t* usr_
 // pinned upload buffer.  `usr_padded` (spheres) holds n values.
 void case_fields(const imexlb_params& P, const Layout& L, const int32_t* ran, std::vector<int32_t>* usr_padded,
                  double* out);
+// The standard sphere channel's voxelised sphere: cell (i, j, k) is solid
+// when |x - c|^2 <= d^2 / 4 (each operation rounded on its own).
+bool std_sphere_solid(const imexlb_params& P, int i, int j, int k);
+// Its fluid mask (1 = fluid) over the interior, x fastest (ncell values).
+void std_sphere_mask(const imexlb_params& P, uint8_t* fluid);
 void solid_links(int nx, int ny, int nz, const uint8_t* fluid, std::vector<uint32_t>& links, int lo[3], int hi[3]);
 
 // Header of a checkpoint (imexlb_checkpoint_*, imexlb_engine_checkpoint_*):
@@ -195,6 +200,9 @@ cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void*
                           const double* v, const double* w, const double* p, double p_shift, const Encoding& enc,
                           cudaStream_t s);
 cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s);
+// Initial u, v, w, p of the standard sphere channel from its interior fluid
+// mask (out: 4 n values; the inflow velocity ui in the fluid, rest elsewhere).
+cudaError_t launch_sphere_fields(const uint8_t* fluid, int64_t n, double ui, double* out, cudaStream_t s);
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
                                 int64_t n, int64_t sq, const Encoding& enc, cudaStream_t s);
 dim3 step_block(int nx);
@@ -211,6 +219,8 @@ cudaError_t launch_drag_links(Store st, const StepArgs& a, cudaStream_t s);
 // for the requested quantity; partial sums of `blocks` blocks go to scratch.
 enum class RedKind : int { Mass = 0, Kinetic = 1, DiffSq = 2, NormSq = 3, UMax = 4 };
 int reduce_blocks();
+// out = sqrt(nd[0] / nd[1]) with the residual's conventions (one thread).
+cudaError_t launch_residual_finish(const double* nd, int first, double* out, cudaStream_t s);
 cudaError_t launch_reduce(RedKind k, const double* u, const double* v, const double* w, const double* p,
                           const double* u2, const double* v2, const double* w2, int64_t n, double* scratch,
                           double* out, cudaStream_t s);

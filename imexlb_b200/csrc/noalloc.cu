@@ -13,7 +13,12 @@
 // The array is a file-scope __device__ variable: every GPU that loads this
 // library holds it (32 KiB) until the process exits.  Host code cannot use the
 // array's name as a device address, so the first call on each device looks the
-// address up with cudaGetSymbolAddress (with that device current) and keeps it.
+// address up with cudaGetSymbolAddress (with that device current) and keeps it
+// together with the CUDA context it belongs to.  A reset of the device's
+// primary context (cudaDeviceReset) reloads the module, and the array may then
+// sit elsewhere: a call that finds a different current context looks the
+// address up again.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,8 +37,12 @@ constexpr int NA_MAX_DEVICES = 64;
 
 __device__ __align__(256) double g_noalloc_partials[NA_MAX_PARTIALS];
 
+// The maximum keeps a NaN (fmax would drop it), so a non-finite field shows
+// in the result of every kind: sums turn NaN or infinite by themselves.
+__device__ __forceinline__ double na_max(double a, double b) { return (a >= b || a != a) ? a : b; }
+
 __device__ __forceinline__ double na_combine(int kind, double a, double b) {
-  return kind == IMEXLB_REDUCE_UMAX ? fmax(a, b) : a + b;
+  return kind == IMEXLB_REDUCE_UMAX ? na_max(a, b) : a + b;
 }
 
 __device__ __forceinline__ double na_block_reduce(int kind, double x) {
@@ -82,25 +91,52 @@ __global__ void na_pass2(int kind, const double* partial, int nparts, double* ou
 }
 
 std::mutex g_mu;
-double* g_partials_addr[NA_MAX_DEVICES] = {};
+struct ScratchAddr {
+  CUcontext ctx = nullptr;  // the context the address belongs to
+  double* addr = nullptr;
+};
+ScratchAddr g_partials_addr[NA_MAX_DEVICES];
 
-// The device address of g_noalloc_partials on the current device, looked up
-// once per device.
+// cuCtxGetCurrent through the runtime's driver entry point (the library does
+// not link the driver library directly); resolved once.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// The device address of g_noalloc_partials on the current device: looked up
+// on the first call on each device and again whenever the device's current
+// context is no longer the one the address was looked up in.
 int partials_on_current_device(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return imx::set_last_error(IMEXLB_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= NA_MAX_DEVICES) return imx::set_last_error(IMEXLB_E_UNSUPPORTED, "device ordinal above 63");
+  const CtxGetCurrentFn get_ctx = ctx_get_current();
+  if (!get_ctx) return imx::set_last_error(IMEXLB_E_CUDA, "no-alloc reduction: cuCtxGetCurrent is unavailable");
+  CUcontext ctx = nullptr;
+  if (get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_partials_addr[dev]) {
+  ScratchAddr& slot = g_partials_addr[dev];
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     void* addr = nullptr;
-    e = cudaGetSymbolAddress(&addr, g_noalloc_partials);
+    e = cudaGetSymbolAddress(&addr, g_noalloc_partials);  // makes the device's primary context current if none is
     if (e != cudaSuccess || !addr)
       return imx::set_last_error(IMEXLB_E_CUDA,
                                  std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
-    g_partials_addr[dev] = static_cast<double*>(addr);
+    if (get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+    slot.ctx = ctx;
+    slot.addr = static_cast<double*>(addr);
   }
-  *out = g_partials_addr[dev];
+  *out = slot.addr;
   return IMEXLB_OK;
 }
 

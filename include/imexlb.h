@@ -95,7 +95,8 @@ typedef struct imexlb_params {
   double inlet_u;
   double sphere_d;
   double sphere_c[3];
-  void* stream; /* cudaStream_t to run on; NULL = the legacy default stream */
+  void* stream; /* cudaStream_t to run on (it must stay valid until imexlb_destroy
+                  returns); NULL = the legacy default stream */
 } imexlb_params;
 
 typedef struct imexlb_lattice imexlb_lattice;
@@ -152,6 +153,16 @@ enum {
 };
 int imexlb_reduce(imexlb_lattice* h, int kind, double* out);
 
+/* The MASS, KINETIC, UMAX or RESIDUAL reduction (one value) without waiting
+ * for the GPU: the reduction and the copy of its value into `out` are queued
+ * on the lattice's stream, and *out holds the value once the next
+ * synchronising call (imexlb_synchronize, imexlb_get_fields, ...) returns.
+ * `out` should be pinned host memory (with pageable memory the copy waits for
+ * the stream).  A non-finite lattice gives NaN or an infinite value instead
+ * of the IMEXLB_E_STATE that imexlb_reduce returns.  A solve loop can so check
+ * its residual every few steps without stalling the steps behind it. */
+int imexlb_reduce_async(imexlb_lattice* h, int kind, double* out);
+
 /* The MASS, KINETIC and UMAX reductions over caller-provided device fields
  * (u, v, w, p, n values each; a field the reduction does not read may be
  * NULL), writing the result to the device address `out`, asynchronously on
@@ -163,11 +174,17 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out);
  * 32 KiB array inside the library that every GPU using the library holds
  * until exit.  n is limited to 268435456 cells; larger n is rejected with
  * IMEXLB_E_ARG.  The first call on a device looks up that array's device
- * address and must come before any stream capture on that device.  All
- * calls on a device share the array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.
- * Nothing in the array needs to start at zero: each call overwrites every
- * partial it reads. */
+ * address and must come before any stream capture on that device; after a
+ * reset of the device's context (cudaDeviceReset) the next call finds the
+ * new context and looks the address up again, so it too must come before
+ * any capture.  All calls on a device share the array: calls that overlap on
+ * the GPU (other streams, other threads) race and must be serialised by the
+ * caller.  Nothing in the array needs to start at zero: each call overwrites
+ * every partial it reads.  The result is computed on the GPU after the call
+ * returns, so a non-finite field cannot be reported as an error code (as
+ * imexlb_reduce reports IMEXLB_E_STATE): it shows in *out instead, which is
+ * NaN when any value read is NaN (UMAX included) and infinite when one is
+ * infinite. */
 int imexlb_reduce_fields_noalloc(int kind, const double* u, const double* v, const double* w, const double* p,
                                  int64_t n, double* out, void* stream);
 
@@ -218,6 +235,13 @@ int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out);
 int imexlb_synchronize(imexlb_lattice* h);
 
 void imexlb_destroy(imexlb_lattice* h);
+
+/* Lattices take their device memory from a stream-ordered pool per device
+ * that keeps up to 16 GiB of freed memory reserved, so that a lattice created
+ * after another was destroyed maps no new memory and does not wait for the
+ * device.  This returns the reserved memory of the current device to the
+ * system (it waits for the device first).  No counterpart in the reference. */
+int imexlb_release_cached_memory(void);
 
 /* Message of the calling thread's last failure ("" if none). */
 const char* imexlb_last_error(void);

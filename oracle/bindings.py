@@ -243,9 +243,11 @@ class Reference:
 
 
 def run_reference_case(case: str, rho0, R, Re, u0, nx, ny, nz, nsteps, warmup=0, out_every=0,
-                       want_f=True, workdir=None):
-    """Write input.in into a scratch directory and run the reference there."""
-    ref = Reference(case)
+                       want_f=True, workdir=None, fast=False):
+    """Write input.in into a scratch directory and run the reference there
+    (fast: the build without the stand-in's view bounds checks; same
+    arithmetic)."""
+    ref = Reference(case, fast=fast)
     d = workdir or tempfile.mkdtemp(prefix=f"imexlb_ref_{case}_")
     Reference.write_input(d, rho0, R, Re, u0, nsteps, max(out_every, 1), nx, ny, nz)
     res = ref.run(d, nsteps, warmup, out_every, want_f)

@@ -5,6 +5,7 @@ reference's lbm.cpp / System.cpp / mpi_view_transfer.cpp from the reference
 tree against oracle/refshim):
 
     OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --configs [name ...]   # the configuration-size runs
 
 Each fixture records the inputs (the nine input.in numbers, the step count,
 the sphere's `ran` field) and the reference's outputs after that many steps:
@@ -13,6 +14,17 @@ f (population fastest, exactly as the reference stores it) and of the solid
 mask.  The three input.in files the reference ships are recorded with the
 parameters System derives from them, and one Tecplot file written by the
 reference's MPIoutput is recorded by digest and header bytes.
+
+``--configs`` adds (under the manifest's "configs" key, leaving the rest as
+it is) the reference's results at the benchmark configurations' sizes and
+step counts: the 64^3 Taylor-Green vortex at Re 100 after 1000 steps and the
+128^3 lid-driven cavity at Re 1000 (the reference's own boundary passes)
+after 200 steps.  Those fields are too large to commit, so each is recorded
+by the SHA-256 of its FP64 bytes ((nz, ny, nx), x fastest) with a few
+summary values; a bit-exact run must reproduce the digests.
+
+The reference tree comes from oracle.refpath.reference_root() (the
+IMEXLB_REFERENCE environment variable, else BASELINE.json's reference_path).
 """
 from __future__ import annotations
 
@@ -27,6 +39,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 from oracle.bindings import Reference, run_reference_case  # noqa: E402
+from oracle.refpath import reference_root  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -51,7 +64,64 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def main(refroot: str = "/root/reference"):
+# configuration-size runs: (name, case, rho0, R, Re, u0, n, steps)
+# (the reference's own cavity boundary passes make the 128^3 cavity at Re
+# 1000 overflow after about 70 steps: the 50-step entry is before that, the
+# 200-step one records the overflowed state)
+CONFIGS = [
+    ("tgv_64_re100_s1000", "tgv", 1.0, 0.1, 100, 0.05, 64, 1000),
+    ("cavity_128_re1000_s50", "cavity", 1.0, 128.0, 1000, 0.1, 128, 50),
+    ("cavity_128_re1000_s200", "cavity", 1.0, 128.0, 1000, 0.1, 128, 200),
+]
+
+
+def canonical_nan(a: np.ndarray) -> np.ndarray:
+    """FP64 copy with every NaN replaced by one bit pattern (NaN payloads
+    differ between processors; which values are NaN does not)."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    a[np.isnan(a)] = np.float64("nan")
+    return np.ascontiguousarray(a)
+
+
+def field_summary(fields: dict) -> dict:
+    """Digests (NaNs canonical) and summary values of the u, v, w, p fields
+    ((nz, ny, nx))."""
+    out = {f"{k}_sha256": sha(canonical_nan(fields[k])) for k in "uvwp"}
+    u, v, w, p = (np.asarray(fields[k], dtype=np.float64) for k in "uvwp")
+    finite = bool(all(np.isfinite(a).all() for a in (u, v, w, p)))
+    out["finite"] = finite
+    out["nonfinite_values"] = {k: int((~np.isfinite(np.asarray(fields[k]))).sum()) for k in "uvwp"}
+    if finite:
+        out["kinetic"] = float(0.5 * (u * u + v * v + w * w).sum())
+        out["mass"] = float((3.0 * p).sum())
+        out["umax"] = float(np.sqrt(u * u + v * v + w * w).max())
+        out["max_abs"] = {k: float(np.abs(fields[k]).max()) for k in "uvwp"}
+    return out
+
+
+def configs(names=None):
+    path = os.path.join(OUT, "manifest.json")
+    with open(path) as fh:
+        manifest = json.load(fh)
+    entries = dict(manifest.get("configs", {}))
+    for name, case, rho0, R, Re, u0, n, steps in CONFIGS:
+        if names and name not in names:
+            continue
+        r = run_reference_case(case, rho0, R, Re, u0, n, n, n, steps, warmup=0, want_f=False, fast=True)
+        s = r["system"]
+        entries[name] = dict(case=case, rho0=rho0, R=R, Re=Re, u0=u0, nx=n, ny=n, nz=n, steps=steps,
+                             tau=s["tau"], **field_summary(r))
+        print(name, "ok", entries[name].get("kinetic"), entries[name]["nonfinite_values"])
+    manifest["configs"] = entries
+    with open(path, "w") as fh:
+        json.dump(manifest, fh, indent=1, sort_keys=True)
+    print("wrote", path)
+
+
+def main(refroot: str | None = None):
+    refroot = refroot or reference_root()
+    if not refroot:
+        raise SystemExit("reference tree not found: set IMEXLB_REFERENCE")
     manifest = {}
     for name, case, rho0, R, Re, u0, nx, ny, nz, steps in CASES:
         r = run_reference_case(case, rho0, R, Re, u0, nx, ny, nz, steps, warmup=20)
@@ -94,4 +164,7 @@ def main(refroot: str = "/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if "--configs" in sys.argv[1:]:
+        configs([a for a in sys.argv[1:] if not a.startswith("--")] or None)
+    else:
+        main(*sys.argv[1:])

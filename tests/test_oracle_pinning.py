@@ -99,3 +99,24 @@ def test_oracle_matches_reference_live(case, rho0, R, Re, u0, nx, ny, nz, steps)
         assert np.array_equal(got, r[name_]), name_
     assert np.array_equal(o.f_padded(), r["f"])
     assert np.array_equal(o.usr_padded(), r["usr"])
+
+
+def _sha_nan(a):
+    """SHA-256 of FP64 bytes with every NaN in one bit pattern (as
+    tests/golden/make_golden.py --configs records them)."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    a[np.isnan(a)] = np.float64("nan")
+    return _sha(a)
+
+
+@pytest.mark.parametrize("name", ["tgv_64_re100_s1000", "cavity_128_re1000_s50", "cavity_128_re1000_s200"])
+def test_oracle_reproduces_reference_at_config_size(golden_dir, name):
+    """The restatement at the benchmark configurations' sizes and step counts
+    reproduces the reference's digests (including the reference cavity's
+    overflow after about 70 steps at Re 1000)."""
+    m = _manifest(golden_dir)["configs"][name]
+    o = Oracle(m["case"], m["nx"], m["ny"], m["nz"], m["tau"], m["rho0"], m["u0"])
+    o.initialize()
+    o.step(m["steps"])
+    for k, got in zip("uvwp", o.moments()):
+        assert _sha_nan(got) == m[f"{k}_sha256"], f"{name}: field {k}"

@@ -73,3 +73,43 @@ def test_noalloc_refuses_sizes_beyond_capacity(env):
     rc = _noalloc(api, torch, "mass", fields, MAX_CELLS + 1, out, torch.cuda.current_stream().cuda_stream)
     assert rc == 1  # IMEXLB_E_ARG, before any work is queued
     assert b"capacity" in api.load_library().imexlb_last_error()
+
+
+@pytest.mark.parametrize("n", [20_000_003, MAX_CELLS])
+def test_noalloc_mass_many_partials(env, n):
+    """More partial sums than the final pass has threads (n / 65536 > 256),
+    a last chunk shorter than the others, and the capacity itself (accepted):
+    the sum of 3p matches torch's FP64 sum under the same relative bound."""
+    torch, api = env
+    g = torch.Generator(device="cuda").manual_seed(5)
+    p = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) - 0.25
+    want = float((3.0 * p).sum().item())
+    scale = float((3.0 * p).abs().sum().item())
+    out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(2):
+        out.fill_(float("nan"))
+        rc = _noalloc(api, torch, "mass", [p, p, p, p], n, out, stream)
+        assert rc == 0, api.load_library().imexlb_last_error().decode()
+        torch.cuda.synchronize()
+        assert abs(out.item() - want) <= TOL * scale, (n, call, out.item(), want)
+    del p
+    torch.cuda.empty_cache()
+
+
+def test_noalloc_umax_reports_nan(env):
+    """A NaN in a field shows as a NaN maximum (the asynchronous call cannot
+    return an error code for it, as imexlb_reduce does)."""
+    torch, api = env
+    n = 100_000
+    u = torch.linspace(0.0, 0.1, n, dtype=torch.float64, device="cuda")
+    z = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert _noalloc(api, torch, "umax", [u, z, z, z], n, out, stream) == 0
+    torch.cuda.synchronize()
+    assert out.item() == pytest.approx(0.1, rel=1e-15)
+    u[77_777] = float("nan")
+    assert _noalloc(api, torch, "umax", [u, z, z, z], n, out, stream) == 0
+    torch.cuda.synchronize()
+    assert np.isnan(out.item())
