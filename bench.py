@@ -91,8 +91,11 @@ WORKLOADS = {
                           u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
     # batched solves: 256 seeded TGV / cavity instances (imexlb_b200.batch) in
     # one engine; case/n/R/Re/u0 name the instance the CPU baseline times
+    # FP16 storage, FP32 for the instances with tau - 1/2 < 0.015 (imexlb_b200.batch)
     "batched256-f16": dict(kind="batch", storage="f16", arith="fast", count=256, case="cavity", bc="standard",
                            n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
+    "batched256-f16-all": dict(kind="batch", storage="f16-all", arith="fast", count=256, case="cavity",
+                               bc="standard", n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
     "batched256-bf16": dict(kind="batch", storage="bf16", arith="fast", count=256, case="cavity", bc="standard",
                             n=(64, 64, 64), Re=400, u0=0.05, R=64.0, lid_u=0.05),
     "batched256-f32": dict(kind="batch", storage="f32", arith="fast", count=256, case="cavity", bc="standard",
@@ -118,7 +121,7 @@ def tau_of(w) -> float:
 
 def dtype_of(w) -> str:
     return {"f64": "f64", "f32": "f32 (fp32 collide)", "f16": "f16 storage / fp32 collide",
-            "bf16": "bf16 storage / fp32 collide"}[w["storage"]]
+            "f16-all": "f16 storage / fp32 collide", "bf16": "bf16 storage / fp32 collide"}[w["storage"]]
 
 
 def load_peaks() -> dict:
@@ -281,13 +284,15 @@ def measure_batch(storage: str, arith: str, steps: int, warmup: int, tune_cache=
 
     specs = batch.batch_specs(count)
     cells = batch.total_cells(specs)
-    tiles = tune.tiles_for(specs, storage, cache=tune_cache)
+    plan = batch.storage_plan(specs, storage)
+    tiles = batch.tiles_for(specs, storage, cache=tune_cache)
     stream = torch.cuda.Stream()
     budget = batch.budget_for(specs, storage)
+    est = batch.engine_storage(storage)
     with torch.cuda.stream(stream):
-        eng = api.Engine(storage=storage, arith=arith, budget_bytes=budget, max_instances=len(specs),
+        eng = api.Engine(storage=est, arith=arith, budget_bytes=budget, max_instances=len(specs),
                          stream=stream.cuda_stream)
-        slots = batch.add_all(eng, specs, tiles)
+        slots = batch.add_all(eng, specs, tiles, storage)
         eng.step(warmup)
         torch.cuda.synchronize()
         sampler = ClockSampler(torch.cuda.current_device())
@@ -316,9 +321,9 @@ def measure_batch(storage: str, arith: str, steps: int, warmup: int, tune_cache=
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
-        eng = api.Engine(storage=storage, arith=arith, budget_bytes=budget, max_instances=len(specs),
+        eng = api.Engine(storage=est, arith=arith, budget_bytes=budget, max_instances=len(specs),
                          stream=stream.cuda_stream)
-        slots = batch.add_all(eng, specs, tiles)
+        slots = batch.add_all(eng, specs, tiles, storage)
         eng.step(steps)
         for sl, sp in zip(slots, specs):
             eng.fields(sl, out=pinned[(sp.edge,) * 3])
@@ -334,18 +339,23 @@ def measure_batch(storage: str, arith: str, steps: int, warmup: int, tune_cache=
         errs = batch.error_report(specs, fields, ref["fields"])
 
     peaks = load_peaks()
-    bpv = api.BYTES_PER_VALUE[storage]
+    # algorithmic bytes of one step: 27 loads + 27 stores per cell in each
+    # instance's own format
+    step_bytes = sum(2 * 27 * api.BYTES_PER_VALUE[st] * sp.cells for sp, st in zip(specs, plan))
     step_ms = ms / steps
-    achieved = 2 * 27 * bpv * cells / (step_ms * 1e-3) / 1e9
-    groups = len({(sp.case, tiles.get(tune.key_of(storage, sp.case, (sp.edge,) * 3), 0) == 0) for sp in specs})
+    achieved = step_bytes / (step_ms * 1e-3) / 1e9
+    groups = len({(st, sp.case, tiles.get(tune.key_of(st, sp.case, (sp.edge,) * 3), 0) == 0)
+                  for sp, st in zip(specs, plan)})
+    storage_cells = {st: sum(sp.cells for sp, x in zip(specs, plan) if x == st) for st in sorted(set(plan))}
     return {
         "value": value, "unit": "MLUPS", "ms_per_step": step_ms, "steps": steps, "warmup": warmup,
         "instances": len(specs), "cells": cells, "storage": storage, "seed": batch.BATCH_SEED,
+        "storage_instances": {st: plan.count(st) for st in sorted(set(plan))}, "storage_cells": storage_cells,
         "roofline": {"bound": "hbm", "kernel": "engine step launches (all kernel groups of one step)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
                      "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
-                     "bytes_per_cell_update": 2 * 27 * bpv},
+                     "bytes_per_cell_update": step_bytes / cells},
         "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * tgv_cells / steps,
                 "d2h_bytes_per_step": 4 * 8 * cells / steps, "seconds": e2e_s},
         "gpu_launches": steps * groups, "clocks": clocks, "engine_tiles": stats["tiles"],
@@ -359,13 +369,16 @@ def bench_batch(args, w, name, cpu) -> int:
 
     r = measure_batch(w["storage"], w["arith"], args.steps, args.warmup, args.tune_cache, args.check_error,
                       w["count"])
-    cells, bpv = r["cells"], 2 if w["storage"] in ("f16", "bf16") else (4 if w["storage"] == "f32" else 8)
+    cells, bpv = r["cells"], r["roofline"]["bytes_per_cell_update"] / 54
     line = {
         "metric": "D3Q27 MLUPS (aggregate over the batch)", "value": r["value"], "unit": "MLUPS", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
         "data": "synthetic: 256 seeded instances (analytic initial and boundary conditions)",
         "config": {"workload": name, "instances": r["instances"], "cells": cells, "storage": w["storage"],
+                   "storage_instances": r["storage_instances"],
+                   "storage_policy": ("FP16 where tau - 1/2 >= 0.015, FP32 below (imexlb_b200.batch)"
+                                      if w["storage"] == "f16" else "every instance in the one format"),
                    "mix": "TGV / lid-driven cavity 50/50, edge in {24..128}, Re log-uniform [50, 1000], U0 = 0.05",
                    "seed": batch.BATCH_SEED, "tiles": "autotuned per (edge, case, storage)",
                    "parallelism": "single GPU, one engine",
@@ -499,7 +512,7 @@ def main(argv=None) -> int:
     checks = 10
     chunk = max(1, args.steps // checks)
     pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for k in "uvwp"}
-    resid = torch.empty(checks + 1, dtype=torch.float64, pin_memory=True).numpy()
+    res_host = torch.empty(checks + 1, dtype=torch.float64, pin_memory=True).numpy()
     barrier()
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
@@ -510,7 +523,7 @@ def main(argv=None) -> int:
             s = min(chunk, args.steps - done)
             lbm2.step(s)
             done += s
-            lbm2.reduce_async("residual", resid, min(nres, checks))
+            lbm2.reduce_async("residual", res_host, min(nres, checks))
             nres += 1
         lbm2.fields(out=pinned, wait=False)
         lbm2.synchronize()  # every residual and the fields are in host memory
@@ -562,7 +575,7 @@ def main(argv=None) -> int:
                     "inputs": ("the case parameters: the cavity starts at rest (f = 0) and its initial state "
                                "is built on the device, as the reference's Initialize builds it"
                                if h2d == 0 else "initial fields and masks uploaded at create"),
-                    "final_residual": float(resid[min(nres, checks) - 1]) if nres else None},
+                    "final_residual": float(res_host[min(nres, checks) - 1]) if nres else None},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": ({"value": cpu["value"], "unit": "MLUPS", "cores": cpu["cores"], "kind": cpu["kind"],

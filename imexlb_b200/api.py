@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libimexlb.so")
 
 CASES = {"tgv": 0, "cavity": 1, "sphere": 2}
-BCS = {"reference": 0, "standard": 1}
+BCS = {"reference": 0, "standard": 1, "slab": 2}
 STORAGES = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 ARITHS = {"exact": 0, "fast": 1}
 REDUCE = {"mass": 0, "kinetic": 1, "residual": 2, "drag": 3, "umax": 4}
@@ -80,7 +80,7 @@ EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imex
            "imexlb_reduce_async", "imexlb_reduce_fields_noalloc", "imexlb_release_cached_memory", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
            "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
-           "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_remove",
+           "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_add_as", "imexlb_engine_remove",
            "imexlb_engine_step", "imexlb_engine_limit", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
            "imexlb_engine_instance_bytes", "imexlb_engine_checkpoint_size", "imexlb_engine_checkpoint_save",
            "imexlb_engine_restore", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
@@ -130,6 +130,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_version.restype = ctypes.c_char_p
     lib.imexlb_engine_create.argtypes = [i, i, ctypes.c_size_t, i, vp, ctypes.POINTER(vp)]
     lib.imexlb_engine_add.argtypes = [vp, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_int)]
+    lib.imexlb_engine_add_as.argtypes = [vp, ctypes.POINTER(InstanceDesc), i, ctypes.POINTER(ctypes.c_int)]
     lib.imexlb_engine_remove.argtypes = [vp, i]
     lib.imexlb_engine_step.argtypes = [vp, i]
     lib.imexlb_engine_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -348,17 +349,20 @@ class Engine:
     def __exit__(self, *exc):
         self.close()
 
-    def add(self, desc: InstanceDesc) -> int:
-        """Admit an instance; raises ImexlbError (code 4) when over budget."""
+    def add(self, desc: InstanceDesc, storage: str | None = None) -> int:
+        """Admit an instance (in the engine's storage format, or in `storage`);
+        raises ImexlbError (code 4) when over budget."""
         slot = ctypes.c_int()
-        _check(self.lib.imexlb_engine_add(self.h, ctypes.byref(desc), ctypes.byref(slot)))
+        st = STORAGES[storage or self.storage]
+        _check(self.lib.imexlb_engine_add_as(self.h, ctypes.byref(desc), st, ctypes.byref(slot)))
         self.shapes[slot.value] = (desc.nx, desc.ny, desc.nz)
         return slot.value
 
-    def try_add(self, desc: InstanceDesc):
+    def try_add(self, desc: InstanceDesc, storage: str | None = None):
         """Admit an instance, or return None if it does not fit now."""
         slot = ctypes.c_int()
-        rc = self.lib.imexlb_engine_add(self.h, ctypes.byref(desc), ctypes.byref(slot))
+        st = STORAGES[storage or self.storage]
+        rc = self.lib.imexlb_engine_add_as(self.h, ctypes.byref(desc), st, ctypes.byref(slot))
         if rc == 4:
             return None
         _check(rc)

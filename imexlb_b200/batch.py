@@ -15,6 +15,21 @@ All instances live in one engine (imexlb_engine_*) and advance one time step
 per persistent launch per kernel group, two steps per CUDA-graph replay,
 with per-instance tile shapes from the autotuner (imexlb_b200.tune).
 
+Storage policy of the FP16 form: FP16 storage rounds every population to 11
+significant bits each step, and a flow whose relaxation time is close to
+1/2 (little viscosity, tau0 = tau - 1/2 = 3 nu small) damps that rounding
+noise too slowly: on this batch after 2000 steps every instance with
+tau0 >= 0.0109 stayed within 1e-3 relative velocity L2 of its FP64 run in
+FP16, and 65 of the 85 below did not (up to 6.6e-2 at tau0 = 1.3e-3), while
+FP32 storage stayed within 2.4e-4 everywhere.  Just above 0.011 the small
+vortices still reach 8e-4; from tau0 = 0.015 on the largest FP16 error was
+5.7e-4.  So the FP16 form stores an instance in FP16 when
+tau0 >= FP16_MIN_TAU0 (0.015) and in FP32 otherwise (storage_plan;
+"f16-all" stores every instance in FP16): three quarters of the batch's
+cells stay in FP16.  Instances whose
+lattice goes non-finite (BGK beyond its stability limit) are retired with
+the status "diverged" and have no fields.
+
     python -m imexlb_b200.batch --storage f16 --steps 2000 [--check]
 """
 from __future__ import annotations
@@ -32,6 +47,7 @@ from . import api
 BATCH_SEED = 20240607
 EDGES = (24, 32, 48, 64, 96, 128)
 PI_REF = 3.1415926
+FP16_MIN_TAU0 = 0.015  # below this tau - 1/2 the FP16 form stores an instance in FP32
 
 
 @dataclasses.dataclass(frozen=True)
@@ -73,9 +89,36 @@ def total_cells(specs) -> int:
     return sum(s.cells for s in specs)
 
 
+def storage_plan(specs, storage: str) -> list[str]:
+    """Per-instance storage format of a batch run in `storage`: "f16" stores
+    the instances with tau0 < FP16_MIN_TAU0 in FP32 (module docstring),
+    "f16-all" every instance in FP16, any other format every instance in it."""
+    if storage == "f16":
+        return ["f16" if s.tau0 >= FP16_MIN_TAU0 else "f32" for s in specs]
+    if storage == "f16-all":
+        return ["f16"] * len(specs)
+    return [storage] * len(specs)
+
+
+def engine_storage(storage: str) -> str:
+    """The engine's own format for a batch storage name."""
+    return "f16" if storage == "f16-all" else storage
+
+
 def budget_for(specs, storage: str, slack: float = 1.05) -> int:
-    need = sum(api.instance_bytes(storage, s.desc()) for s in specs)
+    need = sum(api.instance_bytes(st, s.desc()) for s, st in zip(specs, storage_plan(specs, storage)))
     return int(need * slack) + (64 << 20)
+
+
+def tiles_for(specs, storage: str, cache: str | None = None) -> dict:
+    """Autotuned tile widths for every (format, shape) the batch's storage plan uses."""
+    from . import tune
+
+    plan = storage_plan(specs, storage)
+    tiles = {}
+    for st in sorted(set(plan)):
+        tiles.update(tune.tiles_for([s for s, x in zip(specs, plan) if x == st], st, cache=cache))
+    return tiles
 
 
 def velocity_l2(got: dict, want: dict) -> float:
@@ -85,27 +128,46 @@ def velocity_l2(got: dict, want: dict) -> float:
     return math.sqrt(num / den) if den > 0 else math.sqrt(num)
 
 
-def add_all(eng: api.Engine, specs, tiles: dict | None = None) -> list[int]:
-    """Admit every instance; `tiles` maps tune keys to tile_bx."""
+def add_all(eng: api.Engine, specs, tiles: dict | None = None, storage: str | None = None) -> list[int]:
+    """Admit every instance in the format the storage plan gives it (the
+    engine's own format when `storage` is None); `tiles` maps tune keys to
+    tile_bx."""
     from . import tune
 
+    plan = storage_plan(specs, storage or eng.storage)
     slots = []
-    for s in specs:
-        bx = tiles.get(tune.key_of(eng.storage, s.case, (s.edge,) * 3), 0) if tiles else 0
-        slots.append(eng.add(s.desc(tile_bx=bx)))
+    for s, st in zip(specs, plan):
+        bx = tiles.get(tune.key_of(st, s.case, (s.edge,) * 3), 0) if tiles else 0
+        slots.append(eng.add(s.desc(tile_bx=bx), storage=st))
     return slots
+
+
+def retire_diverged(eng: api.Engine, slots: list[int]) -> list[str]:
+    """Status per instance after a run: "ok", or "diverged" (its velocity
+    field is not finite; the instance is removed from the engine)."""
+    res = eng.residuals()
+    status = []
+    for sl in slots:
+        if np.isnan(res[sl]):
+            eng.remove(sl)
+            status.append("diverged")
+        else:
+            status.append("ok")
+    return status
 
 
 def run(specs, storage: str, steps: int, arith: str = "fast", tiles: dict | None = None, fields: bool = True,
         warmup: int = 0) -> dict:
     """Advance the whole batch `steps` steps; device-timed MLUPS and, when
-    asked, every instance's u, v, w, p afterwards."""
+    asked, every instance's status and its u, v, w, p afterwards (None for
+    a diverged instance, which is retired)."""
     import torch
 
     stream = torch.cuda.Stream()
-    with api.Engine(storage=storage, arith=arith, budget_bytes=budget_for(specs, storage),
+    plan = storage_plan(specs, storage)
+    with api.Engine(storage=engine_storage(storage), arith=arith, budget_bytes=budget_for(specs, storage),
                     max_instances=len(specs), stream=stream.cuda_stream) as eng:
-        slots = add_all(eng, specs, tiles)
+        slots = add_all(eng, specs, tiles, storage)
         if warmup:
             eng.step(warmup)
         torch.cuda.synchronize()
@@ -115,24 +177,27 @@ def run(specs, storage: str, steps: int, arith: str = "fast", tiles: dict | None
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        out = [eng.fields(s) for s in slots] if fields else None
+        status = retire_diverged(eng, slots) if fields else None
+        out = [eng.fields(sl) if st == "ok" else None for sl, st in zip(slots, status)] if fields else None
     cells = total_cells(specs)
-    return dict(mlups=cells * steps / (ms * 1e-3) / 1e6, ms=ms, cells=cells, steps=steps, fields=out)
+    return dict(mlups=cells * steps / (ms * 1e-3) / 1e6, ms=ms, cells=cells, steps=steps, fields=out,
+                status=status, plan=plan)
 
 
 def errors_against(fields, ref_fields) -> list[float]:
     return [velocity_l2(g, w) for g, w in zip(fields, ref_fields)]
 
 
-def finite(f: dict) -> bool:
-    return all(bool(np.isfinite(f[k]).all()) for k in "uvw")
+def finite(f: dict | None) -> bool:
+    return f is not None and all(bool(np.isfinite(f[k]).all()) for k in "uvw")
 
 
-def error_report(specs, fields, ref_fields, worst: int = 5) -> dict:
+def error_report(specs, fields, ref_fields, worst: int = 5, plan=None) -> dict:
     """Per-instance relative velocity L2 against the FP64 run.  Instances
     whose FP64 run itself diverged (BGK past its stability limit: the batch
-    draws Re up to 1000 on edges down to 24, tau - 1/2 down to 7e-4) have no
-    reference and are counted apart."""
+    draws Re up to 1000 on edges down to 24, tau - 1/2 down to 7e-4; the
+    run retires them with the status "diverged") have no reference and are
+    counted apart."""
     errs, bad_ref, bad_run = [], [], []
     for i, (s, g, w) in enumerate(zip(specs, fields, ref_fields)):
         if not finite(w):
@@ -148,6 +213,8 @@ def error_report(specs, fields, ref_fields, worst: int = 5) -> dict:
         "compared": len(errs), "fp64_diverged": len(bad_ref), "diverged_only_here": len(bad_run),
         "max": float(vals.max()), "p95": float(np.percentile(vals, 95)), "median": float(np.median(vals)),
         "within_1e-3": int((vals <= 1e-3).sum()),
+        "over_1e-3": int((vals > 1e-3).sum()),
+        "storage_counts": ({st: plan.count(st) for st in sorted(set(plan))} if plan else None),
         "worst": [dict(err=e, case=specs[i].case, edge=specs[i].edge, Re=round(specs[i].Re, 1),
                        tau=round(specs[i].tau0 + 0.5, 6)) for e, i in errs[:worst]],
         "fp64_diverged_instances": [dict(case=specs[i].case, edge=specs[i].edge, Re=round(specs[i].Re, 1))
@@ -155,44 +222,47 @@ def error_report(specs, fields, ref_fields, worst: int = 5) -> dict:
     }
 
 
-def per_instance(specs, fields, ref_fields) -> list[dict]:
-    """One record per instance: its parameters and its relative velocity L2
-    against the FP64 run (None where either run is not finite)."""
+def per_instance(specs, fields, ref_fields, plan=None) -> list[dict]:
+    """One record per instance: its parameters, storage and relative velocity
+    L2 against the FP64 run (None where either run diverged)."""
     out = []
-    for s, g, w in zip(specs, fields, ref_fields):
+    for i, (s, g, w) in enumerate(zip(specs, fields, ref_fields)):
         ok_ref, ok_run = finite(w), finite(g)
         out.append(dict(case=s.case, edge=s.edge, Re=s.Re, tau=s.tau0 + 0.5, fp64_finite=ok_ref, finite=ok_run,
+                        storage=plan[i] if plan else None,
                         err=velocity_l2(g, w) if ok_ref and ok_run else None))
     return out
 
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--storage", default="f16", help="storage format, or several separated by commas")
+    ap.add_argument("--storage", default="f16",
+                    help="storage (f64, f32, f16 = FP16 with FP32 for tau - 1/2 < 0.015, f16-all, bf16), "
+                         "or several separated by commas")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--check", action="store_true", help="also run FP64 and report per-instance errors")
     ap.add_argument("--dump", default=None, help="with --check: write every instance's error to this JSON file")
     ap.add_argument("--tune-cache", default=None)
     args = ap.parse_args(argv)
-    from . import tune
-
     specs = batch_specs(args.count)
     storages = args.storage.split(",")
     for st in storages:
-        if st not in api.STORAGES:
+        if st not in api.STORAGES and st != "f16-all":
             raise SystemExit(f"unknown storage {st}")
     ref = run(specs, "f64", args.steps, fields=True) if args.check else None
     dump = {}
     for st in storages:
-        tiles = tune.tiles_for(specs, st, cache=args.tune_cache)
+        tiles = tiles_for(specs, st, cache=args.tune_cache)
         t0 = time.perf_counter()
         res = run(specs, st, args.steps, tiles=tiles, fields=args.check)
         line = dict(storage=st, instances=len(specs), cells=res["cells"], steps=args.steps,
                     mlups=res["mlups"], device_ms=res["ms"], wall_s=time.perf_counter() - t0)
         if args.check:
-            line.update(fp64_mlups=ref["mlups"], errors=error_report(specs, res["fields"], ref["fields"]))
-            dump[st] = per_instance(specs, res["fields"], ref["fields"])
+            line.update(fp64_mlups=ref["mlups"],
+                        errors=error_report(specs, res["fields"], ref["fields"], plan=res["plan"]),
+                        diverged=res["status"].count("diverged"), fp64_diverged=ref["status"].count("diverged"))
+            dump[st] = per_instance(specs, res["fields"], ref["fields"], res["plan"])
         print(json.dumps(line), flush=True)
     if args.dump and dump:
         with open(args.dump, "w") as fh:

@@ -463,6 +463,7 @@ class Arena {
 
 struct Slot {
   bool used = false;
+  imexlb_storage storage = IMEXLB_F64;  // the instance's own storage format
   imexlb_instance_desc d{};
   Layout L;
   size_t off = 0, bytes = 0;
@@ -558,12 +559,15 @@ struct imexlb_engine {
   DevBuf<int> d_seg;  // begin[nseg], end[nseg]
   DevBuf<double> d_res;
   std::vector<int> seg_slots;
-  // tile ranges of the kernel groups: group = rule (0 periodic, 1 cavity,
-  // 2 sphere) * 3 + mode (0 one cell or y-pairs, 1 x-pairs, 2 staged rows)
-  int group_begin[9] = {};
-  int group_end[9] = {};
+  // tile ranges of the kernel groups: group = storage format * 9 + rule (0
+  // periodic, 1 cavity, 2 sphere) * 3 + mode (0 one cell or y-pairs, 1
+  // x-pairs, 2 staged rows)
+  static constexpr int GROUPS = 4 * 9;
+  int group_begin[GROUPS] = {};
+  int group_end[GROUPS] = {};
   DevBuf<int> d_err;  // staged kernels' error word
   int staged_resident = 0;  // staged blocks resident on the device
+  bool staged_ready[4] = {};  // staged kernels' shared memory set for this format
   bool dirty = true;
   int64_t gstep = 0;
   int grid = 296;
@@ -603,10 +607,10 @@ int sync_checked(imexlb_engine* e) {
 }
 
 int mode_of(const EngInst& in) { return in.staged ? 2 : (in.x2 ? 1 : 0); }
-int group_of(const EngInst& in) {
+int group_of(const Slot& sl, const EngInst& in) {
   const int rule = in.rule;
   const int rg = rule == static_cast<int>(CaseRule::None) ? 0 : (rule == static_cast<int>(CaseRule::CavityStd) ? 1 : 2);
-  return rg * 3 + mode_of(in);
+  return static_cast<int>(sl.storage) * 9 + rg * 3 + mode_of(in);
 }
 
 int rebuild_tiles(imexlb_engine* e) {
@@ -616,15 +620,15 @@ int rebuild_tiles(imexlb_engine* e) {
   std::vector<int> sb, se;
   // instances ordered by kernel group, so that each group's tiles are one range
   std::vector<int> order;
-  for (int g = 0; g < 9; ++g)
+  for (int g = 0; g < imexlb_engine::GROUPS; ++g)
     for (int s = 0; s < static_cast<int>(e->slots.size()); ++s)
-      if (e->slots[s].used && group_of(e->h_inst[s]) == g) order.push_back(s);
-  for (int g = 0; g < 9; ++g) e->group_begin[g] = e->group_end[g] = 0;
+      if (e->slots[s].used && group_of(e->slots[s], e->h_inst[s]) == g) order.push_back(s);
+  for (int g = 0; g < imexlb_engine::GROUPS; ++g) e->group_begin[g] = e->group_end[g] = 0;
   int prev_group = -1;
   for (int s : order) {
     Slot& sl = e->slots[s];
     const EngInst& in = e->h_inst[s];
-    const int g = group_of(in);
+    const int g = group_of(sl, in);
     if (g != prev_group) {
       e->group_begin[g] = static_cast<int>(e->h_tiles.size());
       prev_group = g;
@@ -701,10 +705,11 @@ void set_staged_smem() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
+// The kernel groups of the instances stored in format S.
 template <Store S, bool EXACT>
 cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
   for (int g = 0; g < 9; ++g) {
-    const int t0 = e->group_begin[g], t1 = e->group_end[g];
+    const int t0 = e->group_begin[static_cast<int>(S) * 9 + g], t1 = e->group_end[static_cast<int>(S) * 9 + g];
     if (t1 <= t0) continue;
     const int rule = g / 3, mode = g % 3;
     if constexpr (S == Store::F16 || S == Store::BF16) {
@@ -747,15 +752,19 @@ cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
   EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, e->d_left.p, static_cast<int>(e->h_tiles.size()), parity,
               store, e->d_err.p};
   if (ea.ntiles == 0) return cudaSuccess;
-  cudaError_t err = cudaErrorInvalidValue;
-  switch (e->storage) {
-    case IMEXLB_F64:
-      err = e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
-      break;
-    case IMEXLB_F32: err = launch_groups<Store::F32, false>(e, ea); break;
-    case IMEXLB_F16: err = launch_groups<Store::F16, false>(e, ea); break;
-    case IMEXLB_BF16: err = launch_groups<Store::BF16, false>(e, ea); break;
-  }
+  // one pass per storage format present (instances of several formats share
+  // the engine and its step graph)
+  auto present = [&](int st) {
+    for (int g = 0; g < 9; ++g)
+      if (e->group_end[st * 9 + g] > e->group_begin[st * 9 + g]) return true;
+    return false;
+  };
+  cudaError_t err = cudaSuccess;
+  if (present(IMEXLB_F64))
+    err = e->exact ? launch_groups<Store::F64, true>(e, ea) : launch_groups<Store::F64, false>(e, ea);
+  if (err == cudaSuccess && present(IMEXLB_F32)) err = launch_groups<Store::F32, false>(e, ea);
+  if (err == cudaSuccess && present(IMEXLB_F16)) err = launch_groups<Store::F16, false>(e, ea);
+  if (err == cudaSuccess && present(IMEXLB_BF16)) err = launch_groups<Store::BF16, false>(e, ea);
   if (err != cudaSuccess) return err;
   const int n = static_cast<int>(e->h_left.size());
   engine_tick<<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_left.p, n);
@@ -763,6 +772,31 @@ cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
 }
 
 }  // namespace
+
+// The staged kernels of a 2-byte format: their shared memory is set, and
+// their resident blocks counted, once per engine and format (outside any
+// stream capture: at creation or at the first admission in the format).
+static int prepare_storage(imexlb_engine* e, imexlb_storage storage) {
+  if ((storage != IMEXLB_F16 && storage != IMEXLB_BF16) || e->staged_ready[storage]) return IMEXLB_OK;
+  int dev = 0, sms = 148, per_sm = 0;
+  IMX_ECUDA(cudaGetDevice(&dev));
+  IMX_ECUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (storage == IMEXLB_F16) {
+    set_staged_smem<Store::F16>();
+    IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, engine_staged_kernel<Store::F16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
+        engine_staged_smem(true)));
+  } else {
+    set_staged_smem<Store::BF16>();
+    IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, engine_staged_kernel<Store::BF16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
+        engine_staged_smem(true)));
+  }
+  const int resident = std::max(per_sm, 1) * sms;
+  e->staged_resident = e->staged_resident ? std::min(e->staged_resident, resident) : resident;
+  e->staged_ready[storage] = true;
+  return IMEXLB_OK;
+}
 
 extern "C" {
 
@@ -799,23 +833,7 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
   e->grid = 2 * sms;
   IMX_ECUDA(e->d_err.reserve(1));
   IMX_ECUDA(cudaMemset(e->d_err.p, 0, sizeof(int)));
-  if (storage == IMEXLB_F16 || storage == IMEXLB_BF16) {
-    // the staged kernels' shared memory, set once outside any capture
-    if (storage == IMEXLB_F16)
-      set_staged_smem<Store::F16>();
-    else
-      set_staged_smem<Store::BF16>();
-    int per_sm = 0;
-    if (storage == IMEXLB_F16)
-      IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, engine_staged_kernel<Store::F16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
-          engine_staged_smem(true)));
-    else
-      IMX_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, engine_staged_kernel<Store::BF16, Bc::Standard, CaseRule::CavityStd>, stage::THREADS,
-          engine_staged_smem(true)));
-    e->staged_resident = std::max(per_sm, 1) * sms;
-  }
+  if (const int rc = prepare_storage(e.get(), storage)) return rc;
   *out = e.release();
   return IMEXLB_OK;
 }
@@ -839,7 +857,14 @@ static size_t record_bytes(int storage, const imexlb_instance_desc* d, const Lay
 }
 
 int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot_out) {
+  if (!e) return efail(IMEXLB_E_ARG, "null engine");
+  return imexlb_engine_add_as(e, d, e->storage, slot_out);
+}
+
+int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb_storage storage, int* slot_out) {
   if (!e || !d || !slot_out) return efail(IMEXLB_E_ARG, "null argument");
+  if (storage < IMEXLB_F64 || storage > IMEXLB_BF16) return efail(IMEXLB_E_ARG, "unknown storage");
+  if (const int rc = prepare_storage(e, storage)) return rc;
   if (d->kase != IMEXLB_TGV && d->kase != IMEXLB_CAVITY && d->kase != IMEXLB_SPHERE)
     return efail(IMEXLB_E_ARG, "unknown case");
   if (d->nx < 2 || d->ny < 2 || d->nz < 2 || d->nz > 65535) return efail(IMEXLB_E_ARG, "bad extents");
@@ -851,8 +876,9 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
       break;
     }
   if (s < 0) return efail(IMEXLB_E_NOMEM, "no free instance slot");
-  const int elem = e->storage == IMEXLB_F64 ? 8 : (e->storage == IMEXLB_F32 ? 4 : 2);
+  const int elem = storage == IMEXLB_F64 ? 8 : (storage == IMEXLB_F32 ? 4 : 2);
   Slot sl;
+  sl.storage = storage;
   sl.d = *d;
   sl.L = make_layout(d->nx, d->ny, d->nz, 0, elem);
   if (static_cast<double>(sl.L.sq) * Q >= 2147483647.0) return efail(IMEXLB_E_ARG, "instance too large for the engine");
@@ -862,7 +888,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   const size_t pbytes = ((3 * sl.ncell * 8) + 511) & ~static_cast<size_t>(511);
   const size_t mask_bytes = static_cast<size_t>((sl.ncell + 255) & ~int64_t(255));
   const size_t sbytes = d->kase == IMEXLB_SPHERE ? ((mask_bytes + 4 * sl.ncell + 511) & ~static_cast<size_t>(511)) : 0;
-  const size_t rbytes = record_bytes(e->storage, d, sl.L);
+  const size_t rbytes = record_bytes(storage, d, sl.L);
   sl.bytes = 2 * fbytes + mbytes + pbytes + sbytes + 2 * rbytes;
   if (!e->arena.alloc(sl.bytes, &sl.off))
     return efail(IMEXLB_E_NOMEM, "instance does not fit the engine's memory budget");
@@ -881,7 +907,7 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   imexlb_params_default(&P);
   P.kase = d->kase;
   P.bc = d->kase == IMEXLB_TGV ? IMEXLB_BC_REFERENCE : IMEXLB_BC_STANDARD;
-  P.storage = e->storage;
+  P.storage = storage;
   P.nx = d->nx;
   P.ny = d->ny;
   P.nz = d->nz;
@@ -951,13 +977,13 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   a.rho_w = P.rho0;
   a.inlet_u = P.inlet_u;
   const double p_rest = d->kase == IMEXLB_TGV ? d->rho0 / 3.0 : 0.0;
-  a.p_shift = e->storage == IMEXLB_F64 ? 0.0 : p_rest;
+  a.p_shift = storage == IMEXLB_F64 ? 0.0 : p_rest;
   for (int q = 0; q < Q; ++q) {
-    const double sc = store_scale(static_cast<Store>(e->storage), D3Q27::wclass[q]);
+    const double sc = store_scale(static_cast<Store>(storage), D3Q27::wclass[q]);
     a.enc.scale[q] = static_cast<float>(sc);
     a.enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
-  a.enc.unit = store_unit(static_cast<Store>(e->storage));
+  a.enc.unit = store_unit(static_cast<Store>(storage));
   in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {
@@ -978,12 +1004,13 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
     }
     const double ui = P.inlet_u;
     // 2-byte x-pair formats store deviations from the inflow's equilibrium
-    const bool ref_flow = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
+    const bool ref_flow = (storage == IMEXLB_F16 || storage == IMEXLB_BF16) && d->nx % 2 == 0;
     if (ref_flow) set_reference_flow(a.enc, ui, a.omega);
     for (int q = 0; q < Q; ++q) {
       const double t = weight_of_class(D3Q27::wclass[q]);
       const double ev = D3Q27::ex[q] * ui;
-      const double br = 3.0 * ev + 4.5 * ev * ev - 1.5 * ui * ui;
+      // the reference's equilibrium bracket (tgv/src/lbm.cpp:228-232) of (ui, 0, 0): edu = e_x ui, udu = ui ui
+      const double br = 3.0 * ev + 4.5 * (ev * ev) - 1.5 * (ui * ui);
       a.feq_in[q] = t * (3.0 * (0.0 - a.p_shift) + (ref_flow ? 0.0 : br));
     }
   }
@@ -995,20 +1022,20 @@ int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot
   sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
   in.bx_log2 = sl.bx_log2;
   in.parity0 = static_cast<int>(e->gstep & 1);
-  in.x2 = (e->storage == IMEXLB_F16 || e->storage == IMEXLB_BF16) && d->nx % 2 == 0;
+  in.x2 = (storage == IMEXLB_F16 || storage == IMEXLB_BF16) && d->nx % 2 == 0;
   // rows staged in shared memory where they fit a stage (and tile_bx asks
   // for no register-staged tile width)
-  in.staged = instance_staged(e->storage, d, sl.L, &in.geo) ? 1 : 0;
+  in.staged = instance_staged(storage, d, sl.L, &in.geo) ? 1 : 0;
   if (in.staged) {
     in.tw = d->nx;
     in.th = in.geo.R;
   } else {
     const int bx = 1 << sl.bx_log2;
-    in.th = (256 / bx) * cpt_of(e->storage);
+    in.th = (256 / bx) * cpt_of(storage);
     in.tw = bx * (in.x2 ? 2 : 1);
   }
-  LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(e->storage), CaseRule::None,
-                e->exact};
+  LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(storage), CaseRule::None,
+                storage == IMEXLB_F64 && e->exact};
   IMX_ECUDA(launch_init_f(cfg, sl.L, buf0, buf1, mom, mom + n, mom + 2 * n, mom + 3 * n, a.p_shift, a.enc, e->stream));
   if (rec0) {
     IMX_ECUDA(launch_cavity_records(sl.L, buf0, rec0, e->stream));
@@ -1177,7 +1204,7 @@ static CheckpointHeader instance_header(const imexlb_engine* e, const Slot& sl) 
   std::memcpy(c.magic, "IMXLBCK1", 8);
   c.kind = 1;
   c.kase = sl.d.kase;
-  c.storage = e->storage;
+  c.storage = sl.storage;
   c.bc = IMEXLB_BC_STANDARD;
   c.nx = sl.d.nx;
   c.ny = sl.d.ny;
@@ -1225,11 +1252,11 @@ int imexlb_engine_restore(imexlb_engine* e, const imexlb_instance_desc* d, const
   CheckpointHeader c;
   std::memcpy(&c, host, sizeof c);
   if (std::memcmp(c.magic, "IMXLBCK1", 8) != 0 || c.kind != 1) return efail(IMEXLB_E_ARG, "not an engine checkpoint");
-  if (c.kase != d->kase || c.storage != e->storage || c.nx != d->nx || c.ny != d->ny || c.nz != d->nz ||
-      c.tau0 != d->tau0 || c.nbuf != 1 || c.steps < 0)
+  if (c.kase != d->kase || c.storage < IMEXLB_F64 || c.storage > IMEXLB_BF16 || c.nx != d->nx || c.ny != d->ny ||
+      c.nz != d->nz || c.tau0 != d->tau0 || c.nbuf != 1 || c.steps < 0)
     return efail(IMEXLB_E_ARG, "checkpoint belongs to an instance with other parameters");
   int slot = -1;
-  if (const int rc = imexlb_engine_add(e, d, &slot)) return rc;
+  if (const int rc = imexlb_engine_add_as(e, d, static_cast<imexlb_storage>(c.storage), &slot)) return rc;
   Slot& sl = e->slots[slot];
   const CheckpointHeader want = instance_header(e, sl);
   if (c.buf_bytes != want.buf_bytes || c.mom_bytes != want.mom_bytes ||

@@ -688,6 +688,12 @@ static cudaError_t step_rule(const LaunchCfg& c, const StepArgs& a, cudaStream_t
     case CaseRule::SphereRef: return step_impl<S, Bc::Ghost, CaseRule::SphereRef, EXACT>(a, s);
     case CaseRule::CavityStd: return step_impl<S, Bc::Standard, CaseRule::CavityStd, EXACT>(a, s);
     case CaseRule::SphereStd: return step_impl<S, Bc::Standard, CaseRule::SphereStd, EXACT>(a, s);
+    case CaseRule::SlabStd:
+      // FP64 and FP32 storage only (register kernels)
+      if constexpr (S == Store::F64 || S == Store::F32)
+        return step_impl<S, Bc::Standard, CaseRule::SlabStd, EXACT>(a, s);
+      else
+        return cudaErrorNotSupported;
   }
   return cudaErrorInvalidValue;
 }

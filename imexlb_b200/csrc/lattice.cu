@@ -558,7 +558,10 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   *out = nullptr;
   imexlb_params P = *pin;
   if (P.kase < IMEXLB_TGV || P.kase > IMEXLB_SPHERE) return fail(IMEXLB_E_ARG, "unknown case");
-  if (P.bc != IMEXLB_BC_REFERENCE && P.bc != IMEXLB_BC_STANDARD) return fail(IMEXLB_E_ARG, "unknown boundary kind");
+  if (P.bc != IMEXLB_BC_REFERENCE && P.bc != IMEXLB_BC_STANDARD && P.bc != IMEXLB_BC_SLAB)
+    return fail(IMEXLB_E_ARG, "unknown boundary kind");
+  if (P.bc == IMEXLB_BC_SLAB && (P.kase != IMEXLB_CAVITY || (P.storage != IMEXLB_F64 && P.storage != IMEXLB_F32)))
+    return fail(IMEXLB_E_UNSUPPORTED, "the slab boundaries are for the cavity in FP64 or FP32 storage");
   if (P.storage < IMEXLB_F64 || P.storage > IMEXLB_BF16) return fail(IMEXLB_E_ARG, "unknown storage");
   if (P.nx < 2 || P.ny < 2 || P.nz < 2) return fail(IMEXLB_E_ARG, "lattice extents must be >= 2");
   if (P.nz > 65535) return fail(IMEXLB_E_ARG, "nz above 65535");
@@ -568,7 +571,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   const bool ref_sphere = P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE;
   if (ref_sphere && (P.nx - 1) / 8 + (P.nx - 1) / 64.0 + 2 >= std::min(P.ny, P.nz))
     return fail(IMEXLB_E_ARG, "reference sphere (centre (nx-1)/8 on every axis) does not fit in ny, nz");
-  if (P.kase == IMEXLB_CAVITY && P.bc == IMEXLB_BC_STANDARD && P.lid_u == 0.0) P.lid_u = P.u0;
+  if (P.kase == IMEXLB_CAVITY && P.bc != IMEXLB_BC_REFERENCE && P.lid_u == 0.0) P.lid_u = P.u0;
   if (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_STANDARD) {
     if (P.inlet_u == 0.0) P.inlet_u = P.u0;
     if (P.sphere_d == 0.0) P.sphere_d = P.nx / 24.0;
@@ -590,7 +593,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   if (P.kase == IMEXLB_TGV)
     h->cfg.rule = CaseRule::None;
   else if (P.kase == IMEXLB_CAVITY)
-    h->cfg.rule = ghost ? CaseRule::CavityRef : CaseRule::CavityStd;
+    h->cfg.rule = ghost ? CaseRule::CavityRef : (P.bc == IMEXLB_BC_SLAB ? CaseRule::SlabStd : CaseRule::CavityStd);
   else
     h->cfg.rule = ghost ? CaseRule::SphereRef : CaseRule::SphereStd;
   const int elem = P.storage == IMEXLB_F64 ? 8 : (P.storage == IMEXLB_F32 ? 4 : 2);
@@ -710,7 +713,8 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       for (int q = 0; q < Q; ++q) {
         const double t = weight_of_class(D3Q27::wclass[q]);
         const double e = D3Q27::ex[q] * ui;
-        const double br = 3.0 * e + 4.5 * e * e - 1.5 * ui * ui;
+        // the reference's equilibrium bracket (tgv/src/lbm.cpp:228-232) of (ui, 0, 0): edu = e_x ui, udu = ui ui
+        const double br = 3.0 * e + 4.5 * (e * e) - 1.5 * (ui * ui);
         a.feq_in[q] = t * (3.0 * (0.0 - h->p_shift) + (ref_flow ? 0.0 : br));
       }
     }

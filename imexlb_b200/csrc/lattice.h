@@ -31,7 +31,8 @@ enum class CaseRule : int {
   CavityRef = 1,    // lid velocity forced on the top plane (Update)
   SphereRef = 2,    // solid mask times moments, inlet profile, outlet p = 0
   CavityStd = 3,    // moving-lid halfway bounce-back
-  SphereStd = 4     // channel: equilibrium inlet, zero-gradient outlet, solid sphere
+  SphereStd = 4,    // channel: equilibrium inlet, zero-gradient outlet, solid sphere
+  SlabStd = 5       // the cavity's bottom wall and moving lid, x and y periodic (plane Couette)
 };
 
 // Storage layout of one distribution buffer: 27 population planes, each a

@@ -88,8 +88,11 @@ __device__ __forceinline__ double div3_rn(double x) {
 //   q1 is the correctly rounded quotient if x/d lies strictly within half the
 //   smaller neighbouring gap of q1, i.e. |r1| < d * gap_below(q1) / 2.  If q1 is
 //   further than one ulp away, |r1| exceeds that bound, so a wrong q1 is never
-//   accepted; rejected cases (ties, near-ties, zero, tiny quotients) take
+//   accepted; rejected cases (ties, near-ties, tiny quotients) take
 //   __ddiv_rn.  The bound is a power of two times d, so it is exact.
+//   A zero numerator gives q1 = x exactly (IEEE: +-0 / d = +-0 for d > 0);
+//   it is common (a cell at rest has f = feq) and is returned without the
+//   division.
 __device__ __forceinline__ double div_rn(double x, double d, double z) {
   const double q0 = __dmul_rn(x, z);
   const double r0 = __fma_rn(-q0, d, x);
@@ -99,6 +102,7 @@ __device__ __forceinline__ double div_rn(double x, double d, double z) {
   const int e = static_cast<int>((bits >> 52) & 0x7ff);
   const int he = e - 53 - ((bits & 0xFFFFFFFFFFFFFLL) == 0 ? 1 : 0);  // exponent field of gap_below / 2
   if (he > 0 && fabs(r1) < __dmul_rn(d, __longlong_as_double(static_cast<long long>(he) << 52))) return q1;
+  if (x == 0.0) return x;
   return __ddiv_rn(x, d);
 }
 
@@ -299,6 +303,30 @@ __device__ __forceinline__ void load_cell(const StepArgs& a, const P& pl, const 
       if constexpr (exq != 0 && D3Q27::ez[q] < 0) {
         // ((6 rho_w u_w) w_q) e_q rounded on its own, then added (EXACT keeps
         // the multiply and the add apart, as the specification does)
+        using A = Ar<R, EXACT>;
+        if (lid) val = A::add(val, A::mul(A::mul(R(6.0 * a.rho_w * a.lid_u), wgt<R>(cls)), R(exq)));
+      }
+      f[q] = val;
+    });
+  } else if constexpr (RULE == CaseRule::SlabStd) {
+    // x and y periodic; halfway bounce-back through the bottom (z-, at rest)
+    // and the lid (z+, moving: the same term as the cavity's lid)
+    const int im = i == 0 ? a.nx - 1 : i - 1, ip = i == a.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? a.ny - 1 : j - 1, jp = j == a.ny - 1 ? 0 : j + 1;
+    const int32_t ry[3] = {jm * a.pitch32, j * a.pitch32, jp * a.pitch32};
+    const int32_t cx[3] = {im, i, ip};
+    const int32_t rz = a.base32 + k * a.sz32;
+    const bool bottom = k == 0, lid = k == a.nz - 1;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int qb = D3Q27::bb[q];
+      constexpr int exq = D3Q27::ex[q], eyq = D3Q27::ey[q], ezq = D3Q27::ez[q];
+      constexpr int cls = D3Q27::wclass[q];
+      const bool out = (ezq > 0 && bottom) || (ezq < 0 && lid);
+      // the pulled address only where the link stays inside (k - e_z is a plane)
+      const int32_t s_pull = out ? b : rz - ezq * a.sz32 + ry[1 - eyq] + cx[1 - exq];
+      R val = decode<S>(out ? pl.load(qb, b) : pl.load(q, s_pull), q, a.enc);
+      if constexpr (exq != 0 && ezq < 0) {
         using A = Ar<R, EXACT>;
         if (lid) val = A::add(val, A::mul(A::mul(R(6.0 * a.rho_w * a.lid_u), wgt<R>(cls)), R(exq)));
       }

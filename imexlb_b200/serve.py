@@ -21,9 +21,19 @@ falls below a tolerance.  The loop does continuous batching:
   read back to the host (the request's answer) and its memory is freed for
   the next admission.
 
+Storage: with storage "f16" each request is stored in FP16 when its
+tau - 1/2 is at least imexlb_b200.batch.FP16_MIN_TAU0 and in FP32 otherwise
+(the batched form's plan; one engine holds both formats).  A request whose
+lattice goes non-finite is retired with the status "diverged" and no fields.
+
 Latency = answer read back - arrival, on the host clock.  The baseline is
-one-at-a-time plain FP64: each request alone on the GPU, its service time
-measured once, queued in arrival order (a single server).
+one-at-a-time plain FP64 queued in arrival order (a single server): each
+request alone on the GPU in its own engine, with its service time either
+measured whole (small streams) or, for long streams, composed from
+measurements per lattice shape: the fixed cost (admission, set-up, answer
+read-back) and the time per step of that shape alone, times the request's
+own step count.  A sample of the served answers is checked against FP64
+runs of the same requests to the same step counts (relative velocity L2).
 
 The request mix: 40% cavity (edge 32..128 in steps of 16, Re 100..1000),
 40% TGV (edge 32..128, Re 50..800), 20% sphere channel (L x L/4 x L/4,
@@ -43,6 +53,7 @@ import time
 import numpy as np
 
 from . import api
+from .batch import FP16_MIN_TAU0
 
 SERVE_SEED = 7051
 EDGES = (32, 48, 64, 80, 96, 112, 128)
@@ -105,6 +116,14 @@ def request_stream(count: int, rate: float, seed: int = SERVE_SEED, steps=(5000,
     return out
 
 
+def storage_for(req: Request, storage: str) -> str:
+    """A request's storage format: the FP16 form keeps marginally stable
+    requests (tau - 1/2 < FP16_MIN_TAU0) in FP32."""
+    if storage == "f16" and req.tau0 < FP16_MIN_TAU0:
+        return "f32"
+    return storage
+
+
 class Server:
     """Continuous batching of requests into one engine."""
 
@@ -122,16 +141,17 @@ class Server:
     def close(self):
         self.eng.close()
 
-    def _tile(self, req: Request) -> int:
+    def _tile(self, req: Request, storage: str) -> int:
         from . import tune
 
-        return self.tiles.get(tune.key_of(self.storage, req.case, req.n), 0)
+        return self.tiles.get(tune.key_of(storage, req.case, req.n), 0)
 
     def try_admit(self, req: Request) -> bool:
         cells = sum(r.cells for r, _ in self.active.values())
         if self.active and cells + req.cells > self.max_active_cells:
             return False
-        slot = self.eng.try_add(req.desc(self._tile(req)))
+        st = storage_for(req, self.storage)
+        slot = self.eng.try_add(req.desc(self._tile(req, st)), storage=st)
         if slot is None:
             return False
         self.eng.limit(slot, req.max_steps)
@@ -151,8 +171,9 @@ class Server:
 
     def collect(self) -> list[tuple]:
         """Wait for the queued steps, read the residuals and retire; returns
-        [(request, fields, steps, residual)] of the retired requests.
-        Requests admitted after launch() did not take part in its steps."""
+        [(request, fields, steps, residual)] of the retired requests (fields
+        None for a diverged one).  Requests admitted after launch() did not
+        take part in its steps."""
         n, stepped = getattr(self, "_stepped", (0, set()))
         self._stepped = (0, set())
         if not n:
@@ -169,7 +190,7 @@ class Server:
             # retire at the step count, at the tolerance, or when the lattice
             # diverged (NaN); the first check after admission reads +inf
             if done >= req.max_steps or r < req.tol or math.isnan(r):
-                f = self.eng.fields(slot)
+                f = None if math.isnan(r) else self.eng.fields(slot)
                 self.eng.remove(slot)
                 del self.active[slot]
                 done_now.append((req, f, done, r))
@@ -181,8 +202,15 @@ class Server:
         return self.collect()
 
 
-def serve(requests: list[Request], storage: str = "f16", keep_fields: bool = False, **kw) -> dict:
-    """Run the stream in real time; latencies and throughput on the host clock."""
+def status_of(req: Request, steps: int, residual: float) -> str:
+    if math.isnan(residual):
+        return "diverged"
+    return "converged" if residual < req.tol and steps < req.max_steps else "steps"
+
+
+def serve(requests: list[Request], storage: str = "f16", keep_fields=False, **kw) -> dict:
+    """Run the stream in real time; latencies and throughput on the host
+    clock.  keep_fields: True, or a set of request ids whose answers to keep."""
     import torch
 
     stream = torch.cuda.Stream()
@@ -209,15 +237,21 @@ def serve(requests: list[Request], storage: str = "f16", keep_fields: bool = Fal
             admit_arrived()  # host set-up of new arrivals overlaps the queued steps
             for req, f, steps, r in srv.collect():
                 t = time.perf_counter() - t0
+                keep = keep_fields is True or (keep_fields and req.rid in keep_fields)
                 results[req.rid] = dict(latency=t - req.arrival, steps=steps, residual=r,
-                                        fields=f if keep_fields else None)
+                                        status=status_of(req, steps, r), storage=storage_for(req, storage),
+                                        fields=f if keep else None)
     finally:
         srv.close()
     span = time.perf_counter() - t0
     lat = np.array([results[r.rid]["latency"] for r in requests])
     work = sum(results[r.rid]["steps"] * r.cells for r in requests)
+    status = [results[r.rid]["status"] for r in requests]
     return dict(results=results, span=span, p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
-                solves_per_s=len(requests) / span, mlups=work / span / 1e6)
+                solves_per_s=len(requests) / span, mlups=work / span / 1e6,
+                status={k: status.count(k) for k in sorted(set(status))},
+                storage={k: sum(1 for r in requests if results[r.rid]["storage"] == k)
+                         for k in sorted({results[r.rid]["storage"] for r in requests})})
 
 
 def service_times_alone(requests: list[Request], storage: str = "f64", chunk: int = 200) -> dict:
@@ -245,6 +279,78 @@ def service_times_alone(requests: list[Request], storage: str = "f64", chunk: in
     return out
 
 
+def run_alone(req: Request, storage: str, steps: int, chunk: int = 200, stream=None):
+    """One request alone in its own engine for exactly `steps` steps: host
+    seconds from admission to its answer read back, and the answer."""
+    import torch
+
+    d = req.desc()
+    budget = api.instance_bytes(storage, d) + (64 << 20)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    with api.Engine(storage=storage, arith="fast", budget_bytes=budget, max_instances=1, stream=stream) as eng:
+        slot = eng.add(d)
+        left = steps
+        while left > 0:
+            n = min(chunk, left)
+            eng.step(n)
+            eng.residuals()  # the per-call check the serving loop makes
+            left -= n
+        f = eng.fields(slot)
+    return time.perf_counter() - t, f
+
+
+def service_model_by_shape(requests: list[Request], storage: str = "f64", probes=(200, 1000)) -> dict:
+    """Per (case, shape): the fixed cost and the time per step of one request
+    alone on the GPU, from two runs of probes[0] and probes[1] steps (the
+    second minus the first gives the per-step time)."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    shapes = sorted({(r.case, r.n) for r in requests})
+    out = {}
+    for case, n in shapes:
+        req = next(r for r in requests if (r.case, r.n) == (case, n))
+        run_alone(req, storage, 20, stream=stream.cuda_stream)  # warm the kernels of this shape
+        t1, _ = run_alone(req, storage, probes[0], stream=stream.cuda_stream)
+        t2, _ = run_alone(req, storage, probes[1], stream=stream.cuda_stream)
+        per_step = max(0.0, (t2 - t1) / (probes[1] - probes[0]))
+        out[(case, n)] = dict(fixed=max(0.0, t1 - per_step * probes[0]), per_step=per_step)
+    return out
+
+
+def modelled_service(requests: list[Request], model: dict, steps: dict) -> dict:
+    """Service time of each request alone: fixed + steps x per-step of its shape."""
+    out = {}
+    for r in requests:
+        m = model[(r.case, r.n)]
+        out[r.rid] = dict(service=m["fixed"] + steps[r.rid] * m["per_step"], steps=steps[r.rid])
+    return out
+
+
+def accuracy_sample(requests: list[Request], results: dict, rids) -> dict:
+    """Relative velocity L2 of served answers against FP64 runs of the same
+    requests alone to the same step counts."""
+    import torch
+
+    from .batch import velocity_l2
+
+    stream = torch.cuda.Stream()
+    errs = []
+    by_id = {r.rid: r for r in requests}
+    for rid in rids:
+        res = results[rid]
+        if res["fields"] is None:
+            continue
+        _, want = run_alone(by_id[rid], "f64", res["steps"], stream=stream.cuda_stream)
+        errs.append(dict(rid=rid, case=by_id[rid].case, n=by_id[rid].n, Re=round(by_id[rid].Re, 1),
+                         storage=res["storage"], steps=res["steps"], err=velocity_l2(res["fields"], want)))
+    vals = np.array([e["err"] for e in errs]) if errs else np.array([np.nan])
+    return dict(checked=len(errs), max=float(vals.max()), p95=float(np.percentile(vals, 95)),
+                median=float(np.median(vals)), over_1e3=int((vals > 1e-3).sum()),
+                worst=sorted(errs, key=lambda e: -e["err"])[:5])
+
+
 def fifo_one_at_a_time(requests: list[Request], service: dict) -> dict:
     """Single-server queue in arrival order with the measured service times."""
     free = 0.0
@@ -268,6 +374,11 @@ def main(argv=None) -> int:
     ap.add_argument("--max-active-cells", type=int, default=48 << 20)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--baseline", choices=["measured", "by-shape"], default="measured",
+                    help="one-at-a-time FP64: every request measured whole, or fixed + per-step time per shape")
+    ap.add_argument("--check-error", type=int, default=0,
+                    help="check this many served answers (seeded sample) against FP64 runs alone")
+    ap.add_argument("--out", default=None, help="append each rate's JSON line to this file")
     args = ap.parse_args(argv)
     from . import tune
 
@@ -275,19 +386,41 @@ def main(argv=None) -> int:
     base_reqs = request_stream(args.count, rates[0], scale_steps=args.scale_steps)
     tiles = tune.load(None)
     tiles = {k: v["tile_bx"] for k, v in tiles.items()}
-    alone = None if args.no_baseline else service_times_alone(base_reqs, "f64")
+    alone = None
+    if not args.no_baseline and args.baseline == "measured":
+        alone = service_times_alone(base_reqs, "f64")
+    model = None
+    if not args.no_baseline and args.baseline == "by-shape":
+        model = service_model_by_shape(base_reqs, "f64")
     for rate in rates:
         reqs = request_stream(args.count, rate, scale_steps=args.scale_steps)
+        sample = set()
+        if args.check_error:
+            rng = np.random.default_rng(SERVE_SEED + 2)
+            sample = set(int(x) for x in rng.choice(len(reqs), min(args.check_error, len(reqs)), replace=False))
+        t0 = time.perf_counter()
         res = serve(reqs, args.storage, budget_bytes=int(args.budget_gb * (1 << 30)),
-                    max_active_cells=args.max_active_cells, tiles=tiles)
+                    max_active_cells=args.max_active_cells, tiles=tiles, keep_fields=sample)
         line = dict(rate=rate, count=args.count, storage=args.storage, p50_s=res["p50"], p99_s=res["p99"],
                     solves_per_s=res["solves_per_s"], mlups=res["mlups"], span_s=res["span"],
-                    steps_scale=args.scale_steps)
+                    steps_scale=args.scale_steps, status=res["status"], storage_requests=res["storage"],
+                    wall_s=time.perf_counter() - t0)
+        steps = {r.rid: res["results"][r.rid]["steps"] for r in reqs}
+        base = None
         if alone:
-            b = fifo_one_at_a_time(reqs, alone)
-            line["fp64_one_at_a_time"] = dict(p50_s=b["p50"], p99_s=b["p99"], solves_per_s=b["solves_per_s"],
-                                              mlups=b["mlups"])
+            base, how = fifo_one_at_a_time(reqs, alone), "each request measured alone"
+        elif model:
+            base = fifo_one_at_a_time(reqs, modelled_service(reqs, model, steps))
+            how = "fixed + per-step time per shape measured alone, times each request's served step count"
+        if base:
+            line["fp64_one_at_a_time"] = dict(p50_s=base["p50"], p99_s=base["p99"],
+                                              solves_per_s=base["solves_per_s"], mlups=base["mlups"], how=how)
+        if sample:
+            line["accuracy_vs_fp64"] = accuracy_sample(reqs, res["results"], sorted(sample))
         print(json.dumps(line), flush=True)
+        if args.out:
+            with open(args.out, "a") as fh:
+                fh.write(json.dumps(line) + "\n")
     return 0
 
 

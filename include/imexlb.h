@@ -47,8 +47,13 @@ typedef enum imexlb_case { IMEXLB_TGV = 0, IMEXLB_CAVITY = 1, IMEXLB_SPHERE = 2 
  * IMEXLB_BC_STANDARD: halfway bounce-back with the moving-wall correction
  *   -2 w_i rho (c_i . u_w)/cs^2 on the cavity lid; for the sphere a periodic
  *   channel with an equilibrium inlet, a zero-gradient outlet and halfway
- *   bounce-back on a voxelised sphere (momentum-exchange drag available). */
-typedef enum imexlb_bc { IMEXLB_BC_REFERENCE = 0, IMEXLB_BC_STANDARD = 1 } imexlb_bc;
+ *   bounce-back on a voxelised sphere (momentum-exchange drag available).
+ * IMEXLB_BC_SLAB (cavity only, FP64 or FP32 storage): the standard cavity's
+ *   bottom wall and moving lid with x and y periodic, a lid-driven slab whose
+ *   steady state is plane Couette flow u(z) = u_w (z + 1/2) / nz; it checks
+ *   the moving-wall rule against that exact solution.  No counterpart in the
+ *   reference. */
+typedef enum imexlb_bc { IMEXLB_BC_REFERENCE = 0, IMEXLB_BC_STANDARD = 1, IMEXLB_BC_SLAB = 2 } imexlb_bc;
 
 /* Storage of the distributions in HBM.  F64 stores f_i; F32/F16/BF16 store
  * the deviation f_i - w_i * 3 p_ref scaled per population, and collide in FP32. */
@@ -283,6 +288,13 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
  * follow the work already queued on the engine's stream, so a host can admit
  * while earlier steps run. */
 int imexlb_engine_add(imexlb_engine* e, const imexlb_instance_desc* d, int* slot);
+/* The same in a storage format of its own: one engine holds instances of
+ * several formats (each format's instances run their own kernel groups in
+ * the same step launches and graph), so a caller can store in FP16 the
+ * instances whose relaxation is far enough from 1/2 and in FP32 the
+ * marginally stable ones.  imexlb_engine_create's storage is the format of
+ * imexlb_engine_add. */
+int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb_storage storage, int* slot);
 int imexlb_engine_remove(imexlb_engine* e, int slot);
 /* Every active instance advances nsteps steps; the moments of the last are stored. */
 int imexlb_engine_step(imexlb_engine* e, int nsteps);
@@ -303,8 +315,8 @@ int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st);
 int imexlb_engine_instance_bytes(imexlb_storage storage, const imexlb_instance_desc* d, size_t* bytes);
 /* Pre-emption of one engine instance: its state (current distribution
  * buffer, moments, step count) into a host buffer, and admission of an
- * instance from such a buffer (same descriptor and storage), which then
- * continues bit for bit.  The restored instance's residual history starts
+ * instance from such a buffer (same descriptor; the instance keeps the
+ * checkpoint's storage format), which then continues bit for bit.  The restored instance's residual history starts
  * over.  No counterpart in the reference. */
 int imexlb_engine_checkpoint_size(const imexlb_engine* e, int slot, size_t* bytes);
 int imexlb_engine_checkpoint_save(imexlb_engine* e, int slot, void* host, size_t bytes);

@@ -139,13 +139,15 @@ class Oracle:
 
 
 class OracleStd:
-    """The standard-boundary specification (moving-lid cavity, sphere channel)."""
+    """The standard-boundary specification (moving-lid cavity, sphere channel,
+    and "slab": the cavity's lid and bottom wall with x and y periodic)."""
 
     def __init__(self, case: str, nx: int, ny: int, nz: int, tau0: float, rho0: float = 1.0, u0: float = 0.1,
                  lid_u: float = 0.0, inlet_u: float = 0.0, sphere_d: float = 0.0, sphere_c=(0.0, 0.0, 0.0)):
         self.lib = oracle_lib()
         self.n = (nx, ny, nz)
-        self.h = self.lib.oracle_std_create(CASES[case], nx, ny, nz, tau0, rho0, u0, lid_u, inlet_u, sphere_d,
+        kase = 3 if case == "slab" else CASES[case]  # ORACLE_SLAB: the cavity's rules, x and y periodic
+        self.h = self.lib.oracle_std_create(kase, nx, ny, nz, tau0, rho0, u0, lid_u, inlet_u, sphere_d,
                                             *sphere_c)
         if not self.h:
             raise ValueError("oracle_std_create failed")

@@ -127,13 +127,41 @@ void oracle_destroy(oracle_lbm* o) {
   free(o);
 }
 
-/* feq of tgv/src/lbm.cpp:211-215 (initf) and :228-232 (collision) */
-static inline double feq_ref(const oracle_lbm* o, int ii, double u, double v, double w, double p) {
-  const double e0 = o->e[ii][0], e1 = o->e[ii][1], e2 = o->e[ii][2];
+/* feq of tgv/src/lbm.cpp:211-215 (initf) and :228-232 (collision), with the
+ * reference's tables t = W_REF, e = E_REF and its expression order.  The
+ * standard-boundary variants below use this function too. */
+static inline double feq_tab(int ii, double u, double v, double w, double p) {
+  const double e0 = E_REF[ii][0], e1 = E_REF[ii][1], e2 = E_REF[ii][2];
+  const double t = W_REF[ii];
   const double edu = e0 * u + e1 * v + e2 * w;
   const double udu = u * u + v * v + w * w;
   const double eu2 = (e0 * u + e1 * v + e2 * w) * (e0 * u + e1 * v + e2 * w);
-  return o->t[ii] * p * 3.0 + o->t[ii] * (3.0 * edu + 4.5 * eu2 - 1.5 * udu);
+  return t * p * 3.0 + t * (3.0 * edu + 4.5 * eu2 - 1.5 * udu);
+}
+
+static inline double feq_ref(const oracle_lbm* o, int ii, double u, double v, double w, double p) {
+  (void)o; /* o->t and o->e are copies of W_REF and E_REF */
+  return feq_tab(ii, u, v, w, p);
+}
+
+/* One population's collision, tgv/src/lbm.cpp:233: f -= (f - feq)/(tau0 + 0.5) */
+static inline double collide_ref(double f, double feq, double tau0) { return f - (f - feq) / (tau0 + 0.5); }
+
+/* Moments of one cell's populations as the cavity and sphere Update sum them
+ * (lid_driven_cavity/src/lbm.cpp:330-339, sphere/src/lbm.cpp:385-394): one
+ * loop over the populations in order from zero accumulators. */
+static inline void moments_ref(const double* fc, double* p, double* u, double* v, double* w) {
+  double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
+  for (int ii = 0; ii < Q; ++ii) {
+    pm = pm + fc[ii] / 3.0;
+    um = um + fc[ii] * E_REF[ii][0];
+    vm = vm + fc[ii] * E_REF[ii][1];
+    wm = wm + fc[ii] * E_REF[ii][2];
+  }
+  *p = pm;
+  *u = um;
+  *v = vm;
+  *w = wm;
 }
 
 /* ------------------------------------------------------------ Initialize */
@@ -212,7 +240,7 @@ void oracle_collision(oracle_lbm* o) { /* tgv/src/lbm.cpp:222-237 */
         for (int ii = 0; ii < Q; ++ii) {
           const double feq = feq_ref(o, ii, o->ua[c], o->va[c], o->wa[c], o->p[c]);
           double* fp = &o->f[ii + Q * c];
-          *fp -= (*fp - feq) / (tau0 + 0.5);
+          *fp = collide_ref(*fp, feq, tau0);
         }
       }
 }
@@ -405,14 +433,8 @@ void oracle_update(oracle_lbm* o) {
     for (int j = GHOST; j < o->ly - GHOST; ++j)
       for (int i = GHOST; i < o->lx - GHOST; ++i) {
         const size_t c = C3(o, i, j, k);
-        const double* fc = &o->f[Q * c];
-        double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
-        for (int ii = 0; ii < Q; ++ii) {
-          pm = pm + fc[ii] / 3.0;
-          um = um + fc[ii] * o->e[ii][0];
-          vm = vm + fc[ii] * o->e[ii][1];
-          wm = wm + fc[ii] * o->e[ii][2];
-        }
+        double pm, um, vm, wm;
+        moments_ref(&o->f[Q * c], &pm, &um, &vm, &wm);
         if (o->kase == ORACLE_CAVITY) {
           o->p[c] = pm;
           o->ua[c] = um;
@@ -605,31 +627,19 @@ static inline size_t SC(const oracle_std* o, int i, int j, int k) {
   return (size_t)i + (size_t)o->nx * ((size_t)j + (size_t)o->ny * (size_t)k);
 }
 
-/* the device's e.u with zero terms dropped (same value as the reference's
- * (e0*u + e1*v) + e2*w) */
-static double std_edu(int q, double u, double v, double w) {
-  const int a = E_REF[q][0], b = E_REF[q][1], c = E_REF[q][2];
-  double t = 0.0;
-  int have = 0;
-  if (a) { t = a > 0 ? u : -u; have = 1; }
-  if (b) { t = have ? (b > 0 ? t + v : t - v) : (b > 0 ? v : -v); have = 1; }
-  if (c) { t = have ? (c > 0 ? t + w : t - w) : (c > 0 ? w : -w); }
-  return t;
-}
-
-static void std_collide(const oracle_std* o, const double* f, double u, double v, double w, double p, double* out) {
-  const double udu15 = 1.5 * ((u * u + v * v) + w * w);
-  for (int q = 0; q < Q; ++q) {
-    const double t = W_REF[q];
-    const double e = std_edu(q, u, v, w);
-    const double feq = (t * p) * 3.0 + t * (((3.0 * e) + (4.5 * (e * e))) - udu15);
-    out[q] = f[q] - ((f[q] - feq) / (o->tau0 + 0.5));
-  }
+/* Post-collision populations of one cell from its pulled populations: the
+ * reference's moments (moments_ref), equilibrium (feq_tab) and collision
+ * (collide_ref), so that only the link rules of oracle_std_step are new. */
+static void std_update_cell(const oracle_std* o, const double* f, double* u, double* v, double* w, double* p,
+                            double* out) {
+  moments_ref(f, p, u, v, w);
+  for (int q = 0; q < Q; ++q) out[q] = collide_ref(f[q], feq_tab(q, *u, *v, *w, *p), o->tau0);
 }
 
 oracle_std* oracle_std_create(int kase, int nx, int ny, int nz, double tau0, double rho0, double u0,
                               double lid_u, double inlet_u, double sphere_d, double cx, double cy, double cz) {
-  if ((kase != ORACLE_CAVITY && kase != ORACLE_SPHERE) || nx < 2 || ny < 2 || nz < 2) return NULL;
+  if ((kase != ORACLE_CAVITY && kase != ORACLE_SPHERE && kase != ORACLE_SLAB) || nx < 2 || ny < 2 || nz < 2)
+    return NULL;
   oracle_std* o = (oracle_std*)calloc(1, sizeof(oracle_std));
   o->kase = kase;
   o->nx = nx;
@@ -660,21 +670,12 @@ oracle_std* oracle_std_create(int kase, int nx, int ny, int nz, double tau0, dou
         o->fluid[c] = (unsigned char)!solid;
         o->u[c] = (kase == ORACLE_SPHERE && !solid) ? inlet_u : 0.0;
       }
-  for (int q = 0; q < Q; ++q) {
-    const double t = W_REF[q];
-    const double e = E_REF[q][0] * inlet_u;
-    o->feq_in[q] = t * (3.0 * (0.0 - 0.0) + 3.0 * e + 4.5 * e * e - 1.5 * inlet_u * inlet_u);
-  }
-  /* f = feq of the initial fields; the first collision leaves it unchanged */
-  for (size_t c = 0; c < n; ++c) {
-    const double uu = o->u[c], vv = o->v[c], ww = o->w[c], pp = o->p[c];
-    const double udu15 = 1.5 * ((uu * uu + vv * vv) + ww * ww);
-    for (int q = 0; q < Q; ++q) {
-      const double t = W_REF[q];
-      const double e = std_edu(q, uu, vv, ww);
-      o->A[q + Q * c] = (t * pp) * 3.0 + t * (((3.0 * e) + (4.5 * (e * e))) - udu15);
-    }
-  }
+  /* the inlet's equilibrium: the reference's feq of (inlet_u, 0, 0) at p = 0 */
+  for (int q = 0; q < Q; ++q) o->feq_in[q] = feq_tab(q, inlet_u, 0.0, 0.0, 0.0);
+  /* f = feq of the initial fields (tgv/src/lbm.cpp:209-218); the first
+   * collision leaves it unchanged */
+  for (size_t c = 0; c < n; ++c)
+    for (int q = 0; q < Q; ++q) o->A[q + Q * c] = feq_tab(q, o->u[c], o->v[c], o->w[c], o->p[c]);
   return o;
 }
 
@@ -707,7 +708,11 @@ void oracle_std_step(oracle_std* o, int nsteps) {
           for (int q = 0; q < Q; ++q) {
             const int ex = E_REF[q][0], ey = E_REF[q][1], ez = E_REF[q][2];
             int si = i - ex, sj = j - ey, sk = k - ez;
-            if (o->kase == ORACLE_CAVITY) {
+            if (o->kase == ORACLE_CAVITY || o->kase == ORACLE_SLAB) {
+              if (o->kase == ORACLE_SLAB) {
+                si = (si + nx) % nx;
+                sj = (sj + ny) % ny;
+              }
               if (si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz) {
                 f[q] = o->A[q + Q * SC(o, si, sj, sk)];
               } else {
@@ -734,18 +739,7 @@ void oracle_std_step(oracle_std* o, int nsteps) {
               }
             }
           }
-          double pm = 0.0, um = 0.0, vm = 0.0, wm = 0.0;
-          for (int q = 0; q < Q; ++q) {
-            pm = pm + f[q] / 3.0;
-            if (E_REF[q][0]) um = E_REF[q][0] > 0 ? um + f[q] : um - f[q];
-            if (E_REF[q][1]) vm = E_REF[q][1] > 0 ? vm + f[q] : vm - f[q];
-            if (E_REF[q][2]) wm = E_REF[q][2] > 0 ? wm + f[q] : wm - f[q];
-          }
-          o->u[c] = um;
-          o->v[c] = vm;
-          o->w[c] = wm;
-          o->p[c] = pm;
-          std_collide(o, f, um, vm, wm, pm, &o->B[Q * c]);
+          std_update_cell(o, f, &o->u[c], &o->v[c], &o->w[c], &o->p[c], &o->B[Q * c]);
         }
     double* t = o->A;
     o->A = o->B;
@@ -833,7 +827,7 @@ int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbac
     }
     const long e = (t % 1009 == 0) ? -1000 : (long)((s >> 52) % 121) - 60;
     cv.u = ((s >> 63) << 63) | ((unsigned long long)(1023 + e) << 52) | (s & 0xFFFFFFFFFFFFFULL);
-    const double x = (t % 997 == 0) ? 0.0 : cv.v;
+    const double x = (t % 997 == 0) ? ((t & 1) ? -0.0 : 0.0) : cv.v; /* zeros of both signs */
     const double q0 = x * z;
     const double r0 = fma(-q0, d, x);
     const double q1 = fma(r0, z, q0);
@@ -857,11 +851,14 @@ int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbac
       q = q0;
     } else if (accept) {
       q = q1;
+    } else if (x == 0.0) {
+      q = x; /* +-0 / d = +-0 for d > 0 */
     } else {
       q = x / d;
       ++fb;
     }
-    if (q != x / d) ++bad;
+    const double want = x / d;
+    if (memcmp(&q, &want, sizeof q) != 0) ++bad; /* bit patterns: a zero's sign counts */
   }
   if (fallbacks) *fallbacks = fb;
   return bad;

@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-enum { ORACLE_TGV = 0, ORACLE_CAVITY = 1, ORACLE_SPHERE = 2 };
+enum { ORACLE_TGV = 0, ORACLE_CAVITY = 1, ORACLE_SPHERE = 2, ORACLE_SLAB = 3 };
 
 typedef struct oracle_lbm oracle_lbm;
 
@@ -80,8 +80,13 @@ int oracle_threads(void);
  *     from x = nx-1 instead of x = nx), halfway bounce-back on the voxelised
  *     sphere |x - c|^2 <= d^2/4; solid cells are not updated and report
  *     zero moments.  Drag = sum over links of -2 f_q(x) e_q.
- * Both use the reference's p-based equilibrium and collision, FP64, with
- * the same operation order as the device's EXACT mode.
+ *   ORACLE_SLAB: the cavity's rules on a slab periodic in x and y: halfway
+ *     bounce-back at the bottom (z < 0, at rest) and at the lid (z >= nz,
+ *     moving along +x at lid_u); its steady state is plane Couette flow,
+ *     u(z) = lid_u (z + 1/2) / nz.
+ * All use the reference's moments, equilibrium and collision (feq_tab,
+ * moments_ref, collide_ref: the expressions of the reference's Update and
+ * Collision, FP64): only the link rules above are this specification's own.
  * ------------------------------------------------------------------------ */
 typedef struct oracle_std oracle_std;
 oracle_std* oracle_std_create(int kase, int nx, int ny, int nz, double tau0, double rho0, double u0,

@@ -43,3 +43,22 @@ def test_tiles_come_from_the_cache(tmp_path):
     cache.write_text(json.dumps({"device": "x", "entries": entries}))
     tiles = tune.tiles_for(specs, "f16", cache=str(cache), tune_missing=False)
     assert tiles["f16/cavity/48x48x48"] == 32 and tiles["f16/tgv/24x24x24"] == 0
+
+
+def test_fp16_storage_plan():
+    """The FP16 form stores marginally stable instances (tau - 1/2 below
+    FP16_MIN_TAU0) in FP32; "f16-all" and the other formats store every
+    instance in one format."""
+    from imexlb_b200 import batch, serve
+
+    specs = batch.batch_specs(256)
+    plan = batch.storage_plan(specs, "f16")
+    assert all((st == "f16") == (s.tau0 >= batch.FP16_MIN_TAU0) for s, st in zip(specs, plan))
+    assert 0 < plan.count("f32") < plan.count("f16")
+    assert batch.storage_plan(specs, "f16-all") == ["f16"] * 256
+    assert batch.storage_plan(specs, "f32") == ["f32"] * 256
+    assert batch.engine_storage("f16-all") == "f16"
+    reqs = serve.request_stream(200, 10.0)
+    for r in reqs:
+        assert serve.storage_for(r, "f16") == ("f16" if r.tau0 >= batch.FP16_MIN_TAU0 else "f32")
+        assert serve.storage_for(r, "f64") == "f64"

@@ -18,8 +18,8 @@ def test_checked_division_matches_ieee_division():
 
     fb = ctypes.c_long()
     assert oracle_lib().oracle_check_div(5_000_000, 424242, 0, ctypes.byref(fb)) == 0
-    # the zero and tiny samples (about 1 in 500) take the IEEE fallback; other
-    # rejections would be rare near-ties
+    # zeros (both signs) are returned as they are; the tiny samples (about 1
+    # in 1000) take the IEEE fallback; other rejections would be rare near-ties
     assert 0 < fb.value < 5_000_000 // 100
 
 

@@ -44,7 +44,7 @@ class FakeEngine:
         self.taken, self.left, self.calls, self.res = {}, {}, [], {}
         self.next = 0
 
-    def try_add(self, desc):
+    def try_add(self, desc, storage=None):
         s = self.next
         self.next += 1
         self.taken[s], self.left[s], self.res[s] = 0, None, float("inf")
