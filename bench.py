@@ -59,9 +59,12 @@ WORKLOADS = {
                           u0=0.1, R=128.0, lid_u=0.1),
     "cavity128-f64-exact": dict(case="cavity", bc="standard", storage="f64", arith="exact", n=(128, 128, 128),
                                 Re=1000, u0=0.1, R=128.0, lid_u=0.1),
-    # the reference's own boundary passes (bit-exact drop-in)
+    # the reference's own boundary passes (bit-exact drop-in) at Re 100: at Re
+    # 1000 they overflow after about 70 steps (the wall sits on the fluid node
+    # and the lid speed is forced on the top plane), and a bench would time
+    # NaN arithmetic; at Re 100 the flow stays bounded
     "cavity128-f64-refbc": dict(case="cavity", bc="reference", storage="f64", arith="exact", n=(128, 128, 128),
-                                Re=1000, u0=0.1, R=128.0, lid_u=0.1),
+                                Re=100, u0=0.1, R=128.0, lid_u=0.1),
     "tgv64-f64": dict(case="tgv", bc="reference", storage="f64", arith="exact", n=(64, 64, 64), Re=100, u0=0.05,
                       R=0.1, lid_u=0.0),
     "tgv256-f64": dict(case="tgv", bc="reference", storage="f64", arith="fast", n=(256, 256, 256), Re=1600,
@@ -69,7 +72,7 @@ WORKLOADS = {
     "cavity128-f16": dict(case="cavity", bc="standard", storage="f16", arith="fast", n=(128, 128, 128), Re=1000,
                           u0=0.1, R=128.0, lid_u=0.1),
     "cavity128-f64-refbc-fast": dict(case="cavity", bc="reference", storage="f64", arith="fast", n=(128, 128, 128),
-                                     Re=1000, u0=0.1, R=128.0, lid_u=0.1),
+                                     Re=100, u0=0.1, R=128.0, lid_u=0.1),
     "cavity128-bf16": dict(case="cavity", bc="standard", storage="bf16", arith="fast", n=(128, 128, 128), Re=1000,
                            u0=0.1, R=128.0, lid_u=0.1),
     "cavity256-f64": dict(case="cavity", bc="standard", storage="f64", arith="fast", n=(256, 256, 256), Re=1000,

@@ -470,6 +470,7 @@ struct Slot {
   int64_t ncell = 0;
   int64_t steps = 0;
   int64_t run = 0;  // steps taken since admission (its buffer parity)
+  int64_t run_checked = -1;  // `run` at the last residual check
   bool have_prev = false;
   int bx_log2 = 5;
   int seg = -1;  // index into the segment table of the current work list
@@ -1072,16 +1073,27 @@ int imexlb_engine_limit(imexlb_engine* e, int slot, int steps) {
   Slot& sl = e->slots[slot];
   EngInst& in = e->h_inst[slot];
   // an instance that stopped missed steps: realign its buffer parity with
-  // the engine's (the next step reads the buffer of its run's parity)
+  // the engine's (the next step reads the buffer of its run's parity).  The
+  // updates follow the work already queued on the stream (the steps queued
+  // before this call still see the old values), through a pinned staging
+  // buffer, so the call does not wait for the GPU.
   const int parity0 = static_cast<int>((e->gstep ^ sl.run) & 1);
-  if (parity0 != in.parity0) {
-    IMX_ECUDA(cudaStreamSynchronize(e->stream));  // no queued step reads the old value
+  const bool realign = parity0 != in.parity0;
+  cudaError_t serr = cudaSuccess;
+  const size_t inst_bytes = (sizeof(EngInst) + 15) & ~static_cast<size_t>(15);
+  const int sb = e->staging.get(inst_bytes + sizeof(int), &serr);
+  if (sb < 0) return efail(IMEXLB_E_NOMEM, std::string("pinned upload buffer: ") + cudaGetErrorString(serr));
+  char* up = e->staging.ptr(sb);
+  if (realign) {
     in.parity0 = parity0;
-    IMX_ECUDA(cudaMemcpy(e->d_inst.p + slot, &in, sizeof(EngInst), cudaMemcpyHostToDevice));
+    std::memcpy(up, &in, sizeof(EngInst));
+    IMX_ECUDA(cudaMemcpyAsync(e->d_inst.p + slot, up, sizeof(EngInst), cudaMemcpyHostToDevice, e->stream));
     e->dirty = true;  // the staged tiles' descriptors carry it too
   }
   e->h_left[slot] = steps < 0 ? ENG_NO_LIMIT : steps;
-  IMX_ECUDA(cudaMemcpyAsync(e->d_left.p + slot, &e->h_left[slot], sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  std::memcpy(up + inst_bytes, &e->h_left[slot], sizeof(int));
+  IMX_ECUDA(cudaMemcpyAsync(e->d_left.p + slot, up + inst_bytes, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(e->staging.release_after(sb, e->stream));
   return IMEXLB_OK;
 }
 
@@ -1163,10 +1175,14 @@ int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
     Slot& sl = e->slots[e->seg_slots[g]];
     const double d2 = res[2 * g], n2 = res[2 * g + 1];
     out[e->seg_slots[g]] = !sl.have_prev ? INFINITY : (n2 > 0 ? std::sqrt(d2 / n2) : (d2 > 0 ? INFINITY : 0.0));
+    // -1: no step since the last check (stopped at its step limit), so no
+    // change to measure -- not a converged solve
+    if (sl.have_prev && sl.run == sl.run_checked) out[e->seg_slots[g]] = -1.0;
     // NaN: the velocity field is not finite (before the first check the
     // previous field is not yet defined, so only the current one counts)
     if (!std::isfinite(n2) || (sl.have_prev && !std::isfinite(d2))) out[e->seg_slots[g]] = NAN;
     sl.have_prev = true;
+    sl.run_checked = sl.run;
   }
   return IMEXLB_OK;
 }

@@ -412,6 +412,66 @@ __global__ void reduce_pass2(RedKind kind, const double* part, int nparts, doubl
   }
 }
 
+// Both sums of the velocity residual in one pass over (u, v, w) and the
+// previous (u2, v2, w2): part[2 b] = sum |u - u2|^2, part[2 b + 1] = sum |u|^2
+// over block b's slice (the same slices and order as reduce_pass1), then
+// one block adds the partials in order into out[0], out[1].
+__global__ void resid_pass1(const double* u, const double* v, const double* w, const double* u2, const double* v2,
+                            const double* w2, int64_t n, double* part) {
+  double d2 = 0.0, n2 = 0.0;
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < n;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double a = u[c], b = v[c], g = w[c];
+    const double du = a - u2[c], dv = b - v2[c], dw = g - w2[c];
+    d2 += du * du + dv * dv + dw * dw;
+    n2 += a * a + b * b + g * g;
+  }
+  __shared__ double sh[2][RED_THREADS / 32];
+  d2 = warp_sum(d2);
+  n2 = warp_sum(n2);
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = d2;
+    sh[1][threadIdx.x >> 5] = n2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double x = threadIdx.x < RED_THREADS / 32 ? sh[0][threadIdx.x] : 0.0;
+    double y = threadIdx.x < RED_THREADS / 32 ? sh[1][threadIdx.x] : 0.0;
+    x = warp_sum(x);
+    y = warp_sum(y);
+    if (threadIdx.x == 0) {
+      part[2 * blockIdx.x] = x;
+      part[2 * blockIdx.x + 1] = y;
+    }
+  }
+}
+
+__global__ void resid_pass2(const double* part, int nparts, double* out) {
+  double x = 0.0, y = 0.0;
+  for (int c = threadIdx.x; c < nparts; c += blockDim.x) {
+    x += part[2 * c];
+    y += part[2 * c + 1];
+  }
+  __shared__ double sh[2][RED_THREADS / 32];
+  x = warp_sum(x);
+  y = warp_sum(y);
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = x;
+    sh[1][threadIdx.x >> 5] = y;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double a = threadIdx.x < RED_THREADS / 32 ? sh[0][threadIdx.x] : 0.0;
+    double b = threadIdx.x < RED_THREADS / 32 ? sh[1][threadIdx.x] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (threadIdx.x == 0) {
+      out[0] = a;
+      out[1] = b;
+    }
+  }
+}
+
 // The velocity residual sqrt(num / den) from the two sums of the residual
 // reduction, as the synchronous path forms it on the host (INFINITY on the
 // first call, NaN when a sum is not finite).
@@ -428,6 +488,14 @@ __global__ void residual_finish_kernel(const double* nd, int first, double* out)
 }
 
 }  // namespace
+
+cudaError_t launch_residual_sums(const double* u, const double* v, const double* w, const double* u2,
+                                 const double* v2, const double* w2, int64_t n, double* scratch, double* out,
+                                 cudaStream_t s) {
+  resid_pass1<<<RED_BLOCKS, RED_THREADS, 0, s>>>(u, v, w, u2, v2, w2, n, scratch);
+  resid_pass2<<<1, RED_THREADS, 0, s>>>(scratch, RED_BLOCKS, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_residual_finish(const double* nd, int first, double* out, cudaStream_t s) {
   residual_finish_kernel<<<1, 1, 0, s>>>(nd, first, out);

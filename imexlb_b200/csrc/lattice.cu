@@ -18,6 +18,8 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/imexlb.h"
@@ -269,6 +271,7 @@ struct imexlb_lattice {
   DevArray<uint32_t> links;   // standard sphere: per-cell solid-link bits
   DevArray<double> inlet;     // reference sphere inlet profile per z
   DevArray<int64_t> gtgt, gsrc;
+  DevArray<int32_t> face_codes;  // reference cavity: the passes resolved per face-cell link
   int64_t gn = 0;
   DevArray<double> red;       // reduction partials + result
   DevArray<double> drag_part; // standard sphere: per-block drag partials of the last step
@@ -507,6 +510,73 @@ int upload_case(imexlb_lattice* h) {
   return IMEXLB_OK;
 }
 
+// The face-code table of a reference cavity (FaceCodes in lattice.h) from
+// its ghost-slot plan (tgt[n] takes src[n], encoded as in GhostPlan) in the
+// index space of `slot(q, i, j, k)` (the pulled slot of interior cell (i, j, k)
+// along -e_q): for every face cell, indexed by the first face it lies on, the
+// source of each link whose pull leaves the box -- the plan's source when the
+// pulled slot is planned, else the slot itself (never written: its initial
+// value) -- and the links whose pulled slot a later step reads as its
+// previous value.  False when an index does not fit 31 bits or a planned slot
+// is not pulled by exactly one face cell (then the gather runs instead).
+template <class Slot>
+bool face_codes_generic(int nx, int ny, int nz, int64_t total, Slot slot, const std::vector<int64_t>& tgt,
+                        const std::vector<int64_t>& src, std::vector<int32_t>& codes, int64_t base[6],
+                        int32_t dim[6]) {
+  if (total >= (int64_t(1) << 31) - 2) return false;
+  std::unordered_map<int64_t, int64_t> plan;
+  plan.reserve(tgt.size() * 2);
+  std::unordered_set<int64_t> keep;  // slots read as previous values
+  for (size_t n = 0; n < tgt.size(); ++n) {
+    plan[tgt[n]] = src[n];
+    if (src[n] <= -2) keep.insert(-src[n] - 2);
+  }
+  const int64_t cells[6] = {int64_t(ny) * nz, int64_t(ny) * nz, int64_t(nx) * nz,
+                            int64_t(nx) * nz, int64_t(nx) * ny, int64_t(nx) * ny};
+  int64_t off = 0;
+  for (int f = 0; f < 6; ++f) {
+    base[f] = off;
+    dim[f] = f < 2 ? ny : nx;
+    off += cells[f] * FACE_CODE_WORDS;
+  }
+  codes.assign(static_cast<size_t>(off), 0);
+  size_t used = 0;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const unsigned wf = (i == 0 ? 1u : 0u) | (i == nx - 1 ? 2u : 0u) | (j == 0 ? 4u : 0u) |
+                            (j == ny - 1 ? 8u : 0u) | (k == 0 ? 16u : 0u) | (k == nz - 1 ? 32u : 0u);
+        if (!wf) continue;
+        int face = 0;
+        while (!((wf >> face) & 1u)) ++face;
+        const int fa = face < 2 ? j : i, fb = face < 4 ? k : j;
+        int32_t* w = codes.data() + base[face] + (static_cast<int64_t>(fb) * dim[face] + fa) * FACE_CODE_WORDS;
+        uint32_t keep_bits = 0;
+        for (int q = 0; q < Q; ++q) {
+          const int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
+          const bool leaves = (ex > 0 && (wf & 1u)) || (ex < 0 && (wf & 2u)) || (ey > 0 && (wf & 4u)) ||
+                              (ey < 0 && (wf & 8u)) || (ez > 0 && (wf & 16u)) || (ez < 0 && (wf & 32u));
+          if (!leaves) continue;
+          const int64_t g = slot(q, i - ex, j - ey, k - ez);
+          const auto it = plan.find(g);
+          const int64_t code = it != plan.end() ? it->second : g;
+          if (code >= total || code < -total - 2) return false;
+          w[q] = static_cast<int32_t>(code);
+          if (it != plan.end()) ++used;
+          if (keep.count(g)) keep_bits |= 1u << q;
+        }
+        w[Q] = static_cast<int32_t>(keep_bits);
+      }
+  return used == tgt.size();  // every planned slot is some face cell's pulled slot
+}
+
+bool face_codes_for(const Layout& L, const std::vector<int64_t>& tgt, const std::vector<int64_t>& src,
+                    std::vector<int32_t>& codes, int64_t base[6], int32_t dim[6]) {
+  return face_codes_generic(L.nx, L.ny, L.nz, static_cast<int64_t>(L.sq) * Q,
+                            [&](int q, int i, int j, int k) { return L.interior(q, i, j, k); }, tgt, src, codes, base,
+                            dim);
+}
+
 }  // namespace
 
 extern "C" {
@@ -629,7 +699,10 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   if (uses_wall_records(h->cfg, P.nx, P.ny, L.pitch))
     for (int b = 0; b < 2; ++b) IMX_CUDA(h->rec[b].alloc(static_cast<size_t>(P.ny) * P.nz * WallRecord::WORDS, h->stream));
   IMX_CUDA(h->mom.alloc(4 * static_cast<size_t>(h->ncell), h->stream));
-  IMX_CUDA(h->red.alloc(reduce_blocks() + 8, h->stream));
+  IMX_CUDA(h->red.alloc(2 * reduce_blocks() + 8, h->stream));
+  // the residual's previous velocity field, allocated here so that a solve
+  // loop's first residual check does not wait for the queued steps
+  IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(h->ncell), h->stream));
   IMX_CUDA(h->err.alloc(1, h->stream));
   IMX_CUDA(cudaMemset(h->err.p, 0, sizeof(int)));
 
@@ -742,11 +815,20 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       const int64_t src = plan.src[n];
       s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
     }
-    h->gn = static_cast<int64_t>(t.size());
-    IMX_CUDA(h->gtgt.alloc(t.size(), h->stream));
-    IMX_CUDA(h->gsrc.alloc(s.size(), h->stream));
-    IMX_CUDA(cudaMemcpy(h->gtgt.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
-    IMX_CUDA(cudaMemcpy(h->gsrc.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice));
+    std::vector<int32_t> codes;
+    if (P.kase == IMEXLB_CAVITY && (P.storage == IMEXLB_F64 || P.storage == IMEXLB_F32) &&
+        face_codes_for(L, t, s, codes, a.face_base, a.face_dim)) {
+      // the step kernel resolves the passes per link: no gather
+      IMX_CUDA(h->face_codes.alloc(codes.size(), h->stream));
+      IMX_CUDA(cudaMemcpy(h->face_codes.p, codes.data(), codes.size() * 4, cudaMemcpyHostToDevice));
+      a.face_codes = h->face_codes.p;
+    } else {
+      h->gn = static_cast<int64_t>(t.size());
+      IMX_CUDA(h->gtgt.alloc(t.size(), h->stream));
+      IMX_CUDA(h->gsrc.alloc(s.size(), h->stream));
+      IMX_CUDA(cudaMemcpy(h->gtgt.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
+      IMX_CUDA(cudaMemcpy(h->gsrc.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice));
+    }
   }
 
   const int rc = upload_case(h.get());
@@ -967,7 +1049,7 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
   const double* w = u + 2 * N;
   const double* p = u + 3 * N;
   double* part = h->red.p;
-  double* res = h->red.p + reduce_blocks();
+  double* res = h->red.p + 2 * reduce_blocks();
   switch (kind) {
     case IMEXLB_REDUCE_MASS:
       IMX_CUDA(launch_reduce(RedKind::Mass, u, v, w, p, nullptr, nullptr, nullptr, N, part, res, h->stream));
@@ -980,16 +1062,15 @@ int imexlb_reduce(imexlb_lattice* h, int kind, double* out) {
       break;
     case IMEXLB_REDUCE_RESIDUAL: {
       if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N), h->stream));
-      double num = 0, den = 0;
+      double nd[2] = {0.0, 0.0};
       if (h->have_prev) {
-        IMX_CUDA(launch_reduce(RedKind::DiffSq, u, v, w, p, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N,
-                               part, res, h->stream));
-        IMX_CUDA(cudaMemcpyAsync(&num, res, 8, cudaMemcpyDeviceToHost, h->stream));
-        IMX_CUDA(launch_reduce(RedKind::NormSq, u, v, w, p, nullptr, nullptr, nullptr, N, part, res + 1, h->stream));
-        IMX_CUDA(cudaMemcpyAsync(&den, res + 1, 8, cudaMemcpyDeviceToHost, h->stream));
+        IMX_CUDA(launch_residual_sums(u, v, w, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N, part, res,
+                                      h->stream));
+        IMX_CUDA(cudaMemcpyAsync(nd, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       }
       IMX_CUDA(cudaMemcpyAsync(h->prev_mom.p, u, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
       if (const int rc = sync_checked(h)) return rc;
+      const double num = nd[0], den = nd[1];
       const bool first = !h->have_prev;
       h->have_prev = true;
       *out = first ? INFINITY : (den > 0 ? std::sqrt(num / den) : (num > 0 ? INFINITY : 0.0));
@@ -1023,7 +1104,7 @@ int imexlb_reduce_async(imexlb_lattice* h, int kind, double* out) {
   const double* w = u + 2 * N;
   const double* p = u + 3 * N;
   double* part = h->red.p;
-  double* res = h->red.p + reduce_blocks();  // res[0..1]: sums, res[2]: the residual
+  double* res = h->red.p + 2 * reduce_blocks();  // res[0..1]: sums, res[2]: the residual
   double* val = res;
   switch (kind) {
     case IMEXLB_REDUCE_MASS:
@@ -1037,11 +1118,9 @@ int imexlb_reduce_async(imexlb_lattice* h, int kind, double* out) {
       break;
     case IMEXLB_REDUCE_RESIDUAL:
       if (!h->prev_mom.p) IMX_CUDA(h->prev_mom.alloc(3 * static_cast<size_t>(N), h->stream));
-      if (h->have_prev) {
-        IMX_CUDA(launch_reduce(RedKind::DiffSq, u, v, w, p, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N,
-                               part, res, h->stream));
-        IMX_CUDA(launch_reduce(RedKind::NormSq, u, v, w, p, nullptr, nullptr, nullptr, N, part, res + 1, h->stream));
-      }
+      if (h->have_prev)
+        IMX_CUDA(launch_residual_sums(u, v, w, h->prev_mom.p, h->prev_mom.p + N, h->prev_mom.p + 2 * N, N, part, res,
+                                      h->stream));
       IMX_CUDA(launch_residual_finish(res, h->have_prev ? 0 : 1, res + 2, h->stream));
       IMX_CUDA(cudaMemcpyAsync(h->prev_mom.p, u, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
       h->have_prev = true;
@@ -1064,7 +1143,8 @@ int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* byte
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
   if (device_bytes)
     *device_bytes = h->buf[0].n + h->buf[1].n + h->mom.n * 8 + h->prev_mom.n * 8 + h->usr.n + h->inlet.n * 8 +
-                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->red.n * 8 + h->drag_part.n * 8 + h->links.n * 4 +
+                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->face_codes.n * 4 + h->red.n * 8 + h->drag_part.n * 8 +
+                    h->links.n * 4 +
                     (h->rec[0].n + h->rec[1].n) * sizeof(uint16_t);
   if (bytes_per_cell_update) *bytes_per_cell_update = 2.0 * Q * h->L.elem;
   return IMEXLB_OK;
@@ -1239,6 +1319,38 @@ int imexlb_debug_solid_links(int nx, int ny, int nz, const uint8_t* fluid, uint3
     box[3 + d] = hi[d];
   }
   return IMEXLB_OK;
+}
+
+// Not part of include/imexlb.h: the reference cavity's face-code table in the
+// reference's slot keys (q + 27 (i + lx (j + ly k)) over the padded box), for
+// a CPU restatement of the step that resolves the boundary passes per link.
+// base_dim: the 6 face bases, then the 6 face widths.  Returns the number of
+// words (call with codes = NULL to size), or -1 when the table is not used.
+int64_t imexlb_debug_face_codes(int nx, int ny, int nz, int32_t* codes, int64_t max_words, int64_t* base_dim) {
+  if (nx < 2 || ny < 2 || nz < 2) return -1;
+  GhostPlan plan;
+  std::string err;
+  if (!build_ghost_plan_keys(IMEXLB_CAVITY, nx, ny, nz, nullptr, &plan, &err)) return -1;
+  const int64_t lx = nx + 2 * GHOST, ly = ny + 2 * GHOST;
+  auto key = [&](int q, int i, int j, int k) {
+    return q + static_cast<int64_t>(Q) * ((i + GHOST) + lx * ((j + GHOST) + ly * (k + GHOST)));
+  };
+  std::vector<int32_t> c;
+  int64_t base[6];
+  int32_t dim[6];
+  if (!face_codes_generic(nx, ny, nz, static_cast<int64_t>(Q) * lx * ly * (nz + 2 * GHOST), key, plan.tgt, plan.src, c,
+                          base, dim))
+    return -1;
+  if (codes) {
+    if (max_words < static_cast<int64_t>(c.size())) return -1;
+    std::copy(c.begin(), c.end(), codes);
+  }
+  if (base_dim)
+    for (int f = 0; f < 6; ++f) {
+      base_dim[f] = base[f];
+      base_dim[6 + f] = dim[f];
+    }
+  return static_cast<int64_t>(c.size());
 }
 
 // Not part of include/imexlb.h: lists the staged kernels' bulk copies so

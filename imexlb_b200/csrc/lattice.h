@@ -119,7 +119,24 @@ struct StepArgs {
   // read and of the buffer written (WallRecord)
   const uint16_t* rec_src = nullptr;
   uint16_t* rec_dst = nullptr;
+  // Reference cavity with the boundary passes resolved in the step kernel
+  // (FaceCodes): per face cell FACE_CODE_WORDS words, at
+  // face_base[face] + (b * face_dim[face] + a) * FACE_CODE_WORDS; null: the
+  // ghost-slot gather runs after each step instead
+  const int32_t* face_codes = nullptr;
+  int64_t face_base[6] = {};
+  int32_t face_dim[6] = {};
 };
+// A face cell's words in the face-code table: word q (for a population whose
+// pull leaves the box) names where the pulled value comes from --
+//   code >= 0   element `code` of the buffer the step reads (this step's
+//               post-collision value, or an unwritten ghost slot)
+//   code == -1  zero
+//   code <= -2  element (-code - 2) of the buffer the step writes (a ghost
+//               slot as it stood after the previous step)
+// -- and word 27 has bit q set when the step must also store that value in
+// the pulled slot of the buffer it reads (a later step's "previous" value).
+constexpr int FACE_CODE_WORDS = 28;
 // Bytes of the StepArgs prefix the staged kernels read, rounded to 16.
 constexpr size_t STAGED_ARGS_BYTES = (offsetof(StepArgs, src) + 15) & ~static_cast<size_t>(15);
 
@@ -220,6 +237,11 @@ cudaError_t launch_drag_links(Store st, const StepArgs& a, cudaStream_t s);
 // for the requested quantity; partial sums of `blocks` blocks go to scratch.
 enum class RedKind : int { Mass = 0, Kinetic = 1, DiffSq = 2, NormSq = 3, UMax = 4 };
 int reduce_blocks();
+// out[0] = sum |u - u2|^2, out[1] = sum |u|^2 in one pass (scratch: 2 values
+// per reduction block, 2 * reduce_blocks()).
+cudaError_t launch_residual_sums(const double* u, const double* v, const double* w, const double* u2,
+                                 const double* v2, const double* w2, int64_t n, double* scratch, double* out,
+                                 cudaStream_t s);
 // out = sqrt(nd[0] / nd[1]) with the residual's conventions (one thread).
 cudaError_t launch_residual_finish(const double* nd, int first, double* out, cudaStream_t s);
 cudaError_t launch_reduce(RedKind k, const double* u, const double* v, const double* w, const double* p,

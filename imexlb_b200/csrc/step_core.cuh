@@ -89,20 +89,24 @@ __device__ __forceinline__ double div3_rn(double x) {
 //   smaller neighbouring gap of q1, i.e. |r1| < d * gap_below(q1) / 2.  If q1 is
 //   further than one ulp away, |r1| exceeds that bound, so a wrong q1 is never
 //   accepted; rejected cases (ties, near-ties, tiny quotients) take
-//   __ddiv_rn.  The bound is a power of two times d, so it is exact.
+//   __ddiv_rn.  The bound is a power of two times d, so it is exact.  The test
+//   reads only the high word of q1: when its 20 high significand bits are not
+//   all zero q1 is no power of two, gap_below(q1) = ulp(q1) and the bound is
+//   d * 2^(E - 53), E the exponent of q1; the other quotients (a 2^-20
+//   fraction, powers of two among them) take __ddiv_rn.
 //   A zero numerator gives q1 = x exactly (IEEE: +-0 / d = +-0 for d > 0);
 //   it is common (a cell at rest has f = feq) and is returned without the
-//   division.
+//   division, as are an infinite numerator (+-inf / d = +-inf) and a NaN (the
+//   quotient is NaN) in a lattice that overflowed.
 __device__ __forceinline__ double div_rn(double x, double d, double z) {
   const double q0 = __dmul_rn(x, z);
   const double r0 = __fma_rn(-q0, d, x);
   const double q1 = __fma_rn(r0, z, q0);
   const double r1 = __fma_rn(-q1, d, x);
-  const long long bits = __double_as_longlong(q1);
-  const int e = static_cast<int>((bits >> 52) & 0x7ff);
-  const int he = e - 53 - ((bits & 0xFFFFFFFFFFFFFLL) == 0 ? 1 : 0);  // exponent field of gap_below / 2
-  if (he > 0 && fabs(r1) < __dmul_rn(d, __longlong_as_double(static_cast<long long>(he) << 52))) return q1;
-  if (x == 0.0) return x;
+  const int hi = __double2hiint(q1);
+  const int he = (hi & 0x7ff00000) - (53 << 20);  // exponent field of ulp(q1) / 2, in the high word
+  if (he > 0 && (hi & 0x000fffff) != 0 && fabs(r1) < __dmul_rn(d, __hiloint2double(he, 0))) return q1;
+  if (x == 0.0 || !isfinite(x)) return x;
   return __ddiv_rn(x, d);
 }
 
@@ -268,8 +272,36 @@ __device__ __forceinline__ void load_cell(const StepArgs& a, const P& pl, const 
   using R = typename StoreT<S>::R;
   const int32_t b = a.base32 + k * a.sz32 + j * a.pitch32 + i;
   if constexpr (B == Bc::Ghost) {
+    if constexpr (RULE == CaseRule::CavityRef) {
+      const unsigned wf = a.face_codes ? wall_flags(a, i, j, k) : 0u;
+      if (wf != 0u) {
+        // a face cell of the reference cavity: the boundary passes resolved
+        // per link (the face-code table, lattice.h); links that stay inside
+        // pull their neighbour as usual
+        using T = typename StoreT<S>::T;
+        const int face = __ffs(static_cast<int>(wf)) - 1;
+        const int fa = face < 2 ? j : i, fb = face < 4 ? k : j;
+        const int32_t* codes =
+            a.face_codes + a.face_base[face] + (static_cast<int64_t>(fb) * a.face_dim[face] + fa) * FACE_CODE_WORDS;
+        const uint32_t keep = static_cast<uint32_t>(__ldg(codes + Q));
+        const T* in = static_cast<const T*>(a.src);
+        const T* out = static_cast<const T*>(a.dst);
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          if (leaves<q>(wf)) {
+            const int32_t c = __ldg(codes + q);
+            const T v = c >= 0 ? __ldg(in + c) : (c == -1 ? T(0) : out[-static_cast<int64_t>(c) - 2]);
+            if ((keep >> q) & 1u) const_cast<T*>(in)[q * a.sq + b + a.rel[q]] = v;
+            f[q] = decode<S>(v, q, a.enc);
+          } else {
+            f[q] = decode<S>(pl.load(q, b + a.rel[q]), q, a.enc);
+          }
+        });
+        return;
+      }
+    }
     // reference boundaries: the ghost slots the pull reaches were filled by
-    // the ghost-slot gather after the previous step
+    // the ghost-slot gather after the previous step (or the cell is inside)
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = decode<S>(pl.load(q, b + a.rel[q]), q, a.enc);

@@ -189,7 +189,7 @@ class Server:
             r = float(res[slot])
             # retire at the step count, at the tolerance, or when the lattice
             # diverged (NaN); the first check after admission reads +inf
-            if done >= req.max_steps or r < req.tol or math.isnan(r):
+            if done >= req.max_steps or 0 <= r < req.tol or math.isnan(r):
                 f = None if math.isnan(r) else self.eng.fields(slot)
                 self.eng.remove(slot)
                 del self.active[slot]
@@ -205,7 +205,8 @@ class Server:
 def status_of(req: Request, steps: int, residual: float) -> str:
     if math.isnan(residual):
         return "diverged"
-    return "converged" if residual < req.tol and steps < req.max_steps else "steps"
+    # a negative residual: the instance took no step since the last check
+    return "converged" if 0 <= residual < req.tol and steps < req.max_steps else "steps"
 
 
 def serve(requests: list[Request], storage: str = "f16", keep_fields=False, **kw) -> dict:

@@ -45,7 +45,8 @@ def run(storage: str, n=(768, 192, 192), D: float = 32.0, centre=(192.0, 96.0, 9
         fields = lbm.fields()
     tail = cds[-max(1, len(cds) // 10):]
     return dict(storage=storage, steps=steps, cd_last=cds[-1], cd_tail_mean=float(np.mean(tail)),
-                cd_tail_std=float(np.std(tail)), seconds=time.perf_counter() - t0, fields=fields)
+                cd_tail_std=float(np.std(tail)), seconds=time.perf_counter() - t0, fields=fields,
+                cd_every=every, cd_series=[round(c, 6) for c in cds])
 
 
 def main(argv=None) -> int:
@@ -53,17 +54,25 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=30000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--storages", default="f64,f16,bf16")
+    ap.add_argument("--out", default=None, help="also write the JSON lines (with the Cd series) to this file")
     args = ap.parse_args(argv)
     results = {}
     for st in args.storages.split(","):
         results[st] = run(st, steps=args.steps, every=args.every)
     ref = results.get("f64")
+    lines = []
     for st, r in results.items():
         line = {k: v for k, v in r.items() if k != "fields"}
+        line.update(lattice=[768, 192, 192], sphere_d=32.0, sphere_c=[192.0, 96.0, 96.0], inlet_u=0.05, Re=100.0)
         if ref is not None and st != "f64":
             line["velocity_l2_vs_f64"] = velocity_l2(r["fields"], ref["fields"])
             line["cd_rel_err_vs_f64"] = abs(r["cd_tail_mean"] - ref["cd_tail_mean"]) / abs(ref["cd_tail_mean"])
-        print(json.dumps(line), flush=True)
+        print(json.dumps({k: v for k, v in line.items() if k != "cd_series"}), flush=True)
+        lines.append(line)
+    if args.out:
+        with open(args.out, "w") as fh:
+            for line in lines:
+                fh.write(json.dumps(line) + "\n")
     return 0
 
 

@@ -301,14 +301,18 @@ int imexlb_engine_step(imexlb_engine* e, int nsteps);
 /* Step limit of one instance: it takes at most `steps` more steps (< 0: no
  * limit, the default at admission), then stays as it is while the others go
  * on; its u, v, w, p views are written at its last step.  A serving loop can
- * so run fixed-length step calls over requests of any step count. */
+ * so run fixed-length step calls over requests of any step count.  The new
+ * limit applies from the next imexlb_engine_step call on (steps already
+ * queued keep the old one); the call does not wait for the GPU. */
 int imexlb_engine_limit(imexlb_engine* e, int slot, int steps);
 /* u, v, w, p of one instance after the last step (host arrays, x fastest). */
 int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, double* w, double* p);
 /* Velocity residual per slot, sqrt(sum|u - u_prev|^2 / sum|u|^2) between this
- * call and the previous one (INFINITY on an instance's first call, NaN for
- * empty slots or a non-finite lattice); out has max_instances entries.  Call
- * it right after imexlb_engine_step. */
+ * call and the previous one (INFINITY on an instance's first call, -1 for an
+ * instance that took no step since the previous call -- it stopped at its
+ * step limit, which is not convergence --, NaN for empty slots or a
+ * non-finite lattice); out has max_instances entries.  Call it right after
+ * imexlb_engine_step. */
 int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out);
 int imexlb_engine_info(const imexlb_engine* e, imexlb_engine_stats* st);
 /* Arena bytes one instance needs in a given storage format. */

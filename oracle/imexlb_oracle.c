@@ -827,7 +827,9 @@ int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbac
     }
     const long e = (t % 1009 == 0) ? -1000 : (long)((s >> 52) % 121) - 60;
     cv.u = ((s >> 63) << 63) | ((unsigned long long)(1023 + e) << 52) | (s & 0xFFFFFFFFFFFFFULL);
-    const double x = (t % 997 == 0) ? ((t & 1) ? -0.0 : 0.0) : cv.v; /* zeros of both signs */
+    double x = (t % 997 == 0) ? ((t & 1) ? -0.0 : 0.0) : cv.v; /* zeros of both signs */
+    if (t % 1013 == 0) x = (t & 1) ? -INFINITY : INFINITY;
+    if (t % 1019 == 0) x = NAN;
     const double q0 = x * z;
     const double r0 = fma(-q0, d, x);
     const double q1 = fma(r0, z, q0);
@@ -836,29 +838,30 @@ int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbac
       double v;
       unsigned long long u;
     } qb = {q1};
-    const int ef = (int)((qb.u >> 52) & 0x7ff);
-    const int he = ef - 53 - ((qb.u & 0xFFFFFFFFFFFFFULL) == 0 ? 1 : 0);
+    /* the device's test on the high word of q1 (step_core.cuh div_rn) */
+    const int hi = (int)(qb.u >> 32);
+    const int he = (hi & 0x7ff00000) - (53 << 20);
     double q;
     int accept = 0;
-    if (he > 0) {
+    if (he > 0 && (hi & 0x000fffff) != 0) {
       union {
         unsigned long long u;
         double v;
-      } hg = {(unsigned long long)he << 52};
+      } hg = {(unsigned long long)(unsigned)he << 32};
       accept = fabs(r1) < d * hg.v;
     }
     if (planted) {
       q = q0;
     } else if (accept) {
       q = q1;
-    } else if (x == 0.0) {
-      q = x; /* +-0 / d = +-0 for d > 0 */
+    } else if (x == 0.0 || !isfinite(x)) {
+      q = x; /* +-0 / d = +-0, +-inf / d = +-inf for d > 0; NaN stays NaN */
     } else {
       q = x / d;
       ++fb;
     }
     const double want = x / d;
-    if (memcmp(&q, &want, sizeof q) != 0) ++bad; /* bit patterns: a zero's sign counts */
+    if (isnan(want) ? !isnan(q) : memcmp(&q, &want, sizeof q) != 0) ++bad; /* bit patterns: a zero's sign counts */
   }
   if (fallbacks) *fallbacks = fb;
   return bad;

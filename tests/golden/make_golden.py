@@ -113,9 +113,23 @@ def configs(names=None):
                              tau=s["tau"], **field_summary(r))
         print(name, "ok", entries[name].get("kinetic"), entries[name]["nonfinite_values"])
     manifest["configs"] = entries
+    if not names or "sphere_mask_shipped" in names:
+        manifest["sphere_mask_shipped"] = shipped_sphere_mask()
     with open(path, "w") as fh:
         json.dump(manifest, fh, indent=1, sort_keys=True)
     print("wrote", path)
+
+
+def shipped_sphere_mask() -> dict:
+    """The reference's solid mask usr (sphere/src/lbm.cpp:238) for the
+    shipped sphere input.in (512 x 128 x 128): SHA-256 of the interior as
+    int32 (nz, ny, nx), the solid cell count and the solid box."""
+    r = run_reference_case("sphere", 1.0, 8.0, 100, 0.1, 512, 128, 128, 0, want_f=False, fast=True)
+    usr = np.ascontiguousarray(r["usr"][3:-3, 3:-3, 3:-3], dtype=np.int32)
+    solid = np.argwhere(usr == 0)
+    return dict(nx=512, ny=128, nz=128, input=["1.0", "8.0", "100", "0.1", "100", "10", "512", "128", "128"],
+                usr_sha256=sha(usr), solid_cells=int((usr == 0).sum()),
+                solid_box_zyx=[solid.min(axis=0).tolist(), solid.max(axis=0).tolist()])
 
 
 def main(refroot: str | None = None):

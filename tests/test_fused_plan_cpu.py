@@ -3,10 +3,13 @@
 The device runs each step as  pull -> moments -> case rules -> collide  into a
 second buffer, followed (reference boundaries) by one gather that applies the
 ghost-slot plan the library derives from the reference's boundary passes
-(imexlb_ghost_plan, host-only).  This test restates exactly that algorithm in
-numpy with the kernel's FP64 operation order, drives it with the library's
-own plan, and requires bit-identical moments against the oracle's literal
-Collision / halo / Streaming / Update sequence.  No GPU is involved.
+(imexlb_ghost_plan, host-only) -- or, for the reference cavity in FP64 and
+FP32 storage, with the passes resolved per link inside the step from the
+library's face-code table (imexlb_debug_face_codes).  This test restates
+both forms in numpy with the kernel's FP64 operation order, drives them with
+the library's own plan and table, and requires bit-identical moments
+against the oracle's literal Collision / halo / Streaming / Update sequence.
+No GPU is involved.
 """
 import numpy as np
 import pytest
@@ -42,14 +45,67 @@ def gather(Y, X, tgt, src):
     Y[tgt] = vals
 
 
-def emulate(case, nx, ny, nz, tau0, rho0, u0, steps, ran=None):
+def face_codes(nx, ny, nz):
+    """The reference cavity's face-code table in reference slot keys
+    (imexlb_debug_face_codes): per face cell, the source of each link that
+    leaves the box, and the links whose value the step also stores."""
+    import ctypes
+
+    lib = api.load_library()
+    fn = lib.imexlb_debug_face_codes
+    fn.restype = ctypes.c_int64
+    fn.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    n = fn(nx, ny, nz, None, 0, None)
+    assert n > 0
+    codes = np.empty(n, dtype=np.int32)
+    bd = np.empty(12, dtype=np.int64)
+    assert fn(nx, ny, nz, codes.ctypes.data, n, bd.ctypes.data) == n
+    return codes, bd[:6], bd[6:]
+
+
+def resolve_faces(cur, nxt, f, nx, ny, nz, codes, base, dim):
+    """The step kernel's per-link form of the boundary passes: a face cell's
+    link that leaves the box takes cur[code] (code >= 0), zero (-1) or
+    nxt[-code - 2], and the links marked in word 27 store that value into
+    their pulled slot of cur (after every read, as no read in the step
+    touches those slots)."""
+    lx, ly = nx + 6, ny + 6
+    writes = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                wf = (i == 0) | (i == nx - 1) << 1 | (j == 0) << 2 | (j == ny - 1) << 3 | (k == 0) << 4 | \
+                     (k == nz - 1) << 5
+                if not wf:
+                    continue
+                face = (wf & -wf).bit_length() - 1
+                fa, fb = (j if face < 2 else i), (k if face < 4 else j)
+                w = codes[base[face] + (fb * dim[face] + fa) * 28:][:28]
+                for q in range(Q):
+                    out = (EX[q] > 0 and wf & 1) or (EX[q] < 0 and wf & 2) or (EY[q] > 0 and wf & 4) or \
+                          (EY[q] < 0 and wf & 8) or (EZ[q] > 0 and wf & 16) or (EZ[q] < 0 and wf & 32)
+                    if not out:
+                        continue
+                    c = int(w[q])
+                    v = cur[c] if c >= 0 else (0.0 if c == -1 else nxt[-c - 2])
+                    f[q][k, j, i] = v
+                    if (int(w[27]) >> q) & 1:
+                        writes.append((q + Q * ((i - EX[q] + 3) + lx * ((j - EY[q] + 3) + ly * (k - EZ[q] + 3))), v))
+    for key, v in writes:
+        cur[key] = v
+
+
+def emulate(case, nx, ny, nz, tau0, rho0, u0, steps, ran=None, per_link=False):
     o = Oracle(case, nx, ny, nz, tau0, rho0, u0, ran)
     o.initialize()
     f0 = o.f_padded().reshape(-1)
     usr = o.usr_padded()
     tgt, src = api.ghost_plan(case, nx, ny, nz, usr if case == "sphere" else None)
     A, B = f0.copy(), f0.copy()
-    gather(A, B, tgt, src)
+    if per_link:
+        codes, base, dim = face_codes(nx, ny, nz)
+    else:
+        gather(A, B, tgt, src)
     lx, ly, lz = nx + 6, ny + 6, nz + 6
     th = tau0 + 0.5
     m_int = usr[3:3 + nz, 3:3 + ny, 3:3 + nx]
@@ -60,6 +116,8 @@ def emulate(case, nx, ny, nz, tau0, rho0, u0, steps, ran=None):
         X4 = cur.reshape(lz, ly, lx, Q)
         f = [X4[3 - EZ[q]:3 - EZ[q] + nz, 3 - EY[q]:3 - EY[q] + ny, 3 - EX[q]:3 - EX[q] + nx, q].copy()
              for q in range(Q)]
+        if per_link:
+            resolve_faces(cur, nxt, f, nx, ny, nz, codes, base, dim)
         p = np.zeros((nz, ny, nx))
         u = np.zeros((nz, ny, nx))
         v = np.zeros((nz, ny, nx))
@@ -88,7 +146,8 @@ def emulate(case, nx, ny, nz, tau0, rho0, u0, steps, ran=None):
             e = edu(q, u, v, w)
             feq = tp3[CLS[q]] + W[CLS[q]] * (((3.0 * e) + (4.5 * (e * e))) - udu15)
             Y4[3:3 + nz, 3:3 + ny, 3:3 + nx, q] = f[q] - ((f[q] - feq) / th)
-        gather(nxt, cur, tgt, src)
+        if not per_link:
+            gather(nxt, cur, tgt, src)
         cur, nxt = nxt, cur
     return (u, v, w, p), o
 
@@ -112,6 +171,19 @@ def test_fused_reformulation_matches_oracle(case, rho0, R, Re, u0, nx, ny, nz, s
         # buffer with the periodic wrap the reference's self-exchange makes
         pytest.skip("periodic case is covered by the GPU parity tests")
     got, o = emulate(case, nx, ny, nz, tau, rho0, u0, steps, ran)
+    o.step(steps)
+    for name, g, want in zip("uvwp", got, o.moments()):
+        assert np.array_equal(g, want), f"{name}: max |diff| {np.abs(g - want).max()}"
+
+
+@pytest.mark.parametrize("nx,ny,nz,R,Re,steps", [(8, 8, 8, 8.0, 100, 20), (9, 7, 10, 6.0, 40, 13),
+                                                 (12, 10, 9, 10.0, 400, 30)])
+def test_per_link_boundaries_match_oracle(nx, ny, nz, R, Re, steps):
+    """The reference cavity with its boundary passes resolved per link in the
+    step (the face-code table the library builds for its FP64 / FP32 step
+    kernel) instead of the gather: bit-identical to the oracle."""
+    tau = oracle_system("cavity", 1.0, R, Re, 0.1, steps, 1, nx)["tau"]
+    got, o = emulate("cavity", nx, ny, nz, tau, 1.0, 0.1, steps, per_link=True)
     o.step(steps)
     for name, g, want in zip("uvwp", got, o.moments()):
         assert np.array_equal(g, want), f"{name}: max |diff| {np.abs(g - want).max()}"

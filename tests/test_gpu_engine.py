@@ -165,3 +165,23 @@ def test_step_limits_stop_instances_at_their_own_count(api, storage, arith):
     want = alone(api, c, n, tau, u0, kw, 12, storage, arith)
     for k in "uvwp":
         assert np.array_equal(resumed[k], want[k]), k
+
+
+def test_stopped_instance_reports_negative_residual(api):
+    """An instance that took no step since the previous check (stopped at
+    its step limit) reports -1, not a residual of 0 that would read as
+    convergence; raising its limit brings real residuals back."""
+    d = api.instance_desc("cavity", 32, 32, 32, 0.03, 1.0, 0.1, lid_u=0.1)
+    with api.Engine(storage="f16", budget_bytes=1 << 30, max_instances=4) as eng:
+        a, b = eng.add(d), eng.add(d)
+        eng.limit(a, 10)
+        eng.step(20)
+        r = eng.residuals()
+        assert np.isinf(r[a]) and np.isinf(r[b])
+        eng.step(20)
+        r = eng.residuals()
+        assert r[a] == -1.0 and 0.0 < r[b] < 1.0
+        eng.limit(a, None)
+        eng.step(20)
+        r = eng.residuals()
+        assert 0.0 < r[a] < 1.0 and 0.0 < r[b] < 1.0

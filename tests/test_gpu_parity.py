@@ -121,3 +121,31 @@ def test_mass_conserved_tgv(api):
         lbm.step(200)
         m1 = lbm.reduce("mass")
     assert abs(m1 - m0) <= 1e-10 * abs(m0)
+
+
+def test_mask_matches_reference_for_the_shipped_sphere(api, golden_dir):
+    """imexlb_get_mask for the shipped sphere input.in (512 x 128 x 128, R = 8)
+    equals the reference's usr (sphere/src/lbm.cpp:238) bit for bit: its
+    digest, solid count and solid box as the reference computed them."""
+    import hashlib
+
+    m = json.load(open(os.path.join(golden_dir, "manifest.json")))["sphere_mask_shipped"]
+    tau = oracle_system("sphere", 1.0, 8.0, 100, 0.1, 100, 10, 512)["tau"]
+    with api.LBM("sphere", m["nx"], m["ny"], m["nz"], tau, 1.0, 0.1) as lbm:
+        mask = np.ascontiguousarray(lbm.mask(), dtype=np.int32)
+    assert int((mask == 0).sum()) == m["solid_cells"]
+    solid = np.argwhere(mask == 0)
+    assert [solid.min(axis=0).tolist(), solid.max(axis=0).tolist()] == m["solid_box_zyx"]
+    assert hashlib.sha256(mask.tobytes()).hexdigest() == m["usr_sha256"]
+
+
+@pytest.mark.parametrize("n", [(72, 12, 12), (100, 20, 20), (129, 24, 22)])
+def test_mask_matches_oracle(api, n):
+    nx, ny, nz = n
+    o = Oracle("sphere", nx, ny, nz, 0.02, 1.0, 0.1)
+    o.initialize()
+    want = o.usr_padded()[3:-3, 3:-3, 3:-3]
+    with api.LBM("sphere", nx, ny, nz, 0.02, 1.0, 0.1) as lbm:
+        got = lbm.mask()
+    assert np.array_equal(got, want)
+    assert (got == 0).any()

@@ -40,7 +40,7 @@ def test_cavity_at_rest_stays_at_rest(api, storage, arith):
         assert np.all(f[k] == 0.0), (storage, k)
 
 
-@pytest.mark.parametrize("storage,tol", [("f64", 1e-14), ("f32", 1e-7), ("f16", 1e-7), ("bf16", 1e-7)])
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-14), ("f32", 1e-7), ("f16", 2e-6), ("bf16", 2e-6)])
 def test_channel_without_solid_stays_uniform(api, storage, tol):
     with api.LBM("sphere", 64, 16, 18, 0.05, 1.0, 0.05, bc="standard", storage=storage, arith="fast",
                  inlet_u=0.05, sphere_d=1e-3, sphere_c=(10.5, 6.5, 7.5)) as lbm:
