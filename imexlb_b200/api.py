@@ -79,9 +79,11 @@ EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imex
            "imexlb_get_fields", "imexlb_get_fields_async", "imexlb_get_mask", "imexlb_write_tecplot", "imexlb_reduce",
            "imexlb_reduce_async", "imexlb_reduce_fields_noalloc", "imexlb_release_cached_memory", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
-           "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_destroy", "imexlb_last_error",
+           "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_set_wait_limit",
+           "imexlb_destroy", "imexlb_last_error",
            "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_add_as", "imexlb_engine_remove",
-           "imexlb_engine_step", "imexlb_engine_limit", "imexlb_engine_fields", "imexlb_engine_residuals", "imexlb_engine_info",
+           "imexlb_engine_step", "imexlb_engine_limit", "imexlb_engine_fields", "imexlb_engine_plane",
+           "imexlb_engine_residuals", "imexlb_engine_info",
            "imexlb_engine_instance_bytes", "imexlb_engine_checkpoint_size", "imexlb_engine_checkpoint_save",
            "imexlb_engine_restore", "imexlb_engine_synchronize", "imexlb_engine_destroy"]
 
@@ -124,6 +126,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_profile.argtypes = [vp, i]
     lib.imexlb_profile_read.argtypes = [vp, ctypes.POINTER(KernelTimes)]
     lib.imexlb_synchronize.argtypes = [vp]
+    lib.imexlb_set_wait_limit.argtypes = [vp, ctypes.c_double]
     lib.imexlb_destroy.argtypes = [vp]
     lib.imexlb_destroy.restype = None
     lib.imexlb_last_error.restype = ctypes.c_char_p
@@ -135,6 +138,7 @@ def load_library() -> ctypes.CDLL:
     lib.imexlb_engine_step.argtypes = [vp, i]
     lib.imexlb_engine_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.imexlb_engine_fields.argtypes = [vp, i, vp, vp, vp, vp]
+    lib.imexlb_engine_plane.argtypes = [vp, i, i, vp, vp, vp, vp]
     lib.imexlb_engine_residuals.argtypes = [vp, vp, i]
     lib.imexlb_engine_info.argtypes = [vp, ctypes.POINTER(EngineStats)]
     lib.imexlb_engine_instance_bytes.argtypes = [i, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_size_t)]
@@ -228,6 +232,11 @@ class LBM:
 
     def synchronize(self):
         _check(self.lib.imexlb_synchronize(self.h))
+
+    def set_wait_limit(self, seconds: float):
+        """Bound on the 2-byte staged kernels' waits for their row copies
+        (imexlb_set_wait_limit)."""
+        _check(self.lib.imexlb_set_wait_limit(self.h, seconds))
 
     def fields(self, out: dict | None = None, wait: bool = True) -> dict:
         """ua, va, wa, p after the last step, each shaped (nz, ny, nx).  With
@@ -407,6 +416,14 @@ class Engine:
             out = {k: np.empty((nz, ny, nx)) for k in ("u", "v", "w", "p")}
         _check(self.lib.imexlb_engine_fields(self.h, slot, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]),
                                              _ptr(out["p"])))
+        return out
+
+    def plane(self, slot: int, k: int) -> dict:
+        """u, v, w, p of one z plane of an instance, each (ny, nx)."""
+        nx, ny, nz = self.shapes[slot]
+        out = {c: np.empty((ny, nx)) for c in ("u", "v", "w", "p")}
+        _check(self.lib.imexlb_engine_plane(self.h, slot, k, _ptr(out["u"]), _ptr(out["v"]), _ptr(out["w"]),
+                                            _ptr(out["p"])))
         return out
 
     def residuals(self) -> np.ndarray:

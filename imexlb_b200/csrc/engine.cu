@@ -1154,6 +1154,21 @@ int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, doubl
   return sync_checked(e);
 }
 
+int imexlb_engine_plane(imexlb_engine* e, int slot, int k, double* u, double* v, double* w, double* p) {
+  if (!e || slot < 0 || slot >= static_cast<int>(e->slots.size()) || !e->slots[slot].used)
+    return efail(IMEXLB_E_ARG, "no such instance");
+  const Slot& sl = e->slots[slot];
+  if (k < 0 || k >= sl.d.nz) return efail(IMEXLB_E_ARG, "plane index outside the lattice");
+  const EngInst& in = e->h_inst[slot];
+  const size_t plane = static_cast<size_t>(sl.d.nx) * sl.d.ny;
+  double* dst[4] = {u, v, w, p};
+  double* src[4] = {in.a.mu, in.a.mv, in.a.mw, in.a.mp};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c])
+      IMX_ECUDA(cudaMemcpyAsync(dst[c], src[c] + plane * k, plane * 8, cudaMemcpyDeviceToHost, e->stream));
+  return sync_checked(e);
+}
+
 int imexlb_engine_residuals(imexlb_engine* e, double* out, int n_out) {
   if (!e || !out) return efail(IMEXLB_E_ARG, "null argument");
   if (n_out < static_cast<int>(e->slots.size())) return efail(IMEXLB_E_ARG, "output shorter than max_instances");

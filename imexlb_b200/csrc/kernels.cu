@@ -94,9 +94,28 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
   constexpr int CPT = CellsPerThread<S>::value;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * CPT;
-  const int k = blockIdx.z;
+  int k = blockIdx.z;
   double drag[3] = {0.0, 0.0, 0.0};
   const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
+  if constexpr (RULE == CaseRule::CavityRef) {
+    // reference cavity with per-link boundaries: the first face_layers
+    // z-layers of blocks take the face cells, one a thread, from the face
+    // list (scheduled first, they run alongside the inside blocks)
+    if (k < a.face_layers) {
+      const int64_t e = ((static_cast<int64_t>(k) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) *
+                            (blockDim.x * blockDim.y) +
+                        threadIdx.y * blockDim.x + threadIdx.x;
+      if (e < a.n_face) {
+        const int32_t c = a.face_cells[e];
+        const int fi = c % a.nx, fj = (c / a.nx) % a.ny, fk = c / (a.nx * a.ny);
+        typename StoreT<S>::R f[Q];
+        load_cell<S, B, RULE, EXACT, DRAG>(a, pl, fi, fj, fk, f, drag);
+        compute_cell<S, RULE, EXACT>(a, pl, fi, fj, fk, f);
+      }
+      return;
+    }
+    k -= a.face_layers;
+  }
   step_cells<S, B, RULE, EXACT, DRAG>(a, pl, i, j0, k, drag);
 
   if constexpr (DRAG) {
@@ -192,7 +211,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       // has released it; the decision to stop is warp-uniform
       const int tn = t + (NS - 1) * grid;
       if (tn < ntiles) {
-        if (i > 0 && !__all_sync(0xffffffffu, bar_wait(&empty[(i - 1) % NS], ((i - 1) / NS) & 1u))) {
+        if (i > 0 && !__all_sync(0xffffffffu, bar_wait_for(&empty[(i - 1) % NS], ((i - 1) / NS) & 1u, a.wait_ns))) {
           *abort_v = 1;
           break;
         }
@@ -202,7 +221,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
         ++issued;
       }
     }
-    if (!__all_sync(0xffffffffu, bar_wait(&full[s], (i / NS) & 1u))) {
+    if (!__all_sync(0xffffffffu, bar_wait_for(&full[s], (i / NS) & 1u, a.wait_ns))) {
       *abort_v = 1;
       break;
     }
@@ -213,7 +232,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
   }
   if (warp == 0 && lane == 0 && *abort_v) {
-    // let copies still in flight land before the block exits (bounded)
+    // let copies still in flight land before the block exits (bounded by the
+    // full second whatever a.wait_ns is)
     for (int m = i; m < issued; ++m) (void)bar_wait(&full[m % NS], (m / NS) & 1u);
   }
   __syncthreads();
@@ -739,7 +759,17 @@ static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
   }
   const dim3 block = step_block(a.nx);
   const int rows = block.y * CellsPerThread<S>::value;
-  const dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);
+  dim3 grid((a.nx + block.x - 1) / block.x, (a.ny + rows - 1) / rows, a.nz);
+  if constexpr (R == CaseRule::CavityRef) {
+    if (a.face_cells) {
+      // the face blocks: leading z-layers of the grid, one face cell a thread
+      StepArgs fa = a;
+      const int64_t per_layer = static_cast<int64_t>(grid.x) * grid.y * block.x * block.y;
+      fa.face_layers = static_cast<int32_t>((a.n_face + per_layer - 1) / per_layer);
+      grid.z += fa.face_layers;
+      return launch_pdl(step_kernel<S, B, R, EXACT, false>, grid, block, 0, s, fa);
+    }
+  }
   if constexpr (R == CaseRule::SphereStd && S != Store::F16 && S != Store::BF16) {
     if (a.drag_part) {
       return launch_pdl(step_kernel<S, B, R, EXACT, true>, grid, block, 0, s, a);

@@ -577,6 +577,71 @@ bool face_codes_for(const Layout& L, const std::vector<int64_t>& tgt, const std:
                             dim);
 }
 
+// The device-side form of the reference boundary passes for one lattice
+// shape: the ghost-slot plan in device indices, and for the cavity in FP64
+// or FP32 storage the face-code table and face-cell list that replace it.
+// It depends only on the case, the extents and the storage width (the
+// reference sphere's mask is a function of the extents), so the last few
+// are kept for the lattices created after them.
+struct GhostSetup {
+  int kase = 0, nx = 0, ny = 0, nz = 0, elem = 0;
+  std::vector<int64_t> t, s;
+  bool faces = false;
+  std::vector<int32_t> codes, cells;
+  int64_t base[6] = {};
+  int32_t dim[6] = {};
+};
+
+std::mutex g_setup_mu;
+std::vector<std::shared_ptr<const GhostSetup>> g_setups;  // most recent last
+constexpr size_t SETUP_CACHE = 4;
+
+std::shared_ptr<const GhostSetup> ghost_setup(const imexlb_params& P, const Layout& L, const int32_t* usr_padded,
+                                              std::string* err) {
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    for (const auto& g : g_setups)
+      if (g->kase == P.kase && g->nx == P.nx && g->ny == P.ny && g->nz == P.nz && g->elem == L.elem) return g;
+  }
+  GhostPlan plan;
+  if (!build_ghost_plan_keys(static_cast<int>(P.kase), P.nx, P.ny, P.nz, usr_padded, &plan, err)) return nullptr;
+  auto g = std::make_shared<GhostSetup>();
+  g->kase = P.kase;
+  g->nx = P.nx;
+  g->ny = P.ny;
+  g->nz = P.nz;
+  g->elem = L.elem;
+  const int lx = P.nx + 2 * GHOST, ly = P.ny + 2 * GHOST;
+  auto to_dev = [&](int64_t key) {
+    const int q = static_cast<int>(key % Q);
+    int64_t c = key / Q;
+    const int i = static_cast<int>(c % lx);
+    c /= lx;
+    const int j = static_cast<int>(c % ly);
+    const int k = static_cast<int>(c / ly);
+    return L.idx(q, i, j, k);
+  };
+  g->t.resize(plan.tgt.size());
+  g->s.resize(plan.src.size());
+  for (size_t n = 0; n < g->t.size(); ++n) {
+    g->t[n] = to_dev(plan.tgt[n]);
+    const int64_t src = plan.src[n];
+    g->s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
+  }
+  if (P.kase == IMEXLB_CAVITY && (L.elem == 8 || L.elem == 4) && face_codes_for(L, g->t, g->s, g->codes, g->base, g->dim)) {
+    g->faces = true;
+    for (int k = 0; k < P.nz; ++k)
+      for (int j = 0; j < P.ny; ++j)
+        for (int i = 0; i < P.nx; ++i)
+          if (i == 0 || i == P.nx - 1 || j == 0 || j == P.ny - 1 || k == 0 || k == P.nz - 1)
+            g->cells.push_back(i + P.nx * (j + P.ny * k));
+  }
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  g_setups.push_back(g);
+  if (g_setups.size() > SETUP_CACHE) g_setups.erase(g_setups.begin());
+  return g;
+}
+
 }  // namespace
 
 extern "C" {
@@ -794,40 +859,30 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   }
 
   if (ghost) {
-    GhostPlan plan;
     std::string err;
-    if (!build_ghost_plan_keys(static_cast<int>(P.kase), P.nx, P.ny, P.nz,
-                               P.kase == IMEXLB_SPHERE ? h->usr_padded.data() : nullptr, &plan, &err))
-      return fail(IMEXLB_E_UNSUPPORTED, err);
-    const int lx = P.nx + 2 * GHOST, ly = P.ny + 2 * GHOST;
-    auto to_dev = [&](int64_t key) {
-      const int q = static_cast<int>(key % Q);
-      int64_t c = key / Q;
-      const int i = static_cast<int>(c % lx);
-      c /= lx;
-      const int j = static_cast<int>(c % ly);
-      const int k = static_cast<int>(c / ly);
-      return L.idx(q, i, j, k);
-    };
-    std::vector<int64_t> t(plan.tgt.size()), s(plan.src.size());
-    for (size_t n = 0; n < t.size(); ++n) {
-      t[n] = to_dev(plan.tgt[n]);
-      const int64_t src = plan.src[n];
-      s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
-    }
-    std::vector<int32_t> codes;
-    if (P.kase == IMEXLB_CAVITY && (P.storage == IMEXLB_F64 || P.storage == IMEXLB_F32) &&
-        face_codes_for(L, t, s, codes, a.face_base, a.face_dim)) {
-      // the step kernel resolves the passes per link: no gather
-      IMX_CUDA(h->face_codes.alloc(codes.size(), h->stream));
-      IMX_CUDA(cudaMemcpy(h->face_codes.p, codes.data(), codes.size() * 4, cudaMemcpyHostToDevice));
+    const std::shared_ptr<const GhostSetup> g =
+        ghost_setup(P, L, P.kase == IMEXLB_SPHERE ? h->usr_padded.data() : nullptr, &err);
+    if (!g) return fail(IMEXLB_E_UNSUPPORTED, err);
+    if (g->faces) {
+      // the step kernel resolves the passes per link: no gather; its face
+      // blocks take the face cells, listed plane by plane and row by row
+      IMX_CUDA(h->face_codes.alloc(g->codes.size() + g->cells.size(), h->stream));
+      IMX_CUDA(cudaMemcpy(h->face_codes.p, g->codes.data(), g->codes.size() * 4, cudaMemcpyHostToDevice));
+      IMX_CUDA(cudaMemcpy(h->face_codes.p + g->codes.size(), g->cells.data(), g->cells.size() * 4,
+                          cudaMemcpyHostToDevice));
       a.face_codes = h->face_codes.p;
+      a.face_cells = h->face_codes.p + g->codes.size();
+      a.n_face = static_cast<int32_t>(g->cells.size());
+      for (int f = 0; f < 6; ++f) {
+        a.face_base[f] = g->base[f];
+        a.face_dim[f] = g->dim[f];
+      }
     } else {
-      h->gn = static_cast<int64_t>(t.size());
-      IMX_CUDA(h->gtgt.alloc(t.size(), h->stream));
-      IMX_CUDA(h->gsrc.alloc(s.size(), h->stream));
-      IMX_CUDA(cudaMemcpy(h->gtgt.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
-      IMX_CUDA(cudaMemcpy(h->gsrc.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice));
+      h->gn = static_cast<int64_t>(g->t.size());
+      IMX_CUDA(h->gtgt.alloc(g->t.size(), h->stream));
+      IMX_CUDA(h->gsrc.alloc(g->s.size(), h->stream));
+      IMX_CUDA(cudaMemcpy(h->gtgt.p, g->t.data(), g->t.size() * 8, cudaMemcpyHostToDevice));
+      IMX_CUDA(cudaMemcpy(h->gsrc.p, g->s.data(), g->s.size() * 8, cudaMemcpyHostToDevice));
     }
   }
 
@@ -1283,6 +1338,14 @@ void imexlb_destroy(imexlb_lattice* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
   delete h;
+}
+
+int imexlb_set_wait_limit(imexlb_lattice* h, double seconds) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (!(seconds > 0.0) || seconds > 1.0) return fail(IMEXLB_E_ARG, "wait limit must lie in (0, 1] seconds");
+  const double ns = seconds * 1e9;
+  h->base_args.wait_ns = ns < 1.0 ? 1ull : static_cast<uint64_t>(ns);
+  return IMEXLB_OK;
 }
 
 int imexlb_release_cached_memory(void) {

@@ -126,6 +126,16 @@ struct StepArgs {
   const int32_t* face_codes = nullptr;
   int64_t face_base[6] = {};
   int32_t face_dim[6] = {};
+  // its face cells (i + nx (j + ny k), in that order), which the first
+  // face_layers z-layers of the step grid process, one cell a thread; the
+  // other blocks leave face cells alone
+  const int32_t* face_cells = nullptr;
+  int32_t n_face = 0;
+  int32_t face_layers = 0;
+  // single-lattice staged kernels: bound on each wait for a tile's copies or
+  // for a stage to be released (the drain of copies in flight after a block
+  // gives up keeps the full second)
+  uint64_t wait_ns = 1000000000ull;
 };
 // A face cell's words in the face-code table: word q (for a population whose
 // pull leaves the box) names where the pulled value comes from --

@@ -137,15 +137,35 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Wait for the phase of `parity` to complete; false after about a second.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
-  if (bar_try_wait(bar, parity)) return true;
+// try_wait that suspends at most about `hint_ns` (the instruction's own
+// suspend-time hint) before it reports the phase as not yet complete.
+__device__ __forceinline__ bool bar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return done != 0;
+}
+
+// Wait for the phase of `parity` to complete; false after about limit_ns.
+// A limit below a millisecond is also passed to each try_wait as its
+// suspend-time hint, since one try_wait may otherwise suspend for longer
+// than the limit.
+__device__ __forceinline__ bool bar_wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  const bool short_limit = limit_ns < 1000000ull;
+  const uint32_t hint = static_cast<uint32_t>(short_limit ? limit_ns : 0ull);
+  if (short_limit ? bar_try_wait_hint(bar, parity, hint) : bar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (true) {
-    if (bar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > WAIT_NS) return false;
+    if (short_limit ? bar_try_wait_hint(bar, parity, hint) : bar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
+
+// The same with the full bound of about a second.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) { return bar_wait_for(bar, parity, WAIT_NS); }
 
 // Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
 // from global to this block's shared memory, completing on `bar`.

@@ -275,27 +275,47 @@ __device__ __forceinline__ void load_cell(const StepArgs& a, const P& pl, const 
     if constexpr (RULE == CaseRule::CavityRef) {
       const unsigned wf = a.face_codes ? wall_flags(a, i, j, k) : 0u;
       if (wf != 0u) {
-        // a face cell of the reference cavity: the boundary passes resolved
-        // per link (the face-code table, lattice.h); links that stay inside
-        // pull their neighbour as usual
+        // a face cell of the reference cavity, with the boundary passes
+        // resolved per link (the face-code table, lattice.h): its 28 code
+        // words in seven 16-byte loads, the pull address of every link that
+        // leaves the box replaced, then all 27 value loads at once.  Only
+        // the face blocks of the step grid reach here (step_kernel), so no
+        // warp mixes this path with the inside cells' one.
         using T = typename StoreT<S>::T;
         const int face = __ffs(static_cast<int>(wf)) - 1;
         const int fa = face < 2 ? j : i, fb = face < 4 ? k : j;
-        const int32_t* codes =
-            a.face_codes + a.face_base[face] + (static_cast<int64_t>(fb) * a.face_dim[face] + fa) * FACE_CODE_WORDS;
-        const uint32_t keep = static_cast<uint32_t>(__ldg(codes + Q));
+        const int4* cw = reinterpret_cast<const int4*>(
+            a.face_codes + a.face_base[face] + (static_cast<int64_t>(fb) * a.face_dim[face] + fa) * FACE_CODE_WORDS);
+        int32_t code[FACE_CODE_WORDS];
+#pragma unroll
+        for (int v = 0; v < FACE_CODE_WORDS / 4; ++v) {
+          const int4 c4 = __ldg(cw + v);
+          code[4 * v] = c4.x;
+          code[4 * v + 1] = c4.y;
+          code[4 * v + 2] = c4.z;
+          code[4 * v + 3] = c4.w;
+        }
         const T* in = static_cast<const T*>(a.src);
-        const T* out = static_cast<const T*>(a.dst);
+        const T* out = static_cast<const T*>(a.dst);  // ghost slots only: this step writes the interior
+        T raw[Q];
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          const T* ptr = pl.srcq[q] + (b + a.rel[q]);
+          if (leaves<q>(wf)) {
+            const int32_t c = code[q];
+            ptr = c >= 0 ? in + c : (c == -1 ? ptr : out + (-static_cast<int64_t>(c) - 2));
+          }
+          raw[q] = __ldg(ptr);
+        });
+        const uint32_t keep = static_cast<uint32_t>(code[Q]);
         static_for<0, Q>([&](auto qc) {
           constexpr int q = decltype(qc)::value;
           if (leaves<q>(wf)) {
-            const int32_t c = __ldg(codes + q);
-            const T v = c >= 0 ? __ldg(in + c) : (c == -1 ? T(0) : out[-static_cast<int64_t>(c) - 2]);
-            if ((keep >> q) & 1u) const_cast<T*>(in)[q * a.sq + b + a.rel[q]] = v;
-            f[q] = decode<S>(v, q, a.enc);
-          } else {
-            f[q] = decode<S>(pl.load(q, b + a.rel[q]), q, a.enc);
+            if (code[q] == -1) raw[q] = T(0);
+            // the value a later step reads as this slot's previous one
+            if ((keep >> q) & 1u) const_cast<T*>(in)[q * a.sq + b + a.rel[q]] = raw[q];
           }
+          f[q] = decode<S>(raw[q], q, a.enc);
         });
         return;
       }
@@ -648,6 +668,10 @@ __device__ __forceinline__ void step_cells(const StepArgs& a, const P& pl, const
   for (int c = 0; c < CPT; ++c) {
     const int j = j0 + c;
     act[c] = i < a.nx && j < a.ny;
+    if constexpr (RULE == CaseRule::CavityRef) {
+      // with the face blocks (step_kernel), the inside blocks skip face cells
+      if (a.face_cells && wall_flags(a, i, j, k) != 0u) act[c] = false;
+    }
     if constexpr (RULE == CaseRule::SphereStd) {
       // solid cells are not updated; they report zero moments
       if (act[c]) {

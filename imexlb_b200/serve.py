@@ -17,9 +17,13 @@ falls below a tolerance.  The loop does continuous batching:
   so it stops at exactly that step, with its fields written there, while
   the others go on;
 * retirement: after each call the residuals are read; an instance that
-  reached its step count or the tolerance is retired, its u, v, w, p are
-  read back to the host (the request's answer) and its memory is freed for
-  the next admission.
+  reached its step count or the tolerance is retired, its answer is read
+  back to the host and its memory is freed for the next admission.  The
+  answer is the u, v, w, p of the lattice's middle z plane (answer="plane",
+  the default: a cut through the flow, at most 2 MB) or of the whole lattice
+  (answer="fields": up to 268 MB for the largest sphere channel, 77 GB for
+  the configuration's 2000 requests, which would make the stream a test of
+  the host link rather than of the solver).
 
 Storage: with storage "f16" each request is stored in FP16 when its
 tau - 1/2 is at least imexlb_b200.batch.FP16_MIN_TAU0 and in FP32 otherwise
@@ -128,8 +132,11 @@ class Server:
     """Continuous batching of requests into one engine."""
 
     def __init__(self, storage: str = "f16", budget_bytes: int = 150 << 30, max_active_cells: int = 48 << 20,
-                 max_instances: int = 512, chunk: int = 200, tiles: dict | None = None, stream=None):
+                 max_instances: int = 512, chunk: int = 200, tiles: dict | None = None, stream=None,
+                 answer: str = "plane", full_ids=()):
         self.storage = storage
+        self.answer = answer
+        self.full_ids = set(full_ids)  # requests answered with their whole fields
         self.eng = api.Engine(storage=storage, arith="fast", budget_bytes=budget_bytes, max_instances=max_instances,
                               stream=stream)
         self.max_active_cells = max_active_cells
@@ -171,9 +178,10 @@ class Server:
 
     def collect(self) -> list[tuple]:
         """Wait for the queued steps, read the residuals and retire; returns
-        [(request, fields, steps, residual)] of the retired requests (fields
-        None for a diverged one).  Requests admitted after launch() did not
-        take part in its steps."""
+        [(request, answer, steps, residual)] of the retired requests (the
+        middle z plane or the whole fields, see the module docstring; None
+        for a diverged one).  Requests admitted after launch() did not take
+        part in its steps."""
         n, stepped = getattr(self, "_stepped", (0, set()))
         self._stepped = (0, set())
         if not n:
@@ -190,7 +198,12 @@ class Server:
             # retire at the step count, at the tolerance, or when the lattice
             # diverged (NaN); the first check after admission reads +inf
             if done >= req.max_steps or 0 <= r < req.tol or math.isnan(r):
-                f = None if math.isnan(r) else self.eng.fields(slot)
+                if math.isnan(r):
+                    f = None
+                elif self.answer == "fields" or req.rid in self.full_ids:
+                    f = self.eng.fields(slot)
+                else:
+                    f = self.eng.plane(slot, req.n[2] // 2)
                 self.eng.remove(slot)
                 del self.active[slot]
                 done_now.append((req, f, done, r))
@@ -215,7 +228,10 @@ def serve(requests: list[Request], storage: str = "f16", keep_fields=False, **kw
     import torch
 
     stream = torch.cuda.Stream()
-    srv = Server(storage=storage, stream=stream.cuda_stream, **kw)
+    full = keep_fields if isinstance(keep_fields, (set, frozenset, list, tuple)) else ()
+    if keep_fields is True:
+        kw["answer"] = "fields"
+    srv = Server(storage=storage, stream=stream.cuda_stream, full_ids=full, **kw)
     waiting = list(requests)
     results = {}
     t0 = time.perf_counter()
@@ -280,9 +296,10 @@ def service_times_alone(requests: list[Request], storage: str = "f64", chunk: in
     return out
 
 
-def run_alone(req: Request, storage: str, steps: int, chunk: int = 200, stream=None):
+def run_alone(req: Request, storage: str, steps: int, chunk: int = 200, stream=None, answer: str = "fields"):
     """One request alone in its own engine for exactly `steps` steps: host
-    seconds from admission to its answer read back, and the answer."""
+    seconds from admission to its answer (the whole fields, or the middle z
+    plane) read back, and the answer."""
     import torch
 
     d = req.desc()
@@ -297,7 +314,7 @@ def run_alone(req: Request, storage: str, steps: int, chunk: int = 200, stream=N
             eng.step(n)
             eng.residuals()  # the per-call check the serving loop makes
             left -= n
-        f = eng.fields(slot)
+        f = eng.fields(slot) if answer == "fields" else eng.plane(slot, req.n[2] // 2)
     return time.perf_counter() - t, f
 
 
@@ -312,9 +329,9 @@ def service_model_by_shape(requests: list[Request], storage: str = "f64", probes
     out = {}
     for case, n in shapes:
         req = next(r for r in requests if (r.case, r.n) == (case, n))
-        run_alone(req, storage, 20, stream=stream.cuda_stream)  # warm the kernels of this shape
-        t1, _ = run_alone(req, storage, probes[0], stream=stream.cuda_stream)
-        t2, _ = run_alone(req, storage, probes[1], stream=stream.cuda_stream)
+        run_alone(req, storage, 20, stream=stream.cuda_stream, answer="plane")  # warm the kernels of this shape
+        t1, _ = run_alone(req, storage, probes[0], stream=stream.cuda_stream, answer="plane")
+        t2, _ = run_alone(req, storage, probes[1], stream=stream.cuda_stream, answer="plane")
         per_step = max(0.0, (t2 - t1) / (probes[1] - probes[0]))
         out[(case, n)] = dict(fixed=max(0.0, t1 - per_step * probes[0]), per_step=per_step)
     return out
@@ -380,6 +397,8 @@ def main(argv=None) -> int:
     ap.add_argument("--check-error", type=int, default=0,
                     help="check this many served answers (seeded sample) against FP64 runs alone")
     ap.add_argument("--out", default=None, help="append each rate's JSON line to this file")
+    ap.add_argument("--answer", choices=["plane", "fields"], default="plane",
+                    help="what a retired request reads back: its middle z plane or its whole fields")
     args = ap.parse_args(argv)
     from . import tune
 
@@ -401,10 +420,11 @@ def main(argv=None) -> int:
             sample = set(int(x) for x in rng.choice(len(reqs), min(args.check_error, len(reqs)), replace=False))
         t0 = time.perf_counter()
         res = serve(reqs, args.storage, budget_bytes=int(args.budget_gb * (1 << 30)),
-                    max_active_cells=args.max_active_cells, tiles=tiles, keep_fields=sample)
+                    max_active_cells=args.max_active_cells, tiles=tiles, keep_fields=sample, answer=args.answer)
         line = dict(rate=rate, count=args.count, storage=args.storage, p50_s=res["p50"], p99_s=res["p99"],
                     solves_per_s=res["solves_per_s"], mlups=res["mlups"], span_s=res["span"],
                     steps_scale=args.scale_steps, status=res["status"], storage_requests=res["storage"],
+                    answer=args.answer,
                     wall_s=time.perf_counter() - t0)
         steps = {r.rid: res["results"][r.rid]["steps"] for r in reqs}
         base = None

@@ -239,6 +239,16 @@ int imexlb_profile_read(imexlb_lattice* h, imexlb_kernel_times* out);
 /* Wait for all work queued on the lattice's stream. */
 int imexlb_synchronize(imexlb_lattice* h);
 
+/* Bound, in (0, 1] seconds (default 1), on each wait of the 2-byte staged
+ * step kernels for their own row copies or for a stage to be released.  A
+ * block that waits longer gives up: it lets its copies in flight land (that
+ * drain keeps the full second), leaves, and the next synchronising call
+ * returns IMEXLB_E_CUDA ("gave up waiting"); the lattice state is then
+ * invalid until imexlb_initialize or a checkpoint load.  Lets a caller, or a
+ * test, exercise that failure path without a fault.  No counterpart in the
+ * reference. */
+int imexlb_set_wait_limit(imexlb_lattice* h, double seconds);
+
 void imexlb_destroy(imexlb_lattice* h);
 
 /* Lattices take their device memory from a stream-ordered pool per device
@@ -307,6 +317,10 @@ int imexlb_engine_step(imexlb_engine* e, int nsteps);
 int imexlb_engine_limit(imexlb_engine* e, int slot, int steps);
 /* u, v, w, p of one instance after the last step (host arrays, x fastest). */
 int imexlb_engine_fields(imexlb_engine* e, int slot, double* u, double* v, double* w, double* p);
+/* The same for one z plane k of the instance (nx * ny values each, x
+ * fastest): a compact answer for a serving loop whose requests want a cut
+ * through the flow rather than the whole field. */
+int imexlb_engine_plane(imexlb_engine* e, int slot, int k, double* u, double* v, double* w, double* p);
 /* Velocity residual per slot, sqrt(sum|u - u_prev|^2 / sum|u|^2) between this
  * call and the previous one (INFINITY on an instance's first call, -1 for an
  * instance that took no step since the previous call -- it stopped at its

@@ -33,7 +33,7 @@ def _requests(serve):
 
 
 def _alone(serve, req, storage):
-    srv = serve.Server(storage=storage, budget_bytes=1 << 30, max_instances=1, chunk=25)
+    srv = serve.Server(storage=storage, budget_bytes=1 << 30, max_instances=1, chunk=25, answer="fields")
     try:
         assert srv.try_admit(req)
         done = []

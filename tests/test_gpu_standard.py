@@ -120,3 +120,26 @@ def test_sphere_reduced_precision_velocity_and_drag(api, storage, vel_bound, dra
     assert err <= vel_bound, f"{storage} sphere: relative velocity L2 error {err:.3e} > {vel_bound:.1e}"
     derr = abs(dgot[0] - dwant[0]) / abs(dwant[0])
     assert derr <= drag_bound, f"{storage} sphere: drag error {derr:.3e} > {drag_bound:.1e}"
+
+
+def test_staged_wait_limit_gives_up_and_the_lattice_recovers(api):
+    """With a 1 ns bound on the staged kernel's waits for its own row copies,
+    blocks give up (after letting their copies in flight land) and the next
+    synchronising call reports it; re-initialised with the default bound, the
+    lattice runs bit for bit like a fresh one."""
+    kw = dict(bc="standard", storage="f16", arith="fast", lid_u=0.1)
+    with api.LBM("cavity", 64, 64, 64, 0.03, 1.0, 0.1, **kw) as lbm:
+        lbm.set_wait_limit(1e-9)
+        lbm.step(3)
+        with pytest.raises(api.ImexlbError) as err:
+            lbm.synchronize()
+        assert err.value.code == 2 and "gave up waiting" in str(err.value)
+        lbm.set_wait_limit(1.0)
+        lbm.Initialize()
+        lbm.step(20)
+        got = lbm.fields()
+    with api.LBM("cavity", 64, 64, 64, 0.03, 1.0, 0.1, **kw) as fresh:
+        fresh.step(20)
+        want = fresh.fields()
+    for k in "uvwp":
+        assert np.array_equal(got[k], want[k]), k

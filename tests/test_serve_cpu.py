@@ -66,7 +66,10 @@ class FakeEngine:
         return [self.res.get(s, float("inf")) for s in range(max(self.next, 1))]
 
     def fields(self, slot):
-        return {"steps": self.taken[slot]}
+        return {"steps": self.taken[slot], "answer": "fields"}
+
+    def plane(self, slot, k):
+        return {"steps": self.taken[slot], "answer": "plane", "k": k}
 
     def remove(self, slot):
         del self.taken[slot], self.left[slot], self.res[slot]
@@ -102,3 +105,19 @@ def test_server_retires_on_the_residual_tolerance(monkeypatch):
         out += srv.advance()
     # residual 1 / (1 + steps) drops under the tolerance after 200 steps
     assert [(r.rid, steps) for r, f, steps, res in out] == [(0, 200)]
+
+
+def test_server_answers_with_a_plane_or_the_whole_fields(monkeypatch):
+    """The default answer is the middle z plane; the requests named in
+    full_ids (the accuracy sample) are answered with their whole fields."""
+    monkeypatch.setattr(serve.api, "Engine", FakeEngine)
+    srv = serve.Server(chunk=100, full_ids={1})
+    reqs = [serve.Request(i, 0.0, "cavity", (32, 32, 40), 100.0, 50, tol=1e-9) for i in range(2)]
+    for r in reqs:
+        assert srv.try_admit(r)
+    got = {}
+    while srv.active:
+        for req, f, steps, res in srv.advance():
+            got[req.rid] = f
+    assert got[0]["answer"] == "plane" and got[0]["k"] == 20
+    assert got[1]["answer"] == "fields"
