@@ -336,11 +336,17 @@ __global__ void engine_resid_kernel(const EngArgs ea, double* part) {
     const EngInst& in = ea.inst[tile.slot];
     const int k = tile.k;
     const int nx = in.a.nx, ny = in.a.ny;
-    const int tw = in.tw, th = in.th;
+    const bool flat = in.staged && in.geo.flat;  // flat tiles: j0 is the tile's first element
+    const int tw = flat ? in.geo.C : in.tw, th = flat ? 1 : in.th;
     const int64_t n = static_cast<int64_t>(nx) * ny * in.a.nz;
     double d2 = 0.0, n2 = 0.0;
     for (int c = threadIdx.x; c < tw * th; c += blockDim.x) {
-      const int i = tile.i0 + c % tw, j = tile.j0 + c / tw;
+      int i = tile.i0 + c % tw, j = tile.j0 + c / tw;
+      if (flat) {
+        const int e = tile.j0 + c;
+        j = e / in.geo.P;
+        i = e - j * in.geo.P;
+      }
       if (i < nx && j < ny) {
         const int64_t cell = i + static_cast<int64_t>(nx) * (j + static_cast<int64_t>(ny) * k);
         const double u = in.a.mu[cell], v = in.a.mv[cell], w = in.a.mw[cell];
@@ -637,9 +643,15 @@ int rebuild_tiles(imexlb_engine* e) {
     sl.seg = static_cast<int>(e->seg_slots.size());
     e->seg_slots.push_back(s);
     sb.push_back(static_cast<int>(e->h_tiles.size()));
-    for (int k = 0; k < sl.L.nz; ++k)
-      for (int j0 = 0; j0 < sl.L.ny; j0 += in.th)
-        for (int i0 = 0; i0 < sl.L.nx; i0 += in.tw) e->h_tiles.push_back(Tile{s, i0, j0, k});
+    if (in.staged && in.geo.flat) {
+      // flat tiles (stage_core.cuh): j0 holds the tile's first element of its plane
+      for (int k = 0; k < sl.L.nz; ++k)
+        for (int t = 0; t < in.geo.nty; ++t) e->h_tiles.push_back(Tile{s, 0, t * in.geo.C, k});
+    } else {
+      for (int k = 0; k < sl.L.nz; ++k)
+        for (int j0 = 0; j0 < sl.L.ny; j0 += in.th)
+          for (int i0 = 0; i0 < sl.L.nx; i0 += in.tw) e->h_tiles.push_back(Tile{s, i0, j0, k});
+    }
     se.push_back(static_cast<int>(e->h_tiles.size()));
     e->group_end[g] = static_cast<int>(e->h_tiles.size());
   }

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
     for (; issued < NS - 1; ++issued) {
       const int t = blockIdx.x + issued * grid;
       if (t >= ntiles) break;
-      issue_tile<T, WRAP>(a, g, src, (t % g.nty) * g.R, t / g.nty, stages + issued * stage_elems, &full[issued],
+      issue_tile<T, WRAP>(a, g, src, tile_origin(g, t), tile_plane(g, t), stages + issued * stage_elems, &full[issued],
                           REC ? a.rec_src : nullptr, rec_stage(issued));
     }
   }
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
           break;
         }
         const int sn = (i + NS - 1) % NS;
-        issue_tile<T, WRAP>(a, g, src, (tn % g.nty) * g.R, tn / g.nty, stages + sn * stage_elems, &full[sn],
+        issue_tile<T, WRAP>(a, g, src, tile_origin(g, tn), tile_plane(g, tn), stages + sn * stage_elems, &full[sn],
                             REC ? a.rec_src : nullptr, rec_stage(sn));
         ++issued;
       }
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       break;
     }
     const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
-    consume_tile<S, B, RULE>(a, pl, g, st, (t % g.nty) * g.R, t / g.nty, a.store != 0, rec_stage(s), a.rec_dst);
+    consume_tile<S, B, RULE>(a, pl, g, st, tile_origin(g, t), tile_plane(g, t), a.store != 0, rec_stage(s), a.rec_dst);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;
@@ -611,11 +611,11 @@ int64_t step_grid_blocks(const LaunchCfg& c, int nx, int ny, int nz) {
 }
 
 // The staged kernels' copy plan of one 2-byte lattice, from the same
-// tile_runs the kernels run (see imexlb_debug_stage_plan).
-int64_t stage_plan(int nx, int ny, int nz, bool wrap_yz, int32_t* geo, int32_t* runs, int64_t max_runs) {
+// tile_runs / tile_runs_flat the kernels run (see imexlb_debug_stage_plan).
+int64_t stage_plan(int nx, int ny, int nz, int mode, int32_t* geo, int32_t* runs, int64_t max_runs) {
   const Layout L = make_layout(nx, ny, nz, 0, 2);
   stage::Geo g;
-  const CaseRule rule = wrap_yz ? CaseRule::None : CaseRule::CavityStd;
+  const CaseRule rule = mode == 0 ? CaseRule::CavityStd : (mode == 2 ? CaseRule::SphereStd : CaseRule::None);
   if (!stage::staged_layout(rule, nx, ny, L.pitch, &g)) return -1;
   StepArgs a;
   a.nx = nx;
@@ -625,16 +625,19 @@ int64_t stage_plan(int nx, int ny, int nz, bool wrap_yz, int32_t* geo, int32_t* 
   a.sz32 = static_cast<int32_t>(L.sz);
   a.pitch32 = static_cast<int32_t>(L.pitch);
   if (geo) {
-    const int32_t v[8] = {g.P, g.R, g.cap, g.nty, static_cast<int32_t>(L.sq), a.sz32, a.pitch32, a.base32};
-    for (int i = 0; i < 8; ++i) geo[i] = v[i];
+    const int32_t v[10] = {g.P, g.R, g.cap, g.nty, static_cast<int32_t>(L.sq), a.sz32, a.pitch32, a.base32,
+                           g.flat, g.C};
+    for (int i = 0; i < 10; ++i) geo[i] = v[i];
   }
   int64_t n = 0;
   for (int t = 0; t < g.nty * nz; ++t) {
-    const int j0 = (t % g.nty) * g.R, k = t / g.nty;
+    const int j0 = stage::tile_origin(g, t), k = stage::tile_plane(g, t);
     const int rv = ny - j0 < g.R ? ny - j0 : g.R;
     for (int q = 0; q < Q; ++q) {
       stage::Run m{0, 0, 0u, q}, w{0, 0, 0u, q};
-      if (wrap_yz)
+      if (g.flat)
+        stage::tile_runs_flat(a, g, q, j0, k, 2, m, w);
+      else if (rule != CaseRule::CavityStd)
         stage::tile_runs<true>(a, g, q, j0, k, rv, 2, m, w);
       else
         stage::tile_runs<false>(a, g, q, j0, k, rv, 2, m, w);

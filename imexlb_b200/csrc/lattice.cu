@@ -1417,10 +1417,10 @@ int64_t imexlb_debug_face_codes(int nx, int ny, int nz, int32_t* codes, int64_t 
 }
 
 // Not part of include/imexlb.h: lists the staged kernels' bulk copies so
-// that their alignment and bounds are checked on the CPU (tests).
-int64_t imexlb_debug_stage_plan(int nx, int ny, int nz, int wrap_yz, int32_t* geo, int32_t* runs,
-                                int64_t max_runs) {
-  return imx::stage_plan(nx, ny, nz, wrap_yz != 0, geo, runs, max_runs);
+// that their alignment and bounds are checked on the CPU (tests).  mode: 0
+// cavity, 1 periodic vortex, 2 sphere channel; geo: 10 values (stage_plan).
+int64_t imexlb_debug_stage_plan(int nx, int ny, int nz, int mode, int32_t* geo, int32_t* runs, int64_t max_runs) {
+  return imx::stage_plan(nx, ny, nz, mode, geo, runs, max_runs);
 }
 
 }  // extern "C"

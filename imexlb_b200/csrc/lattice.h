@@ -217,13 +217,14 @@ bool uses_wall_records(const LaunchCfg& c, int nx, int ny, int64_t pitch);
 // after the buffer was written other than by a step.
 cudaError_t launch_cavity_records(const Layout& L, const void* buf, uint16_t* rec, cudaStream_t s);
 // Copy plan of the shared-memory staged kernels for a 2-byte lattice of
-// nx x ny x nz with y / z wrapping (periodic, sphere) or walls (cavity).
-// geo (8 values): P, R, cap, nty, then the layout's sq, sz, pitch and base.
-// runs: up to max_runs records (tile, q, population read, source element,
-// stage element, bytes); the cavity's wall-record copy of a tile has q = Q,
-// population -1 and its element offset in the record buffer.  Returns the
-// number of copies, or -1 when the lattice is not staged.
-int64_t stage_plan(int nx, int ny, int nz, bool wrap_yz, int32_t* geo, int32_t* runs, int64_t max_runs);
+// nx x ny x nz: mode 0 the cavity (walls), 1 the periodic vortex, 2 the
+// sphere channel (flat tiles where its planes allow them).  geo (10
+// values): P, R, cap, nty, the layout's sq, sz, pitch and base, then flat
+// and C.  runs: up to max_runs records (tile, q, population read, source
+// element, stage element, bytes); the cavity's wall-record copy of a tile
+// has q = Q, population -1 and its element offset in the record buffer.
+// Returns the number of copies, or -1 when the lattice is not staged.
+int64_t stage_plan(int nx, int ny, int nz, int mode, int32_t* geo, int32_t* runs, int64_t max_runs);
 cudaError_t launch_init_f(const LaunchCfg& c, const Layout& L, void* buf0, void* buf1, const double* u,
                           const double* v, const double* w, const double* p, double p_shift, const Encoding& enc,
                           cudaStream_t s);

@@ -50,14 +50,29 @@ constexpr int SLOT_UNITS = 2 * 1024;  // stages x elements per population slot
 constexpr uint64_t WAIT_NS = 1000000000ull;
 constexpr int MAX_STAGES = 2;
 
-// Tile geometry of one lattice.
+// Tile geometry of one lattice.  A tile is R whole rows of a plane, or (flat
+// tiles) a run of C elements of a plane's rows taken as one line.
 struct Geo {
   int P;       // staged row length: the layout's pitch (whole rows)
-  int R;       // rows per tile
-  int cap;     // elements per population slot of a stage (R * P <= cap)
+  int R;       // rows per tile (whole-row tiles)
+  int cap;     // elements per population slot of a stage (R * P <= cap, or C + 2 FLAT_GUARD <= cap)
   int stages;  // stages * cap == SLOT_UNITS
-  int nty;     // tiles along y
+  int nty;     // tiles per plane
+  int flat;    // flat tiles (sphere channel)
+  int C;       // elements per flat tile
 };
+
+// Flat tiles (the sphere channel: x not periodic, y and z periodic).  Whole
+// rows of 768 elements make one-row tiles of 384 x-pairs for 256 threads, a
+// quarter of whom then idle through a second pass.  A flat tile is the run
+// [e0, e0 + C) of a plane's elements e = j P + x, across row ends; each
+// population's slot holds the source run [e0 - e_y P - G, e0 + C - e_y P + G)
+// of its plane (G = FLAT_GUARD elements a side, so that every pair's x - 1
+// and x + 2 neighbours are staged, and 16-byte aligned), split in two where
+// it wraps around the periodic y.  The pulled neighbour across a row end is
+// never used: the inlet (x = 0) takes the inflow's equilibrium and the
+// outlet (x = nx - 1) the cell's own column.
+constexpr int FLAT_GUARD = 8;
 
 // The 2-byte cavity's tiles also stage the wall records of their rows
 // (WallRecord, 64 bytes a row) in an area of REC_ROWS records per stage.
@@ -81,16 +96,42 @@ inline bool make_geo(int ny, int64_t pitch, Geo* g, int max_rows = 1024) {
   return true;
 }
 
+// Flat tiles of C = 1008 elements for a plane of ny rows of `pitch`
+// elements, when the plane is long enough that a tile's source run wraps
+// around y on one side at most.
+inline bool make_geo_flat(int ny, int64_t pitch, Geo* g) {
+  const int cap = 1024, C = cap - 2 * FLAT_GUARD;
+  const int64_t np = static_cast<int64_t>(ny) * pitch;
+  if (pitch % 8 != 0 || np < C + 2 * pitch + 2 * FLAT_GUARD || np > (int64_t(1) << 30)) return false;
+  g->P = static_cast<int>(pitch);
+  g->R = 1;
+  g->cap = cap;
+  g->stages = SLOT_UNITS / cap;
+  g->flat = 1;
+  g->C = C;
+  g->nty = static_cast<int>((np + C - 1) / C);
+  return true;
+}
+
 // Tile geometry of the staged kernels for a lattice of nx x ny cells with
 // rows of `pitch` elements, or false when it is not staged: nx even (the
 // x-pairs); the cavity (wall records) at most REC_ROWS rows a tile and
-// nx >= 4, so that a pair holds at most one x-wall cell.
+// nx >= 4, so that a pair holds at most one x-wall cell; the sphere channel
+// in flat tiles where its planes allow them.
 inline bool staged_layout(CaseRule rule, int nx, int ny, int64_t pitch, Geo* g) {
   if (nx % 2 != 0) return false;
+  g->flat = 0;
+  g->C = 0;
+  if (rule == CaseRule::SphereStd && nx >= 4 && make_geo_flat(ny, pitch, g)) return true;
   const bool rec = rule == CaseRule::CavityStd;
   if (rec && nx < 4) return false;
   return make_geo(ny, pitch, g, rec ? REC_ROWS : 1024);
 }
+
+// First row (whole-row tiles) or first element (flat tiles) of tile t of
+// its plane, and its plane.
+__host__ __device__ __forceinline__ int tile_origin(const Geo& g, int t) { return (t % g.nty) * (g.flat ? g.C : g.R); }
+__host__ __device__ __forceinline__ int tile_plane(const Geo& g, int t) { return t / g.nty; }
 
 // stages of 27 population slots, the wall-record areas (cavity), then the
 // full and empty mbarriers
@@ -250,6 +291,48 @@ __host__ __device__ __forceinline__ void tile_runs(const A& a, const Geo& g, int
   wrap.bytes = (first || last) ? static_cast<uint32_t>(g.P * elem) : 0u;
 }
 
+// The copies of population q for flat tile [e0, e0 + C) of plane k (the
+// sphere channel, y and z periodic): the source run [e0 - e_y P - G,
+// e0 + n - e_y P + G) of plane k - e_z, n = the tile's own length, as at most
+// two runs, the second one the part that wraps around y.
+template <class A>
+__host__ __device__ __forceinline__ void tile_runs_flat(const A& a, const Geo& g, int q, int e0, int k, int elem,
+                                                        Run& main, Run& wrap) {
+  main.bytes = 0;
+  wrap.bytes = 0;
+  main.pop = wrap.pop = q;
+  const int32_t np = a.ny * g.P;
+  int kk = k - ez_of(q);
+  kk = kk < 0 ? kk + a.nz : (kk >= a.nz ? kk - a.nz : kk);
+  const int32_t plane = a.base32 + kk * a.sz32;
+  const int n = np - e0 < g.C ? np - e0 : g.C;
+  const int32_t s0 = e0 - ey_of(q) * g.P - FLAT_GUARD;  // source element of slot element 0
+  const int32_t s1 = s0 + n + 2 * FLAT_GUARD;            // one past the last
+  const int32_t slot = q * g.cap;
+  if (s1 <= 0 || s0 >= np) {
+    // the whole run lies across the y wrap (a short last tile of a plane)
+    main.src = plane + (s1 <= 0 ? s0 + np : s0 - np);
+    main.dst = slot;
+    main.bytes = static_cast<uint32_t>((s1 - s0) * elem);
+    return;
+  }
+  // the part inside [0, np), and the part below 0 or at np and above (the
+  // run is shorter than the plane by two rows: never both)
+  const int32_t lo = s0 < 0 ? 0 : s0, hi = s1 > np ? np : s1;
+  main.src = plane + lo;
+  main.dst = slot + (lo - s0);
+  main.bytes = static_cast<uint32_t>((hi - lo) * elem);
+  if (s0 < 0) {
+    wrap.src = plane + (s0 + np);
+    wrap.dst = slot;
+    wrap.bytes = static_cast<uint32_t>(-s0 * elem);
+  } else if (s1 > np) {
+    wrap.src = plane;
+    wrap.dst = slot + (np - s0);
+    wrap.bytes = static_cast<uint32_t>((s1 - np) * elem);
+  }
+}
+
 // The wall records of tile rows [j0, j0 + rv) of plane k: one contiguous
 // run (element offset into the record buffer, bytes).
 template <class A>
@@ -274,7 +357,12 @@ __device__ __forceinline__ void issue_tile(const A& a, const Geo& g, const T* sr
   const int lane = threadIdx.x & 31;
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   Run m{0, 0, 0u}, w{0, 0, 0u};
-  if (lane < Q) tile_runs<WRAP_YZ>(a, g, lane, j0, k, rv, static_cast<int>(sizeof(T)), m, w);
+  if (lane < Q) {
+    if (g.flat)
+      tile_runs_flat(a, g, lane, j0, k, static_cast<int>(sizeof(T)), m, w);  // j0: the tile's first element
+    else
+      tile_runs<WRAP_YZ>(a, g, lane, j0, k, rv, static_cast<int>(sizeof(T)), m, w);
+  }
   int64_t rsrc = 0;
   uint32_t rbytes = 0;
   if (lane == 30 && rec_src) tile_records(a, j0, k, rv, rsrc, rbytes);
@@ -303,17 +391,23 @@ __device__ __forceinline__ void issue_skip(uint64_t* bar) {
 // row or plane around it.  Cavity: `rec` is the stage's wall records (tile
 // row r at r * WallRecord::WORDS), `rec_row` the pair's row in the record
 // buffer this step writes.
-template <Store S, Bc B, CaseRule RULE, bool EDGE, class P>
+template <Store S, Bc B, CaseRule RULE, bool EDGE, bool FLAT = false, class P>
 __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                                 const int x, const int r, const int j0, const int k,
                                                 const bool store, const uint16_t* rec = nullptr,
-                                                uint16_t* rec_row = nullptr) {
-  const int j = j0 + r;
+                                                uint16_t* rec_row = nullptr, const int flat_j = 0,
+                                                const int flat_pw = 0) {
+  // flat tiles: the pair's row and its word in the slot come from the caller
+  const int j = FLAT ? flat_j : j0 + r;
   const int row = (r * g.P) >> 1;  // word offset of tile row r in a slot
-  const int pw = row + (x >> 1);
+  const int pw = FLAT ? flat_pw : row + (x >> 1);
   const bool left_edge = EDGE && x == 0, right_edge = EDGE && x + 2 >= a.nx;
   int lw, rw;  // the pairs holding x - 1 and x + 2
-  if constexpr (RULE == CaseRule::CavityStd) {
+  if constexpr (FLAT) {
+    // the guards hold both; across a row end their values go unused
+    lw = pw - 1;
+    rw = pw + 1;
+  } else if constexpr (RULE == CaseRule::CavityStd) {
     // at an x wall the value comes from the wall record below; read the
     // pair's own word there, inside the row
     lw = row + ((x == 0 ? x : x - 2) >> 1);
@@ -445,6 +539,26 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
         pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
       else
         pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
+    }
+  } else if constexpr (RULE == CaseRule::SphereStd) {
+    if (g.flat) {
+      // flat tile [e0, e0 + n) (j0 holds e0): pair p is elements e0 + 2p and
+      // e0 + 2p + 1, word p + G/2 of the slot
+      const int e0 = j0;
+      const int np = a.ny * g.P;
+      const int n = np - e0 < g.C ? np - e0 : g.C;
+      for (int p = threadIdx.x; 2 * p < n; p += THREADS) {
+        const int e = e0 + 2 * p;
+        const int j = e / g.P, x = e - j * g.P;
+        if (x < a.nx)
+          pair_from_stage<S, B, RULE, true, true>(a, pl, g, st, x, 0, 0, k, store, nullptr, nullptr, j,
+                                                  p + FLAT_GUARD / 2);
+      }
+    } else {
+      for (int p = threadIdx.x; p < npairs; p += THREADS) {
+        const int r = p / half, x = 2 * (p - r * half);
+        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+      }
     }
   } else {
     for (int p = threadIdx.x; p < npairs; p += THREADS) {

@@ -9,6 +9,10 @@ and its stage slot, and the slot rows must hold exactly the rows the pull
 reads: the periodic image on a wrapping axis, the cell's own opposite
 population beyond a cavity wall (halfway bounce-back).  A cavity tile also
 copies the wall records of its rows (64 bytes a row) into a 1 KB area.
+The sphere channel's flat tiles (a run of C elements of a plane across row
+ends) must stage, in every slot element, the plane element its pull reads:
+the run shifted by -e_y rows, 8 guard elements a side, wrapped around the
+periodic y and z.
 """
 import ctypes
 
@@ -27,18 +31,64 @@ MAX_TX = (1 << 20) - 1  # an mbarrier's transaction count
 REC_BYTES, REC_AREA = 64, 1024  # wall record of a row; record area of a stage
 
 
-def plan(nx, ny, nz, wrap):
+MODES = {"cavity": 0, "tgv": 1, "sphere": 2}
+GUARD = 8  # guard elements a side of a flat tile's slot
+
+
+def plan(nx, ny, nz, mode):
     lib = api.load_library()
     fn = lib.imexlb_debug_stage_plan
     fn.restype = ctypes.c_int64
     fn.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
-    geo = np.zeros(8, np.int32)
-    n = fn(nx, ny, nz, int(wrap), geo.ctypes.data, None, 0)
+    geo = np.zeros(10, np.int32)
+    n = fn(nx, ny, nz, mode, geo.ctypes.data, None, 0)
     if n < 0:
         return None, None
     runs = np.zeros((n, 6), np.int32)
-    assert fn(nx, ny, nz, int(wrap), geo.ctypes.data, runs.ctypes.data, n) == n
-    return dict(zip(("P", "R", "cap", "nty", "sq", "sz", "pitch", "base"), geo.tolist())), runs
+    assert fn(nx, ny, nz, mode, geo.ctypes.data, runs.ctypes.data, n) == n
+    keys = ("P", "R", "cap", "nty", "sq", "sz", "pitch", "base", "flat", "C")
+    return dict(zip(keys, geo.tolist())), runs
+
+
+def check_flat(g, runs, nx, ny, nz):
+    """A flat tile's slots hold, element by element, the plane elements the
+    tile's pulls read (with guards), wrapped around the periodic y and z."""
+    P, cap, C = g["P"], g["cap"], g["C"]
+    NP = ny * P
+    assert g["sz"] == NP and C + 2 * GUARD <= cap and C % 16 == 0
+    t, q, pop, src, dst, nbytes = (runs[:, i].astype(np.int64) for i in range(6))
+    assert np.all(nbytes > 0) and np.all(nbytes % 16 == 0)
+    assert np.all((src * ELEM) % 16 == 0) and np.all((dst * ELEM) % 16 == 0)
+    assert np.all(pop == q)
+    rel = src - g["base"]
+    plane, off = rel // g["sz"], rel % g["sz"]
+    nel = nbytes // ELEM
+    assert np.all(rel >= 0) and np.all(plane < nz) and np.all(off + nel <= NP), "copy leaves its plane"
+    slot0 = dst - q * cap
+    assert np.all(slot0 >= 0) and np.all(slot0 + nel <= cap)
+    per_tile = np.bincount(t, weights=nbytes, minlength=g["nty"] * nz)
+    assert per_tile.max() <= MAX_TX
+    # every slot element once, with the plane element its pull reads: on the
+    # planes where z wraps and one inside plane (the others repeat it)
+    nty = g["nty"]
+    for k in sorted({0, 1, nz // 2, nz - 1}):
+        sel = (t // nty) == k
+        width = C + 2 * GUARD
+        have = np.full((nty, 27, width), -1, np.int64)  # (plane, element) as plane * NP + element
+        count = np.zeros((nty, 27, width), np.int64)
+        for i in np.nonzero(sel)[0]:
+            tt, qq, s0, n = int(t[i]) % nty, int(q[i]), int(slot0[i]), int(nel[i])
+            have[tt, qq, s0:s0 + n] = plane[i] * NP + off[i] + np.arange(n)
+            count[tt, qq, s0:s0 + n] += 1
+        e0 = np.arange(nty) * C
+        n_tile = np.minimum(C, NP - e0)
+        o = np.arange(width)
+        for qq in range(27):
+            want = ((k - EZ[qq]) % nz) * NP + (e0[:, None] - EY[qq] * P - GUARD + o[None, :]) % NP
+            used = o[None, :] < (n_tile[:, None] + 2 * GUARD)
+            assert np.all(count[:, qq][used] == 1), (k, qq, "slot element not written exactly once")
+            assert np.all(have[:, qq][used] == want[used]), (k, qq)
+            assert np.all(count[:, qq][~used] == 0), (k, qq, "elements copied beyond the tile")
 
 
 def shapes():
@@ -56,7 +106,10 @@ def shapes():
         out.add(("cavity", (e, e, e)))
     for L in (256, 384, 512, 768):
         out.add(("sphere", (L, L // 4, L // 4)))
-    out.add(("sphere", (64, 16, 16)))
+    # sphere channels of the GPU tests
+    for n in ((64, 16, 16), (64, 16, 18), (96, 24, 24), (96, 32, 32), (288, 24, 24), (48, 16, 16),
+              (40, 12, 14), (96, 20, 20), (72, 12, 12), (144, 36, 36), (192, 48, 48)):
+        out.add(("sphere", n))
     return sorted(out)
 
 
@@ -64,10 +117,15 @@ def shapes():
 def test_stage_copy_plan(case, n):
     nx, ny, nz = n
     wrap = case != "cavity"
-    g, runs = plan(nx, ny, nz, wrap)
+    g, runs = plan(nx, ny, nz, MODES[case])
     if g is None:
         assert nx % 2 or nx > 1024 or (not wrap and nx < 4), f"{case} {n} should be staged"
         return
+    if g["flat"]:
+        assert case == "sphere"
+        check_flat(g, runs, nx, ny, nz)
+        return
+    assert case != "sphere" or ny * g["P"] < 1008 + 2 * g["P"] + 16, f"{case} {n} should take flat tiles"
     P, R, cap = g["P"], g["R"], g["cap"]
     assert g["pitch"] == P and P % 8 == 0 and P >= nx
     assert 1 <= R <= ny and R * P <= cap and g["nty"] * R >= ny
