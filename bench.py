@@ -92,6 +92,9 @@ WORKLOADS = {
                            u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
     "sphere768-f64": dict(case="sphere", bc="standard", storage="f64", arith="fast", n=(768, 192, 192), Re=100,
                           u0=0.05, R=32.0, lid_u=0.0, inlet_u=0.05, sphere_d=32.0, sphere_c=(192.0, 96.0, 96.0)),
+    # the served stream's middle sphere channel (L = 384, D = L / 24)
+    "sphere384-f16": dict(case="sphere", bc="standard", storage="f16", arith="fast", n=(384, 96, 96), Re=100,
+                          u0=0.05, R=16.0, lid_u=0.0, inlet_u=0.05, sphere_d=16.0, sphere_c=(96.0, 48.0, 48.0)),
     # batched solves: 256 seeded TGV / cavity instances (imexlb_b200.batch) in
     # one engine; case/n/R/Re/u0 name the instance the CPU baseline times
     # FP16 storage, FP32 for the instances with tau - 1/2 < 0.015 (imexlb_b200.batch)

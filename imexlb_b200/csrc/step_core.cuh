@@ -81,7 +81,7 @@ __device__ __forceinline__ double div3_rn(double x) {
 }
 
 // RN(x / d) for d > 0, given z = RN(1/d), proven on the fast path and
-// deferred to IEEE division otherwise:
+// deferred to IEEE division otherwise (div_rn_fast, then div_rn_slow):
 //   q0 = RN(x z), r0 = x - q0 d (fma), q1 = RN(q0 + r0 z)   (Markstein 1990)
 //   r1 = x - q1 d by fma is exact whenever q1 is within one ulp of x/d (the
 //   remainder is then an integer multiple of ulp(q1) ulp(d) below 2^53 of them);
@@ -94,21 +94,29 @@ __device__ __forceinline__ double div3_rn(double x) {
 //   all zero q1 is no power of two, gap_below(q1) = ulp(q1) and the bound is
 //   d * 2^(E - 53), E the exponent of q1; the other quotients (a 2^-20
 //   fraction, powers of two among them) take __ddiv_rn.
-//   A zero numerator gives q1 = x exactly (IEEE: +-0 / d = +-0 for d > 0);
-//   it is common (a cell at rest has f = feq) and is returned without the
-//   division, as are an infinite numerator (+-inf / d = +-inf) and a NaN (the
-//   quotient is NaN) in a lattice that overflowed.
-__device__ __forceinline__ double div_rn(double x, double d, double z) {
+//   A zero numerator is returned as it is (IEEE: +-0 / d = +-0 for d > 0); it
+//   is common (a cell at rest has f = feq).  div_rn_fast is this fast path:
+//   *q is RN(x / d) when it returns true; otherwise the caller finishes with
+//   div_rn_slow, which also returns an infinite numerator (+-inf / d = +-inf)
+//   and a NaN (the quotient is NaN) of a lattice that overflowed as they are.
+//   Branch-free, so that the collision's 27 divisions form one straight run
+//   of code.
+__device__ __forceinline__ bool div_rn_fast(double x, double d, double z, double* q) {
   const double q0 = __dmul_rn(x, z);
   const double r0 = __fma_rn(-q0, d, x);
   const double q1 = __fma_rn(r0, z, q0);
   const double r1 = __fma_rn(-q1, d, x);
   const int hi = __double2hiint(q1);
-  const int he = (hi & 0x7ff00000) - (53 << 20);  // exponent field of ulp(q1) / 2, in the high word
-  if (he > 0 && (hi & 0x000fffff) != 0 && fabs(r1) < __dmul_rn(d, __hiloint2double(he, 0))) return q1;
-  if (x == 0.0 || !isfinite(x)) return x;
-  return __ddiv_rn(x, d);
+  const int he = (hi & 0x7ff00000) - (53 << 20);
+  const bool ok = he > 0 && (hi & 0x000fffff) != 0 && fabs(r1) < __dmul_rn(d, __hiloint2double(he, 0));
+  const bool zero = x == 0.0;
+  *q = zero ? x : q1;
+  return ok || zero;
 }
+
+// The cases div_rn_fast leaves: non-finite numerators (returned as they
+// are) and the rest through IEEE division.
+__device__ __forceinline__ double div_rn_slow(double x, double d) { return isfinite(x) ? __ddiv_rn(x, d) : x; }
 
 template <class R>
 __device__ __forceinline__ R wgt(int cls) {
@@ -469,17 +477,36 @@ __device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, con
   R tp3[4], udu15;
   feq_prep<R, EXACT>(u, v, w, p, tp3, udu15);
   using A = Ar<R, EXACT>;
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
-    R fs;
-    if constexpr (EXACT) {
-      fs = A::sub(f[q], div_rn(A::sub(f[q], feq), a.tau_half, a.omega));
-    } else {
-      fs = f[q] - R(a.omega) * (f[q] - feq);
+  if constexpr (EXACT) {
+    // f - (f - feq) / (tau0 + 1/2) with a correctly rounded division: every
+    // population through the branch-free fast path and stored; the few the
+    // fast path cannot accept (near-ties, tiny or non-finite numerators) are
+    // computed again through IEEE division and stored over the first value
+    uint32_t redo = 0u;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+      double quot;
+      if (!div_rn_fast(A::sub(f[q], feq), a.tau_half, a.omega, &quot)) redo |= 1u << q;
+      pl.store(q, b, encode<S>(A::sub(f[q], quot), q, a.enc));
+    });
+    if (redo) {
+      static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        if ((redo >> q) & 1u) {
+          const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+          pl.store(q, b, encode<S>(A::sub(f[q], div_rn_slow(A::sub(f[q], feq), a.tau_half)), q, a.enc));
+        }
+      });
     }
-    pl.store(q, b, encode<S>(fs, q, a.enc));
-  });
+  } else {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+      const R fs = f[q] - R(a.omega) * (f[q] - feq);
+      pl.store(q, b, encode<S>(fs, q, a.enc));
+    });
+  }
 }
 
 // Two cells at once in FP32 with Blackwell's paired FP32 instructions: every

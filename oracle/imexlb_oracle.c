@@ -838,7 +838,7 @@ int oracle_check_div(long n, unsigned long long seed, int planted, long* fallbac
       double v;
       unsigned long long u;
     } qb = {q1};
-    /* the device's test on the high word of q1 (step_core.cuh div_rn) */
+    /* the device's test on the high word of q1 (step_core.cuh div_rn_fast) */
     const int hi = (int)(qb.u >> 32);
     const int he = (hi & 0x7ff00000) - (53 << 20);
     double q;
