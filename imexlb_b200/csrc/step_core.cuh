@@ -118,6 +118,11 @@ __device__ __forceinline__ bool div_rn_fast(double x, double d, double z, double
 // are) and the rest through IEEE division.
 __device__ __forceinline__ double div_rn_slow(double x, double d) { return isfinite(x) ? __ddiv_rn(x, d) : x; }
 
+// Populations per redo group of the EXACT collision (a divisor of 27): the
+// fast quotients of a group form one straight run of code, and the group's
+// f values stay live until its redo check.
+constexpr int EXACT_GROUP = 3;
+
 template <class R>
 __device__ __forceinline__ R wgt(int cls) {
   return cls == 0 ? R(8.0 / 27.0) : (cls == 1 ? R(2.0 / 27.0) : (cls == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0)));
@@ -478,27 +483,32 @@ __device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, con
   feq_prep<R, EXACT>(u, v, w, p, tp3, udu15);
   using A = Ar<R, EXACT>;
   if constexpr (EXACT) {
-    // f - (f - feq) / (tau0 + 1/2) with a correctly rounded division: every
-    // population through the branch-free fast path and stored; the few the
-    // fast path cannot accept (near-ties, tiny or non-finite numerators) are
-    // computed again through IEEE division and stored over the first value
-    uint32_t redo = 0u;
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
-      double quot;
-      if (!div_rn_fast(A::sub(f[q], feq), a.tau_half, a.omega, &quot)) redo |= 1u << q;
-      pl.store(q, b, encode<S>(A::sub(f[q], quot), q, a.enc));
-    });
-    if (redo) {
-      static_for<0, Q>([&](auto qc) {
+    // f - (f - feq) / (tau0 + 1/2) with a correctly rounded division, in
+    // groups of EXACT_GROUP populations: each population of a group through
+    // the branch-free fast path and stored; the few the fast path cannot
+    // accept (near-ties, tiny or non-finite numerators) are computed again
+    // through IEEE division and stored over the first value before the next
+    // group starts, so that only one group's f stays live for that pass
+    static_for<0, Q / EXACT_GROUP>([&](auto gc) {
+      constexpr int g0 = decltype(gc)::value * EXACT_GROUP;
+      uint32_t redo = 0u;
+      static_for<g0, g0 + EXACT_GROUP>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        if ((redo >> q) & 1u) {
-          const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
-          pl.store(q, b, encode<S>(A::sub(f[q], div_rn_slow(A::sub(f[q], feq), a.tau_half)), q, a.enc));
-        }
+        const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+        double quot;
+        if (!div_rn_fast(A::sub(f[q], feq), a.tau_half, a.omega, &quot)) redo |= 1u << q;
+        pl.store(q, b, encode<S>(A::sub(f[q], quot), q, a.enc));
       });
-    }
+      if (redo) {
+        static_for<g0, g0 + EXACT_GROUP>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          if ((redo >> q) & 1u) {
+            const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
+            pl.store(q, b, encode<S>(A::sub(f[q], div_rn_slow(A::sub(f[q], feq), a.tau_half)), q, a.enc));
+          }
+        });
+      }
+    });
   } else {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
