@@ -73,6 +73,9 @@ WORKLOADS = {
                           u0=0.1, R=128.0, lid_u=0.1),
     "cavity128-f64-refbc-fast": dict(case="cavity", bc="reference", storage="f64", arith="fast", n=(128, 128, 128),
                                      Re=100, u0=0.1, R=128.0, lid_u=0.1),
+    # the same passes resolved per link inside the step kernel (no gather)
+    "cavity128-f64-refbc-links": dict(case="cavity", bc="reference-links", storage="f64", arith="exact",
+                                      n=(128, 128, 128), Re=100, u0=0.1, R=128.0, lid_u=0.1),
     "cavity128-bf16": dict(case="cavity", bc="standard", storage="bf16", arith="fast", n=(128, 128, 128), Re=1000,
                            u0=0.1, R=128.0, lid_u=0.1),
     "cavity256-f64": dict(case="cavity", bc="standard", storage="f64", arith="fast", n=(256, 256, 256), Re=1000,

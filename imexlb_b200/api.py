@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libimexlb.so")
 
 CASES = {"tgv": 0, "cavity": 1, "sphere": 2}
-BCS = {"reference": 0, "standard": 1, "slab": 2}
+BCS = {"reference": 0, "standard": 1, "slab": 2, "reference-links": 3}
 STORAGES = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 ARITHS = {"exact": 0, "fast": 1}
 REDUCE = {"mass": 0, "kinetic": 1, "residual": 2, "drag": 3, "umax": 4}

@@ -8,7 +8,7 @@
 //   --steps N        override the step count (System's Time)
 //   --inter N        output interval (System's inter)
 //   --storage f64|f32|f16|bf16
-//   --bc reference|standard
+//   --bc reference|reference-links|standard
 //   --arith exact|fast
 //   --no-output      do not write output<n>.plt
 #pragma once
@@ -51,7 +51,9 @@ inline Options parse(int argc, char** argv) {
       const std::string v = next();
       o.storage = v == "f32" ? IMEXLB_F32 : v == "f16" ? IMEXLB_F16 : v == "bf16" ? IMEXLB_BF16 : IMEXLB_F64;
     } else if (s == "--bc") {
-      o.bc = next() == "standard" ? IMEXLB_BC_STANDARD : IMEXLB_BC_REFERENCE;
+      const std::string v = next();
+      o.bc = v == "standard" ? IMEXLB_BC_STANDARD : v == "reference-links" ? IMEXLB_BC_REFERENCE_LINKS
+                                                                             : IMEXLB_BC_REFERENCE;
     } else if (s == "--arith") {
       o.arith = next() == "fast" ? IMEXLB_ARITH_FAST : IMEXLB_ARITH_EXACT;
     } else {

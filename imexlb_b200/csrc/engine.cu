@@ -92,6 +92,9 @@ struct EngArgs {
   int parity;
   int store;
   int* err;  // set non-zero by a staged kernel that gave up waiting
+  // per slot: steps the instance has taken (its stochastic-rounding seed is
+  // the hash of this count, as for a single lattice)
+  const uint32_t* seed = nullptr;
 };
 
 // What the consumer warps of a staged engine kernel need of a tile beyond
@@ -106,6 +109,7 @@ struct __align__(16) TileHdr {
   int j0, k;
   int skip;          // the instance has taken its steps: no copies, no update
   int store;         // write the moments (the call's last step or the instance's)
+  uint32_t seed;     // the instance's stochastic-rounding seed for this step
 };
 constexpr size_t TILE_HDR_BYTES = (sizeof(TileHdr) + 15) & ~static_cast<size_t>(15);
 
@@ -115,11 +119,12 @@ constexpr int ENG_NO_LIMIT = 0x7fffffff;
 // Before each step a tile reads its instance's steps left: 0 skips the tile,
 // 1 (the instance's last step) also writes the moments.  engine_tick counts
 // them down after the step.
-__global__ void engine_tick(int* left, int n) {
+__global__ void engine_tick(int* left, uint32_t* taken, int n) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < n) {
     const int l = left[s];
     if (l > 0 && l != ENG_NO_LIMIT) left[s] = l - 1;
+    if (l != 0) taken[s] += 1u;
   }
 }
 
@@ -169,7 +174,10 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
       int4* to = reinterpret_cast<int4*>(&sh);
       for (int w = threadIdx.x; w < static_cast<int>(sizeof(EngInst) / 16); w += blockDim.x) to[w] = from[w];
       __syncthreads();
-      if (threadIdx.x == 0) sh.a.store = ea.store || left == 1;
+      if (threadIdx.x == 0) {
+        sh.a.store = ea.store || left == 1;
+        sh.a.seed = sr_hash(ea.seed[tile.slot]);
+      }
       __syncthreads();
       loaded = tile.slot;
     }
@@ -250,7 +258,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       const int left = ea.left[d.slot];
       if (lane == 0)
         hdr[sn] = TileHdr{src_buf, const_cast<void*>(d.buf[1 - cur]), REC ? d.rec[1 - cur] : nullptr, d.geo, d.j0,
-                          d.k, left == 0, ea.store || left == 1};
+                          d.k, left == 0, ea.store || left == 1, sr_hash(ea.seed[d.slot])};
       if (left == 0)
         issue_skip(&full[sn]);
       else
@@ -266,7 +274,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       const int left = ea.left[tile.slot];
       if (lane == 0)
         hdr[sn] = TileHdr{in->buf[cur], in->buf[1 - cur], REC ? in->rec[1 - cur] : nullptr, in->geo, tile.j0, tile.k,
-                          left == 0, ea.store || left == 1};
+                          left == 0, ea.store || left == 1, sr_hash(ea.seed[tile.slot])};
       if (left == 0)
         issue_skip(&full[sn]);
       else
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
       const Geo g = h.geo;
       consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k,
-                               h.store != 0, rec_stage(s), h.rec);
+                               h.store != 0, h.seed, rec_stage(s), h.rec);
     }
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
@@ -561,6 +569,7 @@ struct imexlb_engine {
   DevBuf<StagedTile> d_stiles;
   std::vector<StagedTile> h_stiles;
   DevBuf<int> d_left;       // per slot: steps left (ENG_NO_LIMIT: no limit)
+  DevBuf<uint32_t> d_taken; // per slot: steps taken (counted on the device by engine_tick)
   std::vector<int> h_left;  // host copy, counted down with the steps run
   DevBuf<double> d_part;
   DevBuf<int> d_seg;  // begin[nseg], end[nseg]
@@ -763,7 +772,7 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
 
 cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
   EngArgs ea{e->d_inst.p, e->d_tiles.p, e->d_stiles.p, e->d_left.p, static_cast<int>(e->h_tiles.size()), parity,
-              store, e->d_err.p};
+              store, e->d_err.p, e->d_taken.p};
   if (ea.ntiles == 0) return cudaSuccess;
   // one pass per storage format present (instances of several formats share
   // the engine and its step graph)
@@ -780,7 +789,7 @@ cudaError_t launch_engine(const imexlb_engine* e, int parity, int store) {
   if (err == cudaSuccess && present(IMEXLB_BF16)) err = launch_groups<Store::BF16, false>(e, ea);
   if (err != cudaSuccess) return err;
   const int n = static_cast<int>(e->h_left.size());
-  engine_tick<<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_left.p, n);
+  engine_tick<<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_left.p, e->d_taken.p, n);
   return cudaGetLastError();
 }
 
@@ -839,6 +848,8 @@ int imexlb_engine_create(imexlb_storage storage, imexlb_arith arith, size_t budg
   IMX_ECUDA(e->d_inst.reserve(max_instances));
   e->h_left.assign(max_instances, ENG_NO_LIMIT);
   IMX_ECUDA(e->d_left.reserve(max_instances));
+  IMX_ECUDA(e->d_taken.reserve(max_instances));
+  IMX_ECUDA(cudaMemset(e->d_taken.p, 0, max_instances * sizeof(uint32_t)));
   IMX_ECUDA(cudaMemcpy(e->d_left.p, e->h_left.data(), max_instances * sizeof(int), cudaMemcpyHostToDevice));
   int dev = 0, sms = 148;
   IMX_ECUDA(cudaGetDevice(&dev));
@@ -997,6 +1008,7 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
     a.enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
   a.enc.unit = store_unit(static_cast<Store>(storage));
+  a.enc.sr = stochastic_rounding_for(d->kase, storage);
   in.rule = static_cast<int>(d->kase == IMEXLB_TGV ? CaseRule::None
                                                    : (d->kase == IMEXLB_CAVITY ? CaseRule::CavityStd : CaseRule::SphereStd));
   if (d->kase == IMEXLB_SPHERE) {
@@ -1063,6 +1075,7 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
   e->slots[s] = sl;
   e->h_left[s] = ENG_NO_LIMIT;
   IMX_ECUDA(cudaMemcpyAsync(e->d_left.p + s, &e->h_left[s], sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  IMX_ECUDA(cudaMemsetAsync(e->d_taken.p + s, 0, sizeof(uint32_t), e->stream));
   e->dirty = true;
   *slot_out = s;
   return IMEXLB_OK;
@@ -1314,6 +1327,8 @@ int imexlb_engine_restore(imexlb_engine* e, const imexlb_instance_desc* d, const
   if (in.rec[0]) IMX_ECUDA(launch_cavity_records(sl.L, in.buf[0], in.rec[0], e->stream));
   p += c.buf_bytes;
   IMX_ECUDA(cudaMemcpyAsync(in.a.mu, p, c.mom_bytes, cudaMemcpyHostToDevice, e->stream));
+  const uint32_t taken = static_cast<uint32_t>(c.steps);
+  IMX_ECUDA(cudaMemcpyAsync(e->d_taken.p + slot, &taken, sizeof taken, cudaMemcpyHostToDevice, e->stream));
   IMX_ECUDA(cudaStreamSynchronize(e->stream));
   sl.steps = c.steps;
   sl.have_prev = false;

@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       break;
     }
     const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
-    consume_tile<S, B, RULE>(a, pl, g, st, tile_origin(g, t), tile_plane(g, t), a.store != 0, rec_stage(s), a.rec_dst);
+    consume_tile<S, B, RULE>(a, pl, g, st, tile_origin(g, t), tile_plane(g, t), a.store != 0, a.seed, rec_stage(s),
+                             a.rec_dst);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
     if (__any_sync(0xffffffffu, *abort_v != 0)) break;

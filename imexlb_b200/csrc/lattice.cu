@@ -597,11 +597,13 @@ std::vector<std::shared_ptr<const GhostSetup>> g_setups;  // most recent last
 constexpr size_t SETUP_CACHE = 4;
 
 std::shared_ptr<const GhostSetup> ghost_setup(const imexlb_params& P, const Layout& L, const int32_t* usr_padded,
-                                              std::string* err) {
+                                              bool per_link, std::string* err) {
   {
     std::lock_guard<std::mutex> lock(g_setup_mu);
     for (const auto& g : g_setups)
-      if (g->kase == P.kase && g->nx == P.nx && g->ny == P.ny && g->nz == P.nz && g->elem == L.elem) return g;
+      if (g->kase == P.kase && g->nx == P.nx && g->ny == P.ny && g->nz == P.nz && g->elem == L.elem &&
+          g->faces == per_link)
+        return g;
   }
   GhostPlan plan;
   if (!build_ghost_plan_keys(static_cast<int>(P.kase), P.nx, P.ny, P.nz, usr_padded, &plan, err)) return nullptr;
@@ -628,7 +630,27 @@ std::shared_ptr<const GhostSetup> ghost_setup(const imexlb_params& P, const Layo
     const int64_t src = plan.src[n];
     g->s[n] = src >= 0 ? to_dev(src) : (src == -1 ? -1 : -to_dev(-src - 2) - 2);
   }
-  if (P.kase == IMEXLB_CAVITY && (L.elem == 8 || L.elem == 4) && face_codes_for(L, g->t, g->s, g->codes, g->base, g->dim)) {
+  // In target order the gather's stores run along the ghost rows of each
+  // population plane, and their sources (mirror or shifted rows) with them;
+  // the order of the copies does not matter (no target is a source of the
+  // same step).
+  {
+    std::vector<int64_t> order(g->t.size());
+    for (size_t n = 0; n < order.size(); ++n) order[n] = static_cast<int64_t>(n);
+    std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return g->t[x] < g->t[y]; });
+    std::vector<int64_t> t2(order.size()), s2(order.size());
+    for (size_t n = 0; n < order.size(); ++n) {
+      t2[n] = g->t[order[n]];
+      s2[n] = g->s[order[n]];
+    }
+    g->t.swap(t2);
+    g->s.swap(s2);
+  }
+  if (per_link) {
+    if (!face_codes_for(L, g->t, g->s, g->codes, g->base, g->dim)) {
+      if (err) *err = "the per-link form does not cover this lattice's boundary passes";
+      return nullptr;
+    }
     g->faces = true;
     for (int k = 0; k < P.nz; ++k)
       for (int j = 0; j < P.ny; ++j)
@@ -693,8 +715,14 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   *out = nullptr;
   imexlb_params P = *pin;
   if (P.kase < IMEXLB_TGV || P.kase > IMEXLB_SPHERE) return fail(IMEXLB_E_ARG, "unknown case");
-  if (P.bc != IMEXLB_BC_REFERENCE && P.bc != IMEXLB_BC_STANDARD && P.bc != IMEXLB_BC_SLAB)
+  if (P.bc != IMEXLB_BC_REFERENCE && P.bc != IMEXLB_BC_STANDARD && P.bc != IMEXLB_BC_SLAB &&
+      P.bc != IMEXLB_BC_REFERENCE_LINKS)
     return fail(IMEXLB_E_ARG, "unknown boundary kind");
+  if (P.bc == IMEXLB_BC_REFERENCE_LINKS &&
+      (P.kase != IMEXLB_CAVITY || (P.storage != IMEXLB_F64 && P.storage != IMEXLB_F32)))
+    return fail(IMEXLB_E_UNSUPPORTED, "per-link reference boundaries are for the cavity in FP64 or FP32 storage");
+  const bool per_link = P.bc == IMEXLB_BC_REFERENCE_LINKS;
+  const bool ref_bc = P.bc == IMEXLB_BC_REFERENCE || per_link;
   if (P.bc == IMEXLB_BC_SLAB && (P.kase != IMEXLB_CAVITY || (P.storage != IMEXLB_F64 && P.storage != IMEXLB_F32)))
     return fail(IMEXLB_E_UNSUPPORTED, "the slab boundaries are for the cavity in FP64 or FP32 storage");
   if (P.storage < IMEXLB_F64 || P.storage > IMEXLB_BF16) return fail(IMEXLB_E_ARG, "unknown storage");
@@ -706,7 +734,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   const bool ref_sphere = P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_REFERENCE;
   if (ref_sphere && (P.nx - 1) / 8 + (P.nx - 1) / 64.0 + 2 >= std::min(P.ny, P.nz))
     return fail(IMEXLB_E_ARG, "reference sphere (centre (nx-1)/8 on every axis) does not fit in ny, nz");
-  if (P.kase == IMEXLB_CAVITY && P.bc != IMEXLB_BC_REFERENCE && P.lid_u == 0.0) P.lid_u = P.u0;
+  if (P.kase == IMEXLB_CAVITY && !ref_bc && P.lid_u == 0.0) P.lid_u = P.u0;
   if (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_STANDARD) {
     if (P.inlet_u == 0.0) P.inlet_u = P.u0;
     if (P.sphere_d == 0.0) P.sphere_d = P.nx / 24.0;
@@ -721,7 +749,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   h->P = P;
   h->P.ran = nullptr;
   h->stream = static_cast<cudaStream_t>(P.stream);
-  const bool ghost = P.bc == IMEXLB_BC_REFERENCE && P.kase != IMEXLB_TGV;
+  const bool ghost = ref_bc && P.kase != IMEXLB_TGV;
   h->cfg.bc = P.kase == IMEXLB_TGV ? Bc::Periodic : (ghost ? Bc::Ghost : Bc::Standard);
   h->cfg.store = static_cast<Store>(P.storage);
   h->cfg.exact = P.storage == IMEXLB_F64 && P.arith == IMEXLB_ARITH_EXACT;
@@ -745,6 +773,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
     h->enc.inv_scale[q] = static_cast<float>(1.0 / sc);
   }
   h->enc.unit = store_unit(static_cast<Store>(P.storage));
+  h->enc.sr = stochastic_rounding_for(P.kase, P.storage);
 
   const size_t padded = static_cast<size_t>(L.ex) * L.ey * L.ez;
   if (P.kase == IMEXLB_SPHERE) {
@@ -861,7 +890,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
   if (ghost) {
     std::string err;
     const std::shared_ptr<const GhostSetup> g =
-        ghost_setup(P, L, P.kase == IMEXLB_SPHERE ? h->usr_padded.data() : nullptr, &err);
+        ghost_setup(P, L, P.kase == IMEXLB_SPHERE ? h->usr_padded.data() : nullptr, per_link, &err);
     if (!g) return fail(IMEXLB_E_UNSUPPORTED, err);
     if (g->faces) {
       // the step kernel resolves the passes per link: no gather; its face
@@ -906,6 +935,7 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
   if (nsteps < 0) return fail(IMEXLB_E_ARG, "negative step count");
   StepArgs a = h->base_args;
   for (int s = 0; s < nsteps; ++s) {
+    a.seed = sr_hash(static_cast<uint32_t>(h->steps));
     a.src = h->buf[h->cur].p;
     a.dst = h->buf[1 - h->cur].p;
     a.rec_src = h->rec[h->cur].p;

@@ -71,7 +71,28 @@ struct Encoding {
   float u_ref[3] = {0.f, 0.f, 0.f};
   float br_ref[Q] = {};
   float kref[Q] = {};  // -omega unit br_ref[q], the collision's share of it
+  uint32_t sr = 0;     // 2-byte formats: 1 = stochastic rounding of the stores
 };
+// Whether a lattice's 2-byte stores round stochastically (Encoding::sr):
+// yes for the cavity and the sphere channel, driven flows that settle into
+// a steady state, where round-to-nearest repeats the same error every step;
+// no for the Taylor-Green vortex, a decaying flow without a steady state,
+// whose error against FP64 is smaller with round-to-nearest (measured over
+// 2000-16000 steps of 64^3 and 96^3 vortices).  `kase` is an imexlb_case,
+// `storage` an imexlb_storage (2 = FP16, 3 = BF16).
+// The stochastic-rounding hash: the 32-bit "lowbias32" integer finaliser
+// (C. Wellons, hash-prospector, 2018).
+IMX_HDC uint32_t sr_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+inline uint32_t stochastic_rounding_for(int kase, int storage) {
+  return (storage == 2 || storage == 3) && kase != 0 ? 1u : 0u;
+}
 // Set u_ref, br_ref and kref of `enc` for the reference velocity (u, 0, 0)
 // and the relaxation rate omega.
 void set_reference_flow(Encoding& enc, double u, double omega);
@@ -96,6 +117,7 @@ struct StepArgs {
   int near_lo[3] = {0, 0, 0};       // box of cells that have solid links
   int near_hi[3] = {-1, -1, -1};
   int store = 0;  // write moments this step
+  uint32_t seed = 0;  // stochastic rounding: hash of the lattice's step count before this step
   Encoding enc;
   double feq_in[Q] = {};  // standard sphere: inlet equilibrium (deviation form)
   // ---- not read by the staged kernels

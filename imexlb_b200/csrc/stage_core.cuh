@@ -180,27 +180,36 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // try_wait that suspends at most about `hint_ns` (the instruction's own
 // suspend-time hint) before it reports the phase as not yet complete.
-__device__ __forceinline__ bool bar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+// Non-blocking test of the phase of `parity` (mbarrier.test_wait).
+__device__ __forceinline__ bool bar_test_wait(uint64_t* bar, uint32_t parity) {
   uint32_t done;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
       : "=r"(done)
-      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "r"(smem_addr(bar)), "r"(parity)
       : "memory");
   return done != 0;
 }
 
+// Below this a wait limit is finer than %globaltimer resolves: such a limit
+// gives up after one failed poll.
+constexpr uint64_t TIMER_FLOOR_NS = 1000;
+
 // Wait for the phase of `parity` to complete; false after about limit_ns.
-// A limit below a millisecond is also passed to each try_wait as its
-// suspend-time hint, since one try_wait may otherwise suspend for longer
-// than the limit.
+// A limit below a millisecond polls with the non-blocking test_wait, since
+// one try_wait may suspend for longer than the limit.
 __device__ __forceinline__ bool bar_wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
-  const bool short_limit = limit_ns < 1000000ull;
-  const uint32_t hint = static_cast<uint32_t>(short_limit ? limit_ns : 0ull);
-  if (short_limit ? bar_try_wait_hint(bar, parity, hint) : bar_try_wait(bar, parity)) return true;
+  if (limit_ns < 1000000ull) {
+    const uint64_t t0 = global_ns();
+    while (!bar_test_wait(bar, parity)) {
+      if (limit_ns < TIMER_FLOOR_NS || global_ns() - t0 > limit_ns) return false;
+    }
+    return true;
+  }
+  if (bar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (true) {
-    if (short_limit ? bar_try_wait_hint(bar, parity, hint) : bar_try_wait(bar, parity)) return true;
+    if (bar_try_wait(bar, parity)) return true;
     if (global_ns() - t0 > limit_ns) return false;
   }
 }
@@ -394,7 +403,7 @@ __device__ __forceinline__ void issue_skip(uint64_t* bar) {
 template <Store S, Bc B, CaseRule RULE, bool EDGE, bool FLAT = false, class P>
 __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                                 const int x, const int r, const int j0, const int k,
-                                                const bool store, const uint16_t* rec = nullptr,
+                                                const bool store, const uint32_t seed, const uint16_t* rec = nullptr,
                                                 uint16_t* rec_row = nullptr, const int flat_j = 0,
                                                 const int flat_pw = 0) {
   // flat tiles: the pair's row and its word in the slot come from the caller
@@ -508,7 +517,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
   // the lid plane is a wall plane: only EDGE pairs can sit under it
   const bool lid = RULE == CaseRule::CavityStd && EDGE && k == a.nz - 1;
   finish_pair_row<S, RULE, RULE == CaseRule::CavityStd>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store,
-                                                        links0, links1, rec_row);
+                                                        seed, links0, links1, rec_row);
 }
 
 // The cells of tile (j0, k) from stage `st`, shared by the block's threads:
@@ -522,7 +531,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
 // `rec_out` the record buffer this step writes.
 template <Store S, Bc B, CaseRule RULE, class P>
 __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
-                                             const int j0, const int k, const bool store,
+                                             const int j0, const int k, const bool store, const uint32_t seed,
                                              const uint16_t* rec = nullptr, uint16_t* rec_out = nullptr) {
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   const int half = g.P >> 1;
@@ -536,9 +545,9 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
       const int j = j0 + r;
       uint16_t* const rec_row = rec_tile + r * WallRecord::WORDS;
       if (wall_plane || j == 0 || j == a.ny - 1)
-        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
+        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
       else
-        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store, rec, rec_row);
+        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
     }
   } else if constexpr (RULE == CaseRule::SphereStd) {
     if (g.flat) {
@@ -551,19 +560,19 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
         const int e = e0 + 2 * p;
         const int j = e / g.P, x = e - j * g.P;
         if (x < a.nx)
-          pair_from_stage<S, B, RULE, true, true>(a, pl, g, st, x, 0, 0, k, store, nullptr, nullptr, j,
+          pair_from_stage<S, B, RULE, true, true>(a, pl, g, st, x, 0, 0, k, store, seed, nullptr, nullptr, j,
                                                   p + FLAT_GUARD / 2);
       }
     } else {
       for (int p = threadIdx.x; p < npairs; p += THREADS) {
         const int r = p / half, x = 2 * (p - r * half);
-        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed);
       }
     }
   } else {
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
       const int r = p / half, x = 2 * (p - r * half);
-      if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store);
+      if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed);
     }
   }
 }

@@ -222,6 +222,38 @@ __device__ __forceinline__ typename StoreT<S>::T encode(typename StoreT<S>::R x,
   }
 }
 
+// ------------------------------------------------------------ stochastic rounding
+// With Encoding::sr the 2-byte stores round stochastically: a pseudo-random
+// fraction of one unit in the last place of the stored format is added to
+// the FP32 value's bits and the sum is rounded toward zero, so the value
+// rounds up with probability equal to its distance from the one below and
+// the rounding error is zero on average (stochastic rounding, Forsythe
+// 1959; Connolly, Higham and Mary, SIAM J. Sci. Comput. 43, 2021).  In a
+// steady flow round-to-nearest makes the same error at the same cell every
+// step, a constant forcing whose effect on the velocity grows with the step
+// count; zero-mean errors do not accumulate that way.  The random bits are
+// a function of (cell, population, step) only: a lattice gives the same
+// bits alone, in the engine and resumed from a checkpoint.  Per cell (or
+// x-pair) one 32-bit integer hash of the cell index and the step's seed
+// (StepArgs::seed, itself the hash of the step count) gives x; population q
+// takes the bits of x * sr_mul(q) (sr_hash: lattice.h).
+// odd multipliers, one per population
+constexpr uint32_t sr_mul(int q) { return 0x9e3779b9u * (2u * static_cast<uint32_t>(q) + 1u) | 1u; }
+// Moments this small keep every stored value finite and in range, so the
+// bit additions cannot reach the exponent's top (NaN, infinity, or FP16
+// overflow, which round-to-nearest reports as infinity and rounding toward
+// zero would not); a cell outside the bound is stored with round-to-nearest.
+constexpr float SR_MOMENT_BOUND = 4.f;
+// one FP32 value to a 2-byte format, rounded stochastically with `r`
+template <Store S>
+__device__ __forceinline__ typename StoreT<S>::T sr_one(float x, uint32_t r) {
+  if constexpr (S == Store::F16) {
+    return __float2half_rz(__uint_as_float(__float_as_uint(x) + (r >> 19)));
+  } else {
+    return __ushort_as_bfloat16(static_cast<unsigned short>((__float_as_uint(x) + (r >> 16)) >> 16));
+  }
+}
+
 template <class T>
 __device__ __forceinline__ T ldg_stream(const T* p) {
   return __ldg(p);
@@ -510,10 +542,22 @@ __device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, con
       }
     });
   } else {
+    [[maybe_unused]] bool sr = false;
+    [[maybe_unused]] uint32_t x = 0;
+    if constexpr ((S == Store::F16 || S == Store::BF16) && RULE != CaseRule::None) {
+      sr = a.enc.sr && fabsf(u) + fabsf(v) + fabsf(w) + fabsf(p) < SR_MOMENT_BOUND;
+      x = sr_hash(static_cast<uint32_t>(cell) ^ a.seed);
+    }
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       const R feq = feq_of<q, R, EXACT>(u, v, w, tp3, udu15);
       const R fs = f[q] - R(a.omega) * (f[q] - feq);
+      if constexpr ((S == Store::F16 || S == Store::BF16) && RULE != CaseRule::None) {
+        if (sr) {
+          pl.store(q, b, sr_one<S>(fs * a.enc.scale[q], x * sr_mul(q)));
+          return;
+        }
+      }
       pl.store(q, b, encode<S>(fs, q, a.enc));
     });
   }
@@ -769,6 +813,24 @@ template <> struct Pack2<Store::BF16> {
   static __device__ __forceinline__ uint16_t from_f(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 };
 
+// An x-pair rounded stochastically (see sr_hash): `r` holds the random bits
+// of both cells.  FP16: cell x0 takes bits 19-31, x0 + 1 bits 6-18 (13 bits
+// below the FP16 significand each); BF16: bits 16-31 and 0-15.
+template <Store S>
+__device__ __forceinline__ uint32_t sr_pair(float2 g, uint32_t r) {
+  if constexpr (S == Store::F16) {
+    const float lo = __uint_as_float(__float_as_uint(g.x) + (r >> 19));
+    const float hi = __uint_as_float(__float_as_uint(g.y) + ((r >> 6) & 0x1fffu));
+    uint32_t word;
+    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(word) : "f"(hi), "f"(lo));
+    return word;
+  } else {
+    const uint32_t lo = __float_as_uint(g.x) + (r >> 16);
+    const uint32_t hi = __float_as_uint(g.y) + (r & 0xffffu);
+    return __byte_perm(lo, hi, 0x7632);
+  }
+}
+
 // pair (lo = cell x0, hi = cell x0 + 1) from two 16-bit halves
 __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { return (lo16 & 0xffffu) | (hi16 << 16); }
 
@@ -797,8 +859,8 @@ template <Store S, CaseRule RULE, bool REC = false, class P>
 __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
                                                 const bool live0, const bool live1, const bool store,
-                                                const uint32_t links0 = 0, const uint32_t links1 = 0,
-                                                uint16_t* rec_row = nullptr) {
+                                                const uint32_t seed, const uint32_t links0 = 0,
+                                                const uint32_t links1 = 0, uint16_t* rec_row = nullptr) {
   // -1.5 u.u below is formed two ways of the same value: the sphere's
   // staged kernels spill 24 bytes with one and none with the other
   constexpr bool NEGADD = RULE == CaseRule::SphereStd;
@@ -890,63 +952,94 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   [[maybe_unused]] const uint32_t rsel = rec_lo ? 0x5410u : 0x7632u;
   [[maybe_unused]] uint16_t* const rec_side = rec_row + (rec_hi ? WallRecord::HI : 0);
   [[maybe_unused]] uint32_t held = 0, pend = 0, w01 = 0, w23 = 0;
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    float2 Kq = K;
-    if constexpr (RULE == CaseRule::SphereStd) {
-      // minus the reference flow's equilibrium, omega unit br_ref[q]
-      Kq = add2rn(K, f2s(a.enc.kref[q]));
-    }
-    float2 gn;
-    if constexpr (q == 0) {
-      gn = fma2rn(g[q], keep, Kq);
-    } else {
-      // with e negated, so are the factors 4.5 and omega unit: same values.
-      // The sphere's kernels keep the signed e, whose negations cost no
-      // register for -omega unit (their registers are at the limit).
-      constexpr bool en = RULE != CaseRule::SphereStd && edu_neg<q>();
-      const float2 e = RULE != CaseRule::SphereStd ? edu2f<q>(u, v, w) : edu2<q>(u, v, w);
-      const float2 t = fma2rn(e, f2s(en ? -4.5f : 4.5f), f2s(3.0f));
-      const float2 h = mul2rn(e, f2s(en ? -om_u : om_u));
-      gn = fma2rn(h, t, fma2rn(g[q], keep, Kq));
-    }
-    if (live0 && live1) {
-      const uint32_t word = Pack2<S>::from_f2(gn);
-      pl.store_pair(q, b, word);
-      if constexpr (REC) {
-        // slot m of a side holds the population of pair m that leaves the
-        // box through that wall: e_x = -1 (q = P_m + 1) at x = 0, e_x = +1
-        // (q = P_m) at x = nx - 1
-        constexpr int ex = D3Q27::ex[q];
-        if constexpr (ex > 0) {
-          held = word;
-        } else if constexpr (ex < 0) {
-          constexpr int m = WallRecord::slot(q);
-          const uint32_t wv = rec_lo ? word : held;
-          if constexpr (m % 2 == 0) {
-            pend = wv;
-          } else {
-            const uint32_t pk = __byte_perm(pend, wv, rsel);
-            if constexpr (m == 1) w01 = pk;
-            if constexpr (m == 3) {
-              if (rec_any) *reinterpret_cast<uint2*>(rec_side) = make_uint2(w01, pk);
+  // Collision and stores; a pair whose two cells are both updated (every
+  // pair but those beside a solid or past the lattice's end) takes a copy of
+  // the loop without the per-population choice between a paired and two
+  // half stores.
+  // With stochastic rounding (Encoding::sr, for cells whose moments are
+  // within SR_MOMENT_BOUND) the pair's random bits come from x.
+  auto collide_store = [&](auto both_c, auto sr_c, const uint32_t x) __attribute__((always_inline)) {
+    constexpr bool BOTH = decltype(both_c)::value;
+    constexpr bool SR = decltype(sr_c)::value;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      float2 Kq = K;
+      if constexpr (RULE == CaseRule::SphereStd) {
+        // minus the reference flow's equilibrium, omega unit br_ref[q]
+        Kq = add2rn(K, f2s(a.enc.kref[q]));
+      }
+      float2 gn;
+      if constexpr (q == 0) {
+        gn = fma2rn(g[q], keep, Kq);
+      } else {
+        // with e negated, so are the factors 4.5 and omega unit: same values.
+        // The sphere's kernels keep the signed e, whose negations cost no
+        // register for -omega unit (their registers are at the limit).
+        constexpr bool en = RULE != CaseRule::SphereStd && edu_neg<q>();
+        const float2 e = RULE != CaseRule::SphereStd ? edu2f<q>(u, v, w) : edu2<q>(u, v, w);
+        const float2 t = fma2rn(e, f2s(en ? -4.5f : 4.5f), f2s(3.0f));
+        const float2 h = mul2rn(e, f2s(en ? -om_u : om_u));
+        gn = fma2rn(h, t, fma2rn(g[q], keep, Kq));
+      }
+      uint32_t word;
+      if constexpr (SR)
+        word = sr_pair<S>(gn, x * sr_mul(q));
+      else
+        word = Pack2<S>::from_f2(gn);
+      if constexpr (BOTH) {
+        pl.store_pair(q, b, word);
+        if constexpr (REC) {
+          // slot m of a side holds the population of pair m that leaves the
+          // box through that wall: e_x = -1 (q = P_m + 1) at x = 0, e_x = +1
+          // (q = P_m) at x = nx - 1
+          constexpr int ex = D3Q27::ex[q];
+          if constexpr (ex > 0) {
+            held = word;
+          } else if constexpr (ex < 0) {
+            constexpr int m = WallRecord::slot(q);
+            const uint32_t wv = rec_lo ? word : held;
+            if constexpr (m % 2 == 0) {
+              pend = wv;
+            } else {
+              const uint32_t pk = __byte_perm(pend, wv, rsel);
+              if constexpr (m == 1) w01 = pk;
+              if constexpr (m == 3) {
+                if (rec_any) *reinterpret_cast<uint2*>(rec_side) = make_uint2(w01, pk);
+              }
+              if constexpr (m == 5) w23 = pk;
+              if constexpr (m == 7) {
+                if (rec_any) *reinterpret_cast<uint2*>(rec_side + 4) = make_uint2(w23, pk);
+              }
             }
-            if constexpr (m == 5) w23 = pk;
-            if constexpr (m == 7) {
-              if (rec_any) *reinterpret_cast<uint2*>(rec_side + 4) = make_uint2(w23, pk);
+            if constexpr (m == 8) {
+              // the side's last 16 bytes: slot 8, then zeros
+              if (rec_any) *reinterpret_cast<uint4*>(rec_side + 8) = make_uint4(__byte_perm(wv, 0u, rsel), 0u, 0u, 0u);
             }
-          }
-          if constexpr (m == 8) {
-            // the side's last 16 bytes: slot 8, then zeros
-            if (rec_any) *reinterpret_cast<uint4*>(rec_side + 8) = make_uint4(__byte_perm(wv, 0u, rsel), 0u, 0u, 0u);
           }
         }
+      } else {
+        if (live0) pl.store_half(q, b, static_cast<uint16_t>(word & 0xffffu));
+        if (live1) pl.store_half(q, b + 1, static_cast<uint16_t>(word >> 16));
       }
-    } else {
-      if (live0) pl.store_half(q, b, Pack2<S>::from_f(gn.x));
-      if (live1) pl.store_half(q, b + 1, Pack2<S>::from_f(gn.y));
+    });
+  };
+  const float2 mag = add2rn(add2rn(f2(fabsf(u.x), fabsf(u.y)), f2(fabsf(v.x), fabsf(v.y))),
+                            add2rn(f2(fabsf(w.x), fabsf(w.y)), f2(fabsf(p.x), fabsf(p.y))));
+  // (the vortex never rounds stochastically: stochastic_rounding_for)
+  if (RULE != CaseRule::None && a.enc.sr && mag.x < SR_MOMENT_BOUND && mag.y < SR_MOMENT_BOUND) {
+    const uint32_t x = sr_hash(static_cast<uint32_t>(c0) ^ seed);
+    if constexpr (RULE != CaseRule::None) {
+      if (live0 && live1)
+        collide_store(std::true_type{}, std::true_type{}, x);
+      else
+        collide_store(std::false_type{}, std::true_type{}, x);
     }
-  });
+  } else {
+    if (live0 && live1)
+      collide_store(std::true_type{}, std::false_type{}, 0u);
+    else
+      collide_store(std::false_type{}, std::false_type{}, 0u);
+  }
 }
 
 template <Store S, Bc B, CaseRule RULE, class P>
@@ -1070,7 +1163,7 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       live0 = a.usr[c0] != 0;
       live1 = a.usr[c0 + 1] != 0;
     }
-    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store,
+    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store, a.seed,
                              lk[r][0], lk[r][1]);
   }
 }

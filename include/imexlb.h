@@ -52,8 +52,17 @@ typedef enum imexlb_case { IMEXLB_TGV = 0, IMEXLB_CAVITY = 1, IMEXLB_SPHERE = 2 
  *   bottom wall and moving lid with x and y periodic, a lid-driven slab whose
  *   steady state is plane Couette flow u(z) = u_w (z + 1/2) / nz; it checks
  *   the moving-wall rule against that exact solution.  No counterpart in the
- *   reference. */
-typedef enum imexlb_bc { IMEXLB_BC_REFERENCE = 0, IMEXLB_BC_STANDARD = 1, IMEXLB_BC_SLAB = 2 } imexlb_bc;
+ *   reference.
+ * IMEXLB_BC_REFERENCE_LINKS (cavity only, FP64 or FP32 storage): the same
+ *   results as IMEXLB_BC_REFERENCE, bit for bit, with the boundary passes
+ *   resolved per link inside the step kernel (a face-code table per face
+ *   cell) instead of a gather of the ghost slots after each step. */
+typedef enum imexlb_bc {
+  IMEXLB_BC_REFERENCE = 0,
+  IMEXLB_BC_STANDARD = 1,
+  IMEXLB_BC_SLAB = 2,
+  IMEXLB_BC_REFERENCE_LINKS = 3
+} imexlb_bc;
 
 /* Storage of the distributions in HBM.  F64 stores f_i; F32/F16/BF16 store
  * the deviation f_i - w_i * 3 p_ref scaled per population, and collide in FP32. */
@@ -243,7 +252,8 @@ int imexlb_synchronize(imexlb_lattice* h);
  * step kernels for their own row copies or for a stage to be released.  A
  * block that waits longer gives up: it lets its copies in flight land (that
  * drain keeps the full second), leaves, and the next synchronising call
- * returns IMEXLB_E_CUDA ("gave up waiting"); the lattice state is then
+ * returns IMEXLB_E_CUDA ("gave up waiting"); a bound below a microsecond
+ * gives up after one failed poll.  The lattice state is then
  * invalid until imexlb_initialize or a checkpoint load.  Lets a caller, or a
  * test, exercise that failure path without a fault.  No counterpart in the
  * reference. */

@@ -11,7 +11,8 @@
   the top fluid plane); EXACT reproduces that state too, every finite value
   bit for bit and NaN exactly where the reference has NaN (NaN payloads
   differ between processors, so both sides are compared with one NaN
-  pattern).
+  pattern).  The same two digests hold with the boundary passes resolved
+  per link inside the step kernel (bc "reference-links").
 * The 128^3 standard cavity (the default benchmark workload, FAST
   arithmetic) after 20000 steps, the configuration's step count, stays within
   1e-12 of the EXACT run of the same lattice.
@@ -83,6 +84,18 @@ def _run(api, m, arith):
 def test_exact_reproduces_reference_at_config(api, configs, name):
     m = configs[name]
     got = _run(api, m, "exact")
+    for k in "uvwp":
+        assert _sha(got[k]) == m[f"{k}_sha256"], f"{name}: field {k} differs from the reference's"
+
+
+@pytest.mark.parametrize("name", ["cavity_128_re1000_s50", "cavity_128_re1000_s200"])
+def test_per_link_boundaries_reproduce_reference_at_config(api, configs, name):
+    """The reference's boundary passes resolved per link inside the step
+    (bc "reference-links") give the same digests as the reference."""
+    m = configs[name]
+    with api.LBM(m["case"], m["nx"], m["ny"], m["nz"], m["tau"], m["rho0"], m["u0"], bc="reference-links") as lbm:
+        lbm.step(m["steps"])
+        got = lbm.fields()
     for k in "uvwp":
         assert _sha(got[k]) == m[f"{k}_sha256"], f"{name}: field {k} differs from the reference's"
 

@@ -76,6 +76,44 @@ def test_fp64_matches_oracle(api, case, rho0, R, Re, u0, nx, ny, nz, steps, arit
             assert _rel(got[k], want[k]) <= 1e-12, f"{k}: rel {_rel(got[k], want[k])}"
 
 
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+@pytest.mark.parametrize("case,rho0,R,Re,u0,nx,ny,nz,steps", [p for p in PARITY if p[0] == "cavity"])
+def test_per_link_boundaries_equal_gather(api, case, rho0, R, Re, u0, nx, ny, nz, steps, arith, storage):
+    """bc "reference-links" (the boundary passes resolved per link in the
+    step kernel) gives the same bits as bc "reference" (the ghost-slot
+    gather after each step) in FP64, EXACT and FAST, and FP64 EXACT is also
+    bit-identical to the oracle.  In FP32 storage the face cells run in
+    blocks of their own, where nvcc may contract other multiply-adds than in
+    the interior blocks (two cells a thread): within 1e-6 of max |field|."""
+    if storage == "f32" and arith == "exact":
+        pytest.skip("EXACT arithmetic is FP64-only")
+    tau = oracle_system(case, rho0, R, Re, u0, steps, 1, nx)["tau"]
+    out = {}
+    for bc in ("reference", "reference-links"):
+        with api.LBM(case, nx, ny, nz, tau, rho0, u0, bc=bc, storage=storage, arith=arith) as lbm:
+            lbm.step(steps)
+            out[bc] = lbm.fields()
+    for k in "uvwp":
+        if storage == "f64":
+            assert np.array_equal(out["reference"][k], out["reference-links"][k]), k
+        else:
+            assert _rel(out["reference-links"][k], out["reference"][k]) <= 1e-6, k
+    if storage == "f64" and arith == "exact":
+        o = Oracle(case, nx, ny, nz, tau, rho0, u0)
+        o.initialize()
+        o.step(steps)
+        for k, want in zip("uvwp", o.moments()):
+            assert np.array_equal(out["reference-links"][k], want), k
+
+
+def test_per_link_boundaries_refused_outside_their_scope(api):
+    with pytest.raises(api.ImexlbError):
+        api.LBM("cavity", 16, 16, 16, 0.02, bc="reference-links", storage="f16")
+    with pytest.raises(api.ImexlbError):
+        api.LBM("sphere", 72, 12, 12, 0.02, bc="reference-links")
+
+
 def test_split_calls_equal_one_call(api):
     """step(a); step(b) == step(a + b), and Initialize() resets."""
     tau = oracle_system("cavity", 1.0, 12.0, 100, 0.1, 1, 1, 12)["tau"]
