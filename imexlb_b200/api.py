@@ -80,7 +80,7 @@ EXPORTS = ["imexlb_params_default", "imexlb_system_read", "imexlb_create", "imex
            "imexlb_reduce_async", "imexlb_reduce_fields_noalloc", "imexlb_release_cached_memory", "imexlb_steps_taken",
            "imexlb_footprint", "imexlb_checkpoint_size", "imexlb_checkpoint_save", "imexlb_checkpoint_load",
            "imexlb_ghost_plan", "imexlb_profile", "imexlb_profile_read", "imexlb_synchronize", "imexlb_set_wait_limit",
-           "imexlb_destroy", "imexlb_last_error",
+           "imexlb_set_rounding", "imexlb_destroy", "imexlb_last_error",
            "imexlb_version", "imexlb_engine_create", "imexlb_engine_add", "imexlb_engine_add_as", "imexlb_engine_remove",
            "imexlb_engine_step", "imexlb_engine_limit", "imexlb_engine_fields", "imexlb_engine_plane",
            "imexlb_engine_residuals", "imexlb_engine_info",
@@ -237,6 +237,11 @@ class LBM:
         """Bound on the 2-byte staged kernels' waits for their row copies
         (imexlb_set_wait_limit)."""
         _check(self.lib.imexlb_set_wait_limit(self.h, seconds))
+
+    def set_rounding(self, mode: str):
+        """Rounding of the 2-byte stores: "stochastic" or "nearest"
+        (imexlb_set_rounding)."""
+        _check(self.lib.imexlb_set_rounding(self.h, {"nearest": 0, "stochastic": 1}[mode]))
 
     def fields(self, out: dict | None = None, wait: bool = True) -> dict:
         """ua, va, wa, p after the last step, each shaped (nz, ny, nx).  With

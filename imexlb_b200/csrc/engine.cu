@@ -187,7 +187,9 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
     const int bxl = sh.bx_log2;
     const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
     if constexpr (X2) {
-      step_cells_x2<S, B, RULE>(sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k);
+      // 2-byte cavity and sphere instances round stochastically (stochastic_rounding_for)
+      step_cells_x2<S, B, RULE, RULE == CaseRule::CavityStd || RULE == CaseRule::SphereStd>(
+          sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k);
     } else {
       double drag[3] = {0.0, 0.0, 0.0};
       step_cells<S, B, RULE, EXACT, false>(sh.a, pl, tile.i0 + tx, tile.j0 + ty * CPT, tile.k, drag);
@@ -314,8 +316,9 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
       const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
       const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
       const Geo g = h.geo;
-      consume_tile<S, B, RULE>(a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k,
-                               h.store != 0, h.seed, rec_stage(s), h.rec);
+      consume_tile<S, B, RULE, RULE == CaseRule::CavityStd || RULE == CaseRule::SphereStd>(
+          a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k, h.store != 0, h.seed,
+          rec_stage(s), h.rec);
     }
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);

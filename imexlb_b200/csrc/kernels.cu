@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
 
 // 2-byte formats with nx even: each thread owns an x-pair in two rows
 // (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
-template <Store S, Bc B, CaseRule RULE>
+template <Store S, Bc B, CaseRule RULE, bool SR>
 __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
   pdl_release();
   pdl_wait();
@@ -153,14 +153,14 @@ __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
   const int j0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
   const int k = blockIdx.z;
   const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
-  step_cells_x2<S, B, RULE>(a, pl, x0, j0, k);
+  step_cells_x2<S, B, RULE, SR>(a, pl, x0, j0, k);
 }
 
 // 2-byte formats, standard and periodic boundaries: rows staged in shared
 // memory by bulk copies (stage_core.cuh).  A persistent grid; block b takes
 // tiles b, b + grid, ... (y fastest, then z), so the blocks in flight cover
 // a few consecutive planes.  Warp 0 also issues the copies.
-template <Store S, Bc B, CaseRule RULE>
+template <Store S, Bc B, CaseRule RULE, bool SR>
 __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArgs a, const stage::Geo g) {
   using T = typename StoreT<S>::T;
   using namespace stage;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
       break;
     }
     const uint32_t* st = reinterpret_cast<const uint32_t*>(stages + s * stage_elems);
-    consume_tile<S, B, RULE>(a, pl, g, st, tile_origin(g, t), tile_plane(g, t), a.store != 0, a.seed, rec_stage(s),
+    consume_tile<S, B, RULE, SR>(a, pl, g, st, tile_origin(g, t), tile_plane(g, t), a.store != 0, a.seed, rec_stage(s),
                              a.rec_dst);
     __syncwarp();
     if (lane == 0) bar_arrive(&empty[s]);
@@ -564,26 +564,27 @@ static int device_sms() {
   return sms;
 }
 
-template <Store S, Bc B, CaseRule R>
+template <Store S, Bc B, CaseRule R, bool SR>
 static int staged_blocks(const stage::Geo& g, int nz) {
   static int resident = 0;  // blocks of this kernel resident on the device
   if (resident == 0) {
     const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)), R == CaseRule::CavityStd);
-    cudaFuncSetAttribute(staged_kernel<S, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaFuncSetAttribute(staged_kernel<S, B, R, SR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_kernel<S, B, R>, stage::THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_kernel<S, B, R, SR>, stage::THREADS, smem);
     resident = (per_sm > 0 ? per_sm : 1) * device_sms();
   }
   const int64_t ntiles = static_cast<int64_t>(g.nty) * nz;
   return static_cast<int>(ntiles < resident ? ntiles : resident);
 }
 
-template <Store S, Bc B, CaseRule R>
+template <Store S, Bc B, CaseRule R, bool SR>
 static cudaError_t launch_staged(const StepArgs& a, const stage::Geo& g, cudaStream_t s) {
   const size_t smem = stage::smem_bytes(static_cast<int>(sizeof(typename StoreT<S>::T)), R == CaseRule::CavityStd);
   if (R == CaseRule::CavityStd && (!a.rec_src || !a.rec_dst)) return cudaErrorInvalidValue;
-  const int blocks = staged_blocks<S, B, R>(g, a.nz);
-  return launch_pdl(staged_kernel<S, B, R>, dim3(blocks), dim3(stage::THREADS), smem, s, a, g);
+  const int blocks = staged_blocks<S, B, R, SR>(g, a.nz);
+  return launch_pdl(staged_kernel<S, B, R, SR>, dim3(blocks), dim3(stage::THREADS), smem, s, a, g);
 }
 
 // ------------------------------------------------------------ launchers
@@ -747,19 +748,35 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+// SR: the 2-byte pair kernels round their stores stochastically (Encoding::sr;
+// the cavity and the sphere only)
+template <Store S, Bc B, CaseRule R, bool EXACT, bool SR>
+static cudaError_t step_pairs(const StepArgs& a, cudaStream_t s, bool* done) {
+  *done = true;
+  if constexpr (B == Bc::Standard || B == Bc::Periodic) {
+    stage::Geo g;
+    if (staged_geo(LaunchCfg{B, S, R, EXACT}, a.nx, a.ny, a.pitch, &g)) return launch_staged<S, B, R, SR>(a, g, s);
+  }
+  // (the 2-byte formats sum their drag in drag_links_kernel)
+  if (use_x2(S, a.nx)) {
+    const dim3 block = step_block_x2(a.nx);
+    const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
+    return launch_pdl(step_kernel_x2<S, B, R, SR>, grid, block, 0, s, a);
+  }
+  *done = false;
+  return cudaSuccess;
+}
+
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
-  if constexpr ((S == Store::F16 || S == Store::BF16) && (B == Bc::Standard || B == Bc::Periodic)) {
-    stage::Geo g;
-    if (staged_geo(LaunchCfg{B, S, R, EXACT}, a.nx, a.ny, a.pitch, &g)) return launch_staged<S, B, R>(a, g, s);
-  }
   if constexpr (S == Store::F16 || S == Store::BF16) {
-    // (the 2-byte formats sum their drag in drag_links_kernel)
-    if (use_x2(S, a.nx)) {
-      const dim3 block = step_block_x2(a.nx);
-      const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
-      return launch_pdl(step_kernel_x2<S, B, R>, grid, block, 0, s, a);
-    }
+    bool done = false;
+    cudaError_t err;
+    if constexpr (R == CaseRule::CavityStd || R == CaseRule::SphereStd)
+      err = a.enc.sr ? step_pairs<S, B, R, EXACT, true>(a, s, &done) : step_pairs<S, B, R, EXACT, false>(a, s, &done);
+    else
+      err = step_pairs<S, B, R, EXACT, false>(a, s, &done);
+    if (done) return err;
   }
   const dim3 block = step_block(a.nx);
   const int rows = block.y * CellsPerThread<S>::value;

@@ -1378,6 +1378,19 @@ int imexlb_set_wait_limit(imexlb_lattice* h, double seconds) {
   return IMEXLB_OK;
 }
 
+int imexlb_set_rounding(imexlb_lattice* h, int stochastic) {
+  if (!h) return fail(IMEXLB_E_ARG, "null lattice");
+  if (stochastic != 0 && stochastic != 1) return fail(IMEXLB_E_ARG, "rounding must be 0 (nearest) or 1 (stochastic)");
+  if (stochastic) {
+    if (h->P.storage != IMEXLB_F16 && h->P.storage != IMEXLB_BF16)
+      return fail(IMEXLB_E_UNSUPPORTED, "stochastic rounding is for the FP16 and BF16 storage formats");
+    if (h->P.kase == IMEXLB_TGV) return fail(IMEXLB_E_UNSUPPORTED, "the vortex's kernels round to nearest only");
+  }
+  h->enc.sr = static_cast<uint32_t>(stochastic);
+  h->base_args.enc.sr = h->enc.sr;
+  return IMEXLB_OK;
+}
+
 int imexlb_release_cached_memory(void) {
   int dev = 0;
   IMX_CUDA(cudaGetDevice(&dev));

@@ -400,7 +400,7 @@ __device__ __forceinline__ void issue_skip(uint64_t* bar) {
 // row or plane around it.  Cavity: `rec` is the stage's wall records (tile
 // row r at r * WallRecord::WORDS), `rec_row` the pair's row in the record
 // buffer this step writes.
-template <Store S, Bc B, CaseRule RULE, bool EDGE, bool FLAT = false, class P>
+template <Store S, Bc B, CaseRule RULE, bool EDGE, bool FLAT = false, bool SR = false, class P>
 __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                                 const int x, const int r, const int j0, const int k,
                                                 const bool store, const uint32_t seed, const uint16_t* rec = nullptr,
@@ -516,8 +516,8 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
   }
   // the lid plane is a wall plane: only EDGE pairs can sit under it
   const bool lid = RULE == CaseRule::CavityStd && EDGE && k == a.nz - 1;
-  finish_pair_row<S, RULE, RULE == CaseRule::CavityStd>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store,
-                                                        seed, links0, links1, rec_row);
+  finish_pair_row<S, RULE, RULE == CaseRule::CavityStd, SR>(a, pl, raw, x, j, k, lid, left_edge, live0, live1, store,
+                                                            seed, links0, links1, rec_row);
 }
 
 // The cells of tile (j0, k) from stage `st`, shared by the block's threads:
@@ -529,7 +529,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
 // bounce-back; a warp holds pairs of one or two rows, so the choice is
 // nearly uniform across it).  Cavity: `rec` is the stage's wall records,
 // `rec_out` the record buffer this step writes.
-template <Store S, Bc B, CaseRule RULE, class P>
+template <Store S, Bc B, CaseRule RULE, bool SR = false, class P>
 __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, const Geo& g, const uint32_t* st,
                                              const int j0, const int k, const bool store, const uint32_t seed,
                                              const uint16_t* rec = nullptr, uint16_t* rec_out = nullptr) {
@@ -545,9 +545,9 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
       const int j = j0 + r;
       uint16_t* const rec_row = rec_tile + r * WallRecord::WORDS;
       if (wall_plane || j == 0 || j == a.ny - 1)
-        pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
+        pair_from_stage<S, B, RULE, true, false, SR>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
       else
-        pair_from_stage<S, B, RULE, false>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
+        pair_from_stage<S, B, RULE, false, false, SR>(a, pl, g, st, x, r, j0, k, store, seed, rec, rec_row);
     }
   } else if constexpr (RULE == CaseRule::SphereStd) {
     if (g.flat) {
@@ -560,19 +560,19 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
         const int e = e0 + 2 * p;
         const int j = e / g.P, x = e - j * g.P;
         if (x < a.nx)
-          pair_from_stage<S, B, RULE, true, true>(a, pl, g, st, x, 0, 0, k, store, seed, nullptr, nullptr, j,
+          pair_from_stage<S, B, RULE, true, true, SR>(a, pl, g, st, x, 0, 0, k, store, seed, nullptr, nullptr, j,
                                                   p + FLAT_GUARD / 2);
       }
     } else {
       for (int p = threadIdx.x; p < npairs; p += THREADS) {
         const int r = p / half, x = 2 * (p - r * half);
-        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed);
+        if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true, false, SR>(a, pl, g, st, x, r, j0, k, store, seed);
       }
     }
   } else {
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
       const int r = p / half, x = 2 * (p - r * half);
-      if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true>(a, pl, g, st, x, r, j0, k, store, seed);
+      if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true, false, SR>(a, pl, g, st, x, r, j0, k, store, seed);
     }
   }
 }

@@ -223,35 +223,40 @@ __device__ __forceinline__ typename StoreT<S>::T encode(typename StoreT<S>::R x,
 }
 
 // ------------------------------------------------------------ stochastic rounding
-// With Encoding::sr the 2-byte stores round stochastically: a pseudo-random
-// fraction of one unit in the last place of the stored format is added to
-// the FP32 value's bits and the sum is rounded toward zero, so the value
-// rounds up with probability equal to its distance from the one below and
-// the rounding error is zero on average (stochastic rounding, Forsythe
-// 1959; Connolly, Higham and Mary, SIAM J. Sci. Comput. 43, 2021).  In a
-// steady flow round-to-nearest makes the same error at the same cell every
-// step, a constant forcing whose effect on the velocity grows with the step
-// count; zero-mean errors do not accumulate that way.  The random bits are
-// a function of (cell, population, step) only: a lattice gives the same
-// bits alone, in the engine and resumed from a checkpoint.  Per cell (or
-// x-pair) one 32-bit integer hash of the cell index and the step's seed
-// (StepArgs::seed, itself the hash of the step count) gives x; population q
-// takes the bits of x * sr_mul(q) (sr_hash: lattice.h).
-// odd multipliers, one per population
+// With stochastic rounding (Encoding::sr; the cavity's and the sphere's
+// 2-byte formats) the stores convert with sm_100a's `cvt.rs` (PTX ISA 8.7:
+// FP32 to f16x2 / bf16x2 rounded stochastically with caller-given random
+// bits), so a value rounds up with probability equal to its distance from
+// the one below and the rounding error is zero on average (stochastic
+// rounding: Forsythe 1959; Connolly, Higham and Mary, SIAM J. Sci. Comput.
+// 43, 2021).  In a steady flow round-to-nearest makes the same error at the
+// same cell every step, a constant forcing whose effect on the velocity
+// grows with the step count; zero-mean errors do not accumulate that way.
+// The random bits are a function of (cell, population, step) only, so a
+// lattice gives the same bits alone, in the engine and resumed from a
+// checkpoint: per cell (or x-pair) x = sr_hash(cell index ^ seed), with
+// StepArgs::seed the hash of the lattice's step count (sr_hash: lattice.h),
+// and population q takes the 32 bits of x * sr_mul(q).
 constexpr uint32_t sr_mul(int q) { return 0x9e3779b9u * (2u * static_cast<uint32_t>(q) + 1u) | 1u; }
-// Moments this small keep every stored value finite and in range, so the
-// bit additions cannot reach the exponent's top (NaN, infinity, or FP16
-// overflow, which round-to-nearest reports as infinity and rounding toward
-// zero would not); a cell outside the bound is stored with round-to-nearest.
-constexpr float SR_MOMENT_BOUND = 4.f;
-// one FP32 value to a 2-byte format, rounded stochastically with `r`
+// An x-pair of FP32 values (lo = cell x0) to the 2-byte format's packed
+// pair, rounded stochastically with the 32 random bits `rbits`.
 template <Store S>
-__device__ __forceinline__ typename StoreT<S>::T sr_one(float x, uint32_t r) {
-  if constexpr (S == Store::F16) {
-    return __float2half_rz(__uint_as_float(__float_as_uint(x) + (r >> 19)));
-  } else {
-    return __ushort_as_bfloat16(static_cast<unsigned short>((__float_as_uint(x) + (r >> 16)) >> 16));
-  }
+__device__ __forceinline__ uint32_t sr_pair(float2 g, uint32_t rbits) {
+  uint32_t word;
+  if constexpr (S == Store::F16)
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(word) : "f"(g.y), "f"(g.x), "r"(rbits));
+  else
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(word) : "f"(g.y), "f"(g.x), "r"(rbits));
+  return word;
+}
+// One FP32 value, the same way (the low half of a pair whose high half is 0).
+template <Store S>
+__device__ __forceinline__ typename StoreT<S>::T sr_one(float x, uint32_t rbits) {
+  const unsigned short h = static_cast<unsigned short>(sr_pair<S>(make_float2(x, 0.f), rbits) & 0xffffu);
+  if constexpr (S == Store::F16)
+    return __ushort_as_half(h);
+  else
+    return __ushort_as_bfloat16(h);
 }
 
 template <class T>
@@ -545,7 +550,7 @@ __device__ __forceinline__ void compute_cell(const StepArgs& a, const P& pl, con
     [[maybe_unused]] bool sr = false;
     [[maybe_unused]] uint32_t x = 0;
     if constexpr ((S == Store::F16 || S == Store::BF16) && RULE != CaseRule::None) {
-      sr = a.enc.sr && fabsf(u) + fabsf(v) + fabsf(w) + fabsf(p) < SR_MOMENT_BOUND;
+      sr = a.enc.sr != 0;
       x = sr_hash(static_cast<uint32_t>(cell) ^ a.seed);
     }
     static_for<0, Q>([&](auto qc) {
@@ -813,24 +818,6 @@ template <> struct Pack2<Store::BF16> {
   static __device__ __forceinline__ uint16_t from_f(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 };
 
-// An x-pair rounded stochastically (see sr_hash): `r` holds the random bits
-// of both cells.  FP16: cell x0 takes bits 19-31, x0 + 1 bits 6-18 (13 bits
-// below the FP16 significand each); BF16: bits 16-31 and 0-15.
-template <Store S>
-__device__ __forceinline__ uint32_t sr_pair(float2 g, uint32_t r) {
-  if constexpr (S == Store::F16) {
-    const float lo = __uint_as_float(__float_as_uint(g.x) + (r >> 19));
-    const float hi = __uint_as_float(__float_as_uint(g.y) + ((r >> 6) & 0x1fffu));
-    uint32_t word;
-    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(word) : "f"(hi), "f"(lo));
-    return word;
-  } else {
-    const uint32_t lo = __float_as_uint(g.x) + (r >> 16);
-    const uint32_t hi = __float_as_uint(g.y) + (r & 0xffffu);
-    return __byte_perm(lo, hi, 0x7632);
-  }
-}
-
 // pair (lo = cell x0, hi = cell x0 + 1) from two 16-bit halves
 __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { return (lo16 & 0xffffu) | (hi16 << 16); }
 
@@ -855,7 +842,7 @@ __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { retu
 // values the halfway bounce-back returns to it next step, 32 bytes per wall
 // side in three aligned stores, so that the next step's tile finds them in
 // one bulk copy instead of nine scattered rows.
-template <Store S, CaseRule RULE, bool REC = false, class P>
+template <Store S, CaseRule RULE, bool REC = false, bool SR = false, class P>
 __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
                                                 const bool live0, const bool live1, const bool store,
@@ -956,11 +943,10 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   // pair but those beside a solid or past the lattice's end) takes a copy of
   // the loop without the per-population choice between a paired and two
   // half stores.
-  // With stochastic rounding (Encoding::sr, for cells whose moments are
-  // within SR_MOMENT_BOUND) the pair's random bits come from x.
-  auto collide_store = [&](auto both_c, auto sr_c, const uint32_t x) __attribute__((always_inline)) {
+  // SR: stochastic rounding, the pair's random bits from x
+  [[maybe_unused]] const uint32_t x = SR ? sr_hash(static_cast<uint32_t>(c0) ^ seed) : 0u;
+  auto collide_store = [&](auto both_c) __attribute__((always_inline)) {
     constexpr bool BOTH = decltype(both_c)::value;
-    constexpr bool SR = decltype(sr_c)::value;
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       float2 Kq = K;
@@ -1023,26 +1009,13 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
       }
     });
   };
-  const float2 mag = add2rn(add2rn(f2(fabsf(u.x), fabsf(u.y)), f2(fabsf(v.x), fabsf(v.y))),
-                            add2rn(f2(fabsf(w.x), fabsf(w.y)), f2(fabsf(p.x), fabsf(p.y))));
-  // (the vortex never rounds stochastically: stochastic_rounding_for)
-  if (RULE != CaseRule::None && a.enc.sr && mag.x < SR_MOMENT_BOUND && mag.y < SR_MOMENT_BOUND) {
-    const uint32_t x = sr_hash(static_cast<uint32_t>(c0) ^ seed);
-    if constexpr (RULE != CaseRule::None) {
-      if (live0 && live1)
-        collide_store(std::true_type{}, std::true_type{}, x);
-      else
-        collide_store(std::false_type{}, std::true_type{}, x);
-    }
-  } else {
-    if (live0 && live1)
-      collide_store(std::true_type{}, std::false_type{}, 0u);
-    else
-      collide_store(std::false_type{}, std::false_type{}, 0u);
-  }
+  if (live0 && live1)
+    collide_store(std::true_type{});
+  else
+    collide_store(std::false_type{});
 }
 
-template <Store S, Bc B, CaseRule RULE, class P>
+template <Store S, Bc B, CaseRule RULE, bool SR = false, class P>
 __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, const int x0, const int j0, const int k) {
   constexpr int RY = 2;
   const bool xin = x0 < a.nx;  // nx even: both cells of the pair or neither
@@ -1163,8 +1136,8 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       live0 = a.usr[c0] != 0;
       live1 = a.usr[c0 + 1] != 0;
     }
-    finish_pair_row<S, RULE>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1, a.store, a.seed,
-                             lk[r][0], lk[r][1]);
+    finish_pair_row<S, RULE, false, SR>(a, pl, raw[r], x0, j0 + r, k, (lid_mask >> r) & 1u, left_edge, live0, live1,
+                                        a.store, a.seed, lk[r][0], lk[r][1]);
   }
 }
 

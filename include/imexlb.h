@@ -259,6 +259,15 @@ int imexlb_synchronize(imexlb_lattice* h);
  * reference. */
 int imexlb_set_wait_limit(imexlb_lattice* h, double seconds);
 
+/* Rounding of the FP16 / BF16 stores: 1 = stochastic (the default for the
+ * cavity and the sphere channel: a pseudo-random fraction of a unit in the
+ * last place, from a hash of cell, population and step count, is added
+ * before rounding toward zero, so the rounding error is zero on average and
+ * does not accumulate in a steady flow), 0 = to nearest (the vortex's only
+ * mode).  IMEXLB_E_UNSUPPORTED for stochastic rounding of another storage
+ * format or of the vortex.  No counterpart in the reference. */
+int imexlb_set_rounding(imexlb_lattice* h, int stochastic);
+
 void imexlb_destroy(imexlb_lattice* h);
 
 /* Lattices take their device memory from a stream-ordered pool per device

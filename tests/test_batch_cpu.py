@@ -60,5 +60,9 @@ def test_fp16_storage_plan():
     assert batch.engine_storage("f16-all") == "f16"
     reqs = serve.request_stream(200, 10.0)
     for r in reqs:
-        assert serve.storage_for(r, "f16") == ("f16" if r.tau0 >= batch.FP16_MIN_TAU0 else "f32")
+        if r.case == "tgv":
+            want = "f32" if r.tau0 >= serve.TGV_FP32_MIN_TAU0 else "f64"
+        else:
+            want = "f16" if r.tau0 >= batch.FP16_MIN_TAU0 else "f32"
+        assert serve.storage_for(r, "f16") == want
         assert serve.storage_for(r, "f64") == "f64"

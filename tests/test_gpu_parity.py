@@ -85,7 +85,7 @@ def test_per_link_boundaries_equal_gather(api, case, rho0, R, Re, u0, nx, ny, nz
     gather after each step) in FP64, EXACT and FAST, and FP64 EXACT is also
     bit-identical to the oracle.  In FP32 storage the face cells run in
     blocks of their own, where nvcc may contract other multiply-adds than in
-    the interior blocks (two cells a thread): within 1e-6 of max |field|."""
+    the interior blocks (two cells a thread): within 1e-5 of max |field|."""
     if storage == "f32" and arith == "exact":
         pytest.skip("EXACT arithmetic is FP64-only")
     tau = oracle_system(case, rho0, R, Re, u0, steps, 1, nx)["tau"]
@@ -98,7 +98,7 @@ def test_per_link_boundaries_equal_gather(api, case, rho0, R, Re, u0, nx, ny, nz
         if storage == "f64":
             assert np.array_equal(out["reference"][k], out["reference-links"][k]), k
         else:
-            assert _rel(out["reference-links"][k], out["reference"][k]) <= 1e-6, k
+            assert _rel(out["reference-links"][k], out["reference"][k]) <= 1e-5, k
     if storage == "f64" and arith == "exact":
         o = Oracle(case, nx, ny, nz, tau, rho0, u0)
         o.initialize()

@@ -74,14 +74,19 @@ def test_cavity_lid_drives_flow(api):
     assert f["u"][: 16].mean() < 0.0  # the return flow in the lower half
 
 
-# (case, storage, n, steps, bound on the relative velocity L2 error vs FP64)
+# (case, storage, n, steps, bound on the relative velocity L2 error vs FP64).
+# The cavity's 2-byte stores round stochastically: zero-mean errors whose
+# spread is about 1.4 times round-to-nearest's, so within the first few
+# hundred steps the error is somewhat larger than with round-to-nearest, and
+# it stays at that level instead of growing with the step count; the cavity
+# is checked at 2000 steps (the batched configuration's count).
 PRECISION = [
     ("tgv", "f32", (32, 32, 32), 200, 1e-5),
     ("tgv", "f16", (32, 32, 32), 200, 1e-3),
     ("tgv", "bf16", (32, 32, 32), 200, 3e-2),
     ("cavity", "f32", (32, 32, 32), 300, 1e-5),
-    ("cavity", "f16", (32, 32, 32), 300, 1e-3),
-    ("cavity", "bf16", (32, 32, 32), 300, 3e-2),
+    ("cavity", "f16", (32, 32, 32), 2000, 1e-3),
+    ("cavity", "bf16", (32, 32, 32), 2000, 1e-2),
 ]
 
 
@@ -143,3 +148,54 @@ def test_staged_wait_limit_gives_up_and_the_lattice_recovers(api):
         want = fresh.fields()
     for k in "uvwp":
         assert np.array_equal(got[k], want[k]), k
+
+
+def _cavity_u(api, n, tau0, steps, storage, rounding=None):
+    with api.LBM("cavity", n, n, n, tau0, 1.0, 0.05, bc="standard", storage=storage, arith="fast",
+                 lid_u=0.05) as lbm:
+        if rounding:
+            lbm.set_rounding(rounding)
+        out = []
+        done = 0
+        for s in steps:
+            lbm.step(s - done)
+            done = s
+            out.append(lbm.fields())
+    return out
+
+
+def test_stochastic_rounding_keeps_the_fp16_cavity_error_flat(api):
+    """The 2-byte cavity rounds its stores stochastically by default: its
+    velocity error against FP64 stays within 1e-3 from 2000 to 10000 steps,
+    where round-to-nearest's grows past it (64^3, Re 117, tau - 1/2 = 0.082;
+    measured 2.4e-4 and 2.5e-4 against 2.2e-4 and 4.4e-3)."""
+    n, tau0, steps = 64, 0.0819, (2000, 10000)
+    want = _cavity_u(api, n, tau0, steps, "f64")
+    sr = _cavity_u(api, n, tau0, steps, "f16")
+    rn = _cavity_u(api, n, tau0, steps, "f16", "nearest")
+    e_sr = [rel_l2(g, w) for g, w in zip(sr, want)]
+    e_rn = [rel_l2(g, w) for g, w in zip(rn, want)]
+    assert max(e_sr) <= 1e-3, e_sr
+    assert e_sr[1] <= 1.5 * e_sr[0], e_sr          # no growth with the step count
+    assert e_rn[1] > 2.0 * e_sr[1], (e_rn, e_sr)   # round-to-nearest accumulates
+
+
+def test_rounding_mode_scope(api):
+    with api.LBM("cavity", 16, 16, 16, 0.05, bc="standard", storage="f64", arith="fast") as lbm:
+        with pytest.raises(api.ImexlbError):
+            lbm.set_rounding("stochastic")
+        lbm.set_rounding("nearest")
+    with api.LBM("tgv", 16, 16, 16, 0.05, bc="standard", storage="f16", arith="fast") as lbm:
+        with pytest.raises(api.ImexlbError):
+            lbm.set_rounding("stochastic")
+
+
+def test_diverging_fp16_cavity_goes_non_finite(api):
+    """Stochastic rounding keeps infinities and NaNs: a cavity far beyond
+    BGK's stability limit (tau - 1/2 = 1e-4) turns non-finite in FP16 as in
+    FP64, so the serving loop can retire it as diverged."""
+    with api.LBM("cavity", 32, 32, 32, 1e-4, 1.0, 0.1, bc="standard", storage="f16", arith="fast",
+                 lid_u=0.1) as lbm:
+        lbm.step(4000)
+        f = lbm.fields()
+    assert not all(np.isfinite(f[k]).all() for k in "uvwp")
