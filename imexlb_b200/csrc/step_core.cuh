@@ -930,19 +930,21 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   }
   // omega unit (3 p~ - 1.5 u.u)
   const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), mudu15));
-  // wall record: the pair holds the x = 0 cell (lo) or the x = nx - 1 cell
-  // (hi; nx >= 4, so not both).  Each 16-bit value sits in the pair's packed
-  // store word of its population (low half: cell x0, high half: x0 + 1);
-  // rsel picks those halves of two words into one record word.
-  [[maybe_unused]] const bool rec_lo = REC && x0 == 0, rec_hi = REC && x0 + 2 >= a.nx;
-  [[maybe_unused]] const bool rec_any = rec_lo || rec_hi;
-  [[maybe_unused]] const uint32_t rsel = rec_lo ? 0x5410u : 0x7632u;
-  [[maybe_unused]] uint16_t* const rec_side = rec_row + (rec_hi ? WallRecord::HI : 0);
-  [[maybe_unused]] uint32_t held = 0, pend = 0, w01 = 0, w23 = 0;
   // Collision and stores; a pair whose two cells are both updated (every
   // pair but those beside a solid or past the lattice's end) takes a copy of
   // the loop without the per-population choice between a paired and two
   // half stores.
+  // Wall record (REC): the pair holds the x = 0 cell (lo) or the x = nx - 1
+  // cell (hi; nx >= 4, so not both).  Slot m of a side holds the 16-bit
+  // value of pair m's population that leaves the box through that wall:
+  // e_x = -1 (q = P_m + 1, low half of its word) at x = 0, e_x = +1 (q = P_m,
+  // high half) at x = nx - 1; each is stored as the loop produces it, after
+  // the side's zero padding (slots 9-15).
+  [[maybe_unused]] const bool rec_lo = REC && x0 == 0, rec_hi = REC && x0 + 2 >= a.nx;
+  if constexpr (REC) {
+    if (rec_lo || rec_hi)
+      *reinterpret_cast<uint4*>(rec_row + (rec_hi ? WallRecord::HI : 0) + 8) = make_uint4(0u, 0u, 0u, 0u);
+  }
   // SR: stochastic rounding, the pair's random bits from x
   [[maybe_unused]] const uint32_t x = SR ? sr_hash(static_cast<uint32_t>(c0) ^ seed) : 0u;
   auto collide_store = [&](auto both_c) __attribute__((always_inline)) {
@@ -954,9 +956,10 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
         // minus the reference flow's equilibrium, omega unit br_ref[q]
         Kq = add2rn(K, f2s(a.enc.kref[q]));
       }
+      const float2 gq = g[q];
       float2 gn;
       if constexpr (q == 0) {
-        gn = fma2rn(g[q], keep, Kq);
+        gn = fma2rn(gq, keep, Kq);
       } else {
         // with e negated, so are the factors 4.5 and omega unit: same values.
         // The sphere's kernels keep the signed e, whose negations cost no
@@ -965,7 +968,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
         const float2 e = RULE != CaseRule::SphereStd ? edu2f<q>(u, v, w) : edu2<q>(u, v, w);
         const float2 t = fma2rn(e, f2s(en ? -4.5f : 4.5f), f2s(3.0f));
         const float2 h = mul2rn(e, f2s(en ? -om_u : om_u));
-        gn = fma2rn(h, t, fma2rn(g[q], keep, Kq));
+        gn = fma2rn(h, t, fma2rn(gq, keep, Kq));
       }
       uint32_t word;
       if constexpr (SR)
@@ -975,32 +978,11 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
       if constexpr (BOTH) {
         pl.store_pair(q, b, word);
         if constexpr (REC) {
-          // slot m of a side holds the population of pair m that leaves the
-          // box through that wall: e_x = -1 (q = P_m + 1) at x = 0, e_x = +1
-          // (q = P_m) at x = nx - 1
           constexpr int ex = D3Q27::ex[q];
-          if constexpr (ex > 0) {
-            held = word;
-          } else if constexpr (ex < 0) {
-            constexpr int m = WallRecord::slot(q);
-            const uint32_t wv = rec_lo ? word : held;
-            if constexpr (m % 2 == 0) {
-              pend = wv;
-            } else {
-              const uint32_t pk = __byte_perm(pend, wv, rsel);
-              if constexpr (m == 1) w01 = pk;
-              if constexpr (m == 3) {
-                if (rec_any) *reinterpret_cast<uint2*>(rec_side) = make_uint2(w01, pk);
-              }
-              if constexpr (m == 5) w23 = pk;
-              if constexpr (m == 7) {
-                if (rec_any) *reinterpret_cast<uint2*>(rec_side + 4) = make_uint2(w23, pk);
-              }
-            }
-            if constexpr (m == 8) {
-              // the side's last 16 bytes: slot 8, then zeros
-              if (rec_any) *reinterpret_cast<uint4*>(rec_side + 8) = make_uint4(__byte_perm(wv, 0u, rsel), 0u, 0u, 0u);
-            }
+          if constexpr (ex < 0) {
+            if (rec_lo) rec_row[WallRecord::slot(q)] = static_cast<uint16_t>(word & 0xffffu);
+          } else if constexpr (ex > 0) {
+            if (rec_hi) rec_row[WallRecord::HI + WallRecord::slot(q)] = static_cast<uint16_t>(word >> 16);
           }
         }
       } else {
