@@ -372,6 +372,39 @@ __global__ void ghost_gather_kernel(typename StoreT<S>::T* __restrict__ dst, con
   }
 }
 
+// The same gather over a packed plan: entry e is (target, source) as two
+// 32-bit indices (int2), one 8-byte load instead of two.
+template <Store S>
+__global__ void ghost_gather_packed_kernel(typename StoreT<S>::T* __restrict__ dst,
+                                           const typename StoreT<S>::T* __restrict__ prev,
+                                           const int2* __restrict__ plan, int64_t n, int64_t sq, Encoding enc) {
+  using T = typename StoreT<S>::T;
+  constexpr int V = 4;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * V;
+  for (int64_t e0 = static_cast<int64_t>(blockIdx.x) * blockDim.x * V + threadIdx.x; e0 < n; e0 += stride) {
+    int2 p[V];
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      const int64_t e = e0 + static_cast<int64_t>(u) * blockDim.x;
+      p[u] = e < n ? __ldg(plan + e) : make_int2(-1, -1);
+    }
+    T val[V];
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      if (p[u].y >= 0) {
+        val[u] = dst[p[u].y];
+      } else if (p[u].y <= -2) {
+        val[u] = prev[-static_cast<int64_t>(p[u].y) - 2];
+      } else {
+        val[u] = encode<S>(typename StoreT<S>::R(0), p[u].x >= 0 ? static_cast<int>(p[u].x / sq) : 0, enc);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < V; ++u)
+      if (p[u].x >= 0) dst[p[u].x] = val[u];
+  }
+}
+
 // ------------------------------------------------------------ reductions
 constexpr int RED_THREADS = 256;
 constexpr int RED_BLOCKS = 592;  // 4 per SM on 148 SMs
@@ -825,6 +858,28 @@ cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s) {
     case Store::BF16: return step_rule<Store::BF16, false>(c, a, s);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ghost_gather_packed(Store st, void* dst, const void* prev, const int2* plan, int64_t n, int64_t sq,
+                                       const Encoding& enc, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int threads = 256;
+  const int64_t want = (n + threads * 4 - 1) / (threads * 4);
+  const int blocks = static_cast<int>(want < 148 * 8 ? want : 148 * 8);
+  switch (st) {
+#define IMX_GGP(S)                                                                                               \
+  case S:                                                                                                        \
+    ghost_gather_packed_kernel<S><<<blocks, threads, 0, s>>>(static_cast<typename StoreT<S>::T*>(dst),           \
+                                                            static_cast<const typename StoreT<S>::T*>(prev), plan, \
+                                                            n, sq, enc);                                           \
+    break;
+    IMX_GGP(Store::F64)
+    IMX_GGP(Store::F32)
+    IMX_GGP(Store::F16)
+    IMX_GGP(Store::BF16)
+#undef IMX_GGP
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,

@@ -270,7 +270,8 @@ struct imexlb_lattice {
   DevArray<uint8_t> usr;      // interior mask (sphere)
   DevArray<uint32_t> links;   // standard sphere: per-cell solid-link bits
   DevArray<double> inlet;     // reference sphere inlet profile per z
-  DevArray<int64_t> gtgt, gsrc;
+  DevArray<int64_t> gtgt, gsrc;  // ghost-slot plan, 64-bit indices (very large buffers)
+  DevArray<int2> gpk;            // the plan as packed 32-bit (target, source) pairs
   DevArray<int32_t> face_codes;  // reference cavity: the passes resolved per face-cell link
   int64_t gn = 0;
   DevArray<double> red;       // reduction partials + result
@@ -432,6 +433,14 @@ bool device_initial_state(const imexlb_params& P) {
   return P.kase == IMEXLB_CAVITY || (P.kase == IMEXLB_SPHERE && P.bc == IMEXLB_BC_STANDARD);
 }
 
+// The reference boundaries' ghost-slot gather into `dst`, previous-step
+// values from `prev`, over whichever form of the plan the lattice holds.
+cudaError_t ghost_gather(imexlb_lattice* h, void* dst, const void* prev) {
+  if (h->gpk.p)
+    return launch_ghost_gather_packed(h->cfg.store, dst, prev, h->gpk.p, h->gn, h->L.sq, h->enc, h->stream);
+  return launch_ghost_gather(h->cfg.store, dst, prev, h->gtgt.p, h->gsrc.p, h->gn, h->L.sq, h->enc, h->stream);
+}
+
 int upload_device_case(imexlb_lattice* h) {
   const Layout& L = h->L;
   if (h->P.kase == IMEXLB_CAVITY) {
@@ -450,9 +459,7 @@ int upload_device_case(imexlb_lattice* h) {
   }
   for (int b = 0; b < 2 && h->rec[b].p; ++b) IMX_CUDA(launch_cavity_records(L, h->buf[b].p, h->rec[b].p, h->stream));
   // reference boundaries: the first step's passes act on the initial state
-  if (h->gn)
-    IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[0].p, h->buf[1].p, h->gtgt.p, h->gsrc.p, h->gn, L.sq, h->enc,
-                                 h->stream));
+  if (h->gn) IMX_CUDA(ghost_gather(h, h->buf[0].p, h->buf[1].p));
   IMX_CUDA(cudaStreamSynchronize(h->stream));
   h->cur = 0;
   h->steps = 0;
@@ -500,9 +507,7 @@ int upload_case(imexlb_lattice* h) {
     IMX_CUDA(cudaStreamSynchronize(h->stream));  // before the host vector goes
   }
   // reference boundaries: the first step's passes act on the initial state
-  if (h->gn)
-    IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[0].p, h->buf[1].p, h->gtgt.p, h->gsrc.p, h->gn, L.sq, h->enc,
-                                 h->stream));
+  if (h->gn) IMX_CUDA(ghost_gather(h, h->buf[0].p, h->buf[1].p));
   IMX_CUDA(cudaStreamSynchronize(h->stream));
   h->cur = 0;
   h->steps = 0;
@@ -908,10 +913,20 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
       }
     } else {
       h->gn = static_cast<int64_t>(g->t.size());
-      IMX_CUDA(h->gtgt.alloc(g->t.size(), h->stream));
-      IMX_CUDA(h->gsrc.alloc(g->s.size(), h->stream));
-      IMX_CUDA(cudaMemcpy(h->gtgt.p, g->t.data(), g->t.size() * 8, cudaMemcpyHostToDevice));
-      IMX_CUDA(cudaMemcpy(h->gsrc.p, g->s.data(), g->s.size() * 8, cudaMemcpyHostToDevice));
+      const int64_t elems = static_cast<int64_t>(L.sq) * Q;
+      if (elems < 2147483646ll) {
+        // every index and source code fits 32 bits: one packed pair an entry
+        std::vector<int2> pk(g->t.size());
+        for (size_t n = 0; n < pk.size(); ++n)
+          pk[n] = make_int2(static_cast<int32_t>(g->t[n]), static_cast<int32_t>(g->s[n]));
+        IMX_CUDA(h->gpk.alloc(pk.size(), h->stream));
+        IMX_CUDA(cudaMemcpy(h->gpk.p, pk.data(), pk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      } else {
+        IMX_CUDA(h->gtgt.alloc(g->t.size(), h->stream));
+        IMX_CUDA(h->gsrc.alloc(g->s.size(), h->stream));
+        IMX_CUDA(cudaMemcpy(h->gtgt.p, g->t.data(), g->t.size() * 8, cudaMemcpyHostToDevice));
+        IMX_CUDA(cudaMemcpy(h->gsrc.p, g->s.data(), g->s.size() * 8, cudaMemcpyHostToDevice));
+      }
     }
   }
 
@@ -972,8 +987,7 @@ int imexlb_step(imexlb_lattice* h, int nsteps) {
         t1.a = t0.b;
         t1.b = h->take_event();
       }
-      IMX_CUDA(launch_ghost_gather(h->cfg.store, h->buf[1 - h->cur].p, h->buf[h->cur].p, h->gtgt.p, h->gsrc.p, h->gn,
-                                   h->L.sq, h->enc, h->stream));
+      IMX_CUDA(ghost_gather(h, h->buf[1 - h->cur].p, h->buf[h->cur].p));
       if (h->profiling) {
         IMX_CUDA(cudaEventRecord(t1.b, h->stream));
         h->timed.push_back(t1);
@@ -1228,7 +1242,7 @@ int imexlb_footprint(const imexlb_lattice* h, size_t* device_bytes, double* byte
   if (!h) return fail(IMEXLB_E_ARG, "null lattice");
   if (device_bytes)
     *device_bytes = h->buf[0].n + h->buf[1].n + h->mom.n * 8 + h->prev_mom.n * 8 + h->usr.n + h->inlet.n * 8 +
-                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->face_codes.n * 4 + h->red.n * 8 + h->drag_part.n * 8 +
+                    h->gtgt.n * 8 + h->gsrc.n * 8 + h->gpk.n * 8 + h->face_codes.n * 4 + h->red.n * 8 + h->drag_part.n * 8 +
                     h->links.n * 4 +
                     (h->rec[0].n + h->rec[1].n) * sizeof(uint16_t);
   if (bytes_per_cell_update) *bytes_per_cell_update = 2.0 * Q * h->L.elem;

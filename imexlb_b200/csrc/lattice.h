@@ -256,6 +256,10 @@ cudaError_t launch_step(const LaunchCfg& c, const StepArgs& a, cudaStream_t s);
 cudaError_t launch_sphere_fields(const uint8_t* fluid, int64_t n, double ui, double* out, cudaStream_t s);
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
                                 int64_t n, int64_t sq, const Encoding& enc, cudaStream_t s);
+// The same with the plan packed as (target, source) 32-bit pairs, for
+// buffers of fewer than 2^31 - 2 elements.
+cudaError_t launch_ghost_gather_packed(Store st, void* dst, const void* prev, const int2* plan, int64_t n, int64_t sq,
+                                       const Encoding& enc, cudaStream_t s);
 dim3 step_block(int nx);
 // Blocks that write one drag partial each: the step launch of this
 // configuration, or the drag kernel's blocks for the 2-byte formats.
