@@ -1040,6 +1040,7 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
       // the reference's equilibrium bracket (tgv/src/lbm.cpp:228-232) of (ui, 0, 0): edu = e_x ui, udu = ui ui
       const double br = 3.0 * ev + 4.5 * (ev * ev) - 1.5 * (ui * ui);
       a.feq_in[q] = t * (3.0 * (0.0 - a.p_shift) + (ref_flow ? 0.0 : br));
+      a.enc.inlet_g[q] = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
     }
   }
   in.buf[0] = buf0;

@@ -888,6 +888,7 @@ int imexlb_create(const imexlb_params* pin, imexlb_lattice** out) {
         // the reference's equilibrium bracket (tgv/src/lbm.cpp:228-232) of (ui, 0, 0): edu = e_x ui, udu = ui ui
         const double br = 3.0 * e + 4.5 * (e * e) - 1.5 * (ui * ui);
         a.feq_in[q] = t * (3.0 * (0.0 - h->p_shift) + (ref_flow ? 0.0 : br));
+        a.enc.inlet_g[q] = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
       }
     }
   }

@@ -72,6 +72,9 @@ struct Encoding {
   float br_ref[Q] = {};
   float kref[Q] = {};  // -omega unit br_ref[q], the collision's share of it
   uint32_t sr = 0;     // 2-byte formats: 1 = stochastic rounding of the stores
+  // standard sphere, 2-byte pair kernels: StepArgs::feq_in[q] in stored
+  // units, float(feq_in[q] * scale[q]) (the inlet column's values)
+  float inlet_g[Q] = {};
 };
 // Whether a lattice's 2-byte stores round stochastically (Encoding::sr):
 // yes for the cavity and the sphere channel, driven flows that settle into

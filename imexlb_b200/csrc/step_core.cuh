@@ -866,7 +866,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
       if (lid) x = add2rn(x, f2s(ex > 0 ? lid_g : -lid_g));
     }
     if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
-      if (left_edge) x.x = static_cast<float>(a.feq_in[q] * static_cast<double>(a.enc.scale[q]));
+      if (left_edge) x.x = a.enc.inlet_g[q];
     }
     // d_q = g_q w_q / unit enters each moment as one fused multiply-add
     constexpr float isc = static_cast<float>(1.0 / store_scale(S, D3Q27::wclass[q]));
