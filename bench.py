@@ -84,6 +84,8 @@ WORKLOADS = {
                           u0=0.1, R=256.0, lid_u=0.1),
     "cavity128-f32": dict(case="cavity", bc="standard", storage="f32", arith="fast", n=(128, 128, 128), Re=1000,
                           u0=0.1, R=128.0, lid_u=0.1),
+    "tgv128-f32": dict(case="tgv", bc="standard", storage="f32", arith="fast", n=(128, 128, 128), Re=1600,
+                       u0=0.05, R=0.1, lid_u=0.0),
     "tgv128-f16": dict(case="tgv", bc="standard", storage="f16", arith="fast", n=(128, 128, 128), Re=1600,
                        u0=0.05, R=0.1, lid_u=0.0),
     "tgv256-f16": dict(case="tgv", bc="standard", storage="f16", arith="fast", n=(256, 256, 256), Re=1600,
