@@ -47,7 +47,7 @@ struct __align__(16) EngInst {
   int rule;      // CaseRule
   int bx_log2;   // tile width 2^bx_log2 threads along x (register-staged kernels)
   int parity0;   // engine step parity at admission
-  int x2;        // 2-byte format with nx even: threads own x-pairs (step_cells_x2)
+  int x2;        // nx even, 2-byte format or FP32 vortex: threads own x-pairs (step_cells_x2)
   int staged;    // 2-byte format, rows staged in shared memory (stage_core.cuh)
   int tw, th;    // cells of a tile along x and y
   stage::Geo geo;
@@ -137,17 +137,20 @@ struct FlatPlanes {
   int32_t sq;
   __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(src + (q * sq + idx)); }
   __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dst[q * sq + idx] = v; }
-  __device__ __forceinline__ uint32_t load_pair(int q, int32_t idx) const {
-    return __ldg(reinterpret_cast<const unsigned int*>(src + (q * sq + idx)));
+  // x-pair words: 32-bit pairs of 16-bit values; FP32: 64-bit pairs
+  using W = std::conditional_t<sizeof(T) == 4, uint2, uint32_t>;
+  using H = std::conditional_t<sizeof(T) == 4, uint32_t, uint16_t>;
+  __device__ __forceinline__ W load_pair(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const W*>(src + (q * sq + idx)));
   }
   __device__ __forceinline__ uint32_t load_half(int q, int32_t idx) const {
     return __ldg(reinterpret_cast<const unsigned short*>(src + (q * sq + idx)));
   }
-  __device__ __forceinline__ void store_pair(int q, int32_t idx, uint32_t v) const {
-    *reinterpret_cast<unsigned int*>(dst + (q * sq + idx)) = v;
+  __device__ __forceinline__ void store_pair(int q, int32_t idx, W v) const {
+    *reinterpret_cast<W*>(dst + (q * sq + idx)) = v;
   }
-  __device__ __forceinline__ void store_half(int q, int32_t idx, uint16_t v) const {
-    *reinterpret_cast<unsigned short*>(dst + (q * sq + idx)) = v;
+  __device__ __forceinline__ void store_half(int q, int32_t idx, H v) const {
+    *reinterpret_cast<H*>(dst + (q * sq + idx)) = v;
   }
 };
 
@@ -188,8 +191,8 @@ __global__ void __launch_bounds__(256, 2) engine_step_kernel(const EngArgs ea, c
     const int tx = threadIdx.x & ((1 << bxl) - 1), ty = threadIdx.x >> bxl;
     if constexpr (X2) {
       // 2-byte cavity and sphere instances round stochastically (stochastic_rounding_for)
-      step_cells_x2<S, B, RULE, RULE == CaseRule::CavityStd || RULE == CaseRule::SphereStd>(
-          sh.a, pl, tile.i0 + 2 * tx, tile.j0 + 2 * ty, tile.k);
+      step_cells_x2<S, B, RULE, S != Store::F32 && (RULE == CaseRule::CavityStd || RULE == CaseRule::SphereStd)>(
+          sh.a, pl, tile.i0 + 2 * tx, tile.j0 + PairRows<S>::value * ty, tile.k);
     } else {
       double drag[3] = {0.0, 0.0, 0.0};
       step_cells<S, B, RULE, EXACT, false>(sh.a, pl, tile.i0 + tx, tile.j0 + ty * CPT, tile.k, drag);
@@ -762,6 +765,14 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
         continue;
       }
     }
+    if constexpr (S == Store::F32) {
+      // FP32 x-pairs (the vortex)
+      if (mode == 1 && rule == 0) {
+        const int grid = std::min(e->grid, t1 - t0);
+        engine_step_kernel<S, false, Bc::Periodic, CaseRule::None, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+        continue;
+      }
+    }
     const int grid = std::min(e->grid, t1 - t0);
     if (rule == 0)
       engine_step_kernel<S, EXACT, Bc::Periodic, CaseRule::None, false><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
@@ -1051,7 +1062,9 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
   sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
   in.bx_log2 = sl.bx_log2;
   in.parity0 = static_cast<int>(e->gstep & 1);
-  in.x2 = (storage == IMEXLB_F16 || storage == IMEXLB_BF16) && d->nx % 2 == 0;
+  // x-pairs: the 2-byte formats, and FP32 for the vortex
+  in.x2 = d->nx % 2 == 0 && (storage == IMEXLB_F16 || storage == IMEXLB_BF16 ||
+                             (storage == IMEXLB_F32 && d->kase == IMEXLB_TGV));
   // rows staged in shared memory where they fit a stage (and tile_bx asks
   // for no register-staged tile width)
   in.staged = instance_staged(storage, d, sl.L, &in.geo) ? 1 : 0;
@@ -1060,7 +1073,7 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
     in.th = in.geo.R;
   } else {
     const int bx = 1 << sl.bx_log2;
-    in.th = (256 / bx) * cpt_of(storage);
+    in.th = (256 / bx) * (in.x2 ? (storage == IMEXLB_F32 ? 1 : 2) : cpt_of(storage));
     in.tw = bx * (in.x2 ? 2 : 1);
   }
   LaunchCfg cfg{d->kase == IMEXLB_TGV ? Bc::Periodic : Bc::Standard, static_cast<Store>(storage), CaseRule::None,

@@ -144,13 +144,14 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
 
 // 2-byte formats with nx even: each thread owns an x-pair in two rows
 // (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
+// FP32 vortex with nx even: x-pairs of one row.
 template <Store S, Bc B, CaseRule RULE, bool SR>
 __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
   pdl_release();
   pdl_wait();
   using T = typename StoreT<S>::T;
   const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int j0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
+  const int j0 = PairRows<S>::value * (blockIdx.y * blockDim.y + threadIdx.y);
   const int k = blockIdx.z;
   const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
   step_cells_x2<S, B, RULE, SR>(a, pl, x0, j0, k);
@@ -793,7 +794,8 @@ static cudaError_t step_pairs(const StepArgs& a, cudaStream_t s, bool* done) {
   // (the 2-byte formats sum their drag in drag_links_kernel)
   if (use_x2(S, a.nx)) {
     const dim3 block = step_block_x2(a.nx);
-    const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + 2 * block.y - 1) / (2 * block.y), a.nz);
+    constexpr int RY = PairRows<S>::value;
+    const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + RY * block.y - 1) / (RY * block.y), a.nz);
     return launch_pdl(step_kernel_x2<S, B, R, SR>, grid, block, 0, s, a);
   }
   *done = false;
@@ -802,6 +804,13 @@ static cudaError_t step_pairs(const StepArgs& a, cudaStream_t s, bool* done) {
 
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
+  if constexpr (S == Store::F32 && R == CaseRule::None && B == Bc::Periodic) {
+    if (a.nx % 2 == 0) {
+      const dim3 block = step_block_x2(a.nx);
+      const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + block.y - 1) / block.y, a.nz);
+      return launch_pdl(step_kernel_x2<S, B, R, false>, grid, block, 0, s, a);
+    }
+  }
   if constexpr (S == Store::F16 || S == Store::BF16) {
     bool done = false;
     cudaError_t err;

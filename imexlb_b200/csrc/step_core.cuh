@@ -301,19 +301,20 @@ struct Planes {
   T* const* dstq;        // 27 destination plane pointers
   __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(srcq[q] + idx); }
   __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dstq[q][idx] = v; }
-  // 2-byte formats: an aligned pair (idx even) or one value, as raw bits
-  __device__ __forceinline__ uint32_t load_pair(int q, int32_t idx) const {
-    return __ldg(reinterpret_cast<const unsigned int*>(srcq[q] + idx));
+  // x-pair formats: an aligned pair (idx even) or one value, as raw bits
+  // (32-bit pairs of 16-bit values; FP32: 64-bit pairs of 32-bit values)
+  using W = std::conditional_t<sizeof(T) == 4, uint2, uint32_t>;
+  using H = std::conditional_t<sizeof(T) == 4, uint32_t, uint16_t>;
+  __device__ __forceinline__ W load_pair(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const W*>(srcq[q] + idx));
   }
   __device__ __forceinline__ uint32_t load_half(int q, int32_t idx) const {
     return __ldg(reinterpret_cast<const unsigned short*>(srcq[q] + idx));
   }
-  __device__ __forceinline__ void store_pair(int q, int32_t idx, uint32_t v) const {
-    *reinterpret_cast<unsigned int*>(dstq[q] + idx) = v;
+  __device__ __forceinline__ void store_pair(int q, int32_t idx, W v) const {
+    *reinterpret_cast<W*>(dstq[q] + idx) = v;
   }
-  __device__ __forceinline__ void store_half(int q, int32_t idx, uint16_t v) const {
-    *reinterpret_cast<unsigned short*>(dstq[q] + idx) = v;
-  }
+  __device__ __forceinline__ void store_half(int q, int32_t idx, H v) const { *reinterpret_cast<H*>(dstq[q] + idx) = v; }
 };
 
 template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG, class P>
@@ -736,6 +737,11 @@ __device__ __forceinline__ void compute_pair(const StepArgs& a, const P& pl, con
   });
 }
 
+// Rows of x-pairs a thread of the register pair kernels owns: two for the
+// 2-byte formats (4-byte pair words), one for FP32 (8-byte pair words), so
+// that a thread has 216 bytes of loads in flight either way.
+template <Store S> struct PairRows { static constexpr int value = S == Store::F32 ? 1 : 2; };
+
 template <Store S> struct CellsPerThread { static constexpr int value = 1; };
 template <> struct CellsPerThread<Store::F32> { static constexpr int value = 2; };
 template <> struct CellsPerThread<Store::F16> { static constexpr int value = 2; };
@@ -818,8 +824,38 @@ template <> struct Pack2<Store::BF16> {
   static __device__ __forceinline__ uint16_t from_f(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 };
 
+// FP32 x-pairs: two FP32 values in one 8-byte word (deviations, unscaled).
+template <> struct Pack2<Store::F32> {
+  static __device__ __forceinline__ float2 to_f2(uint2 b) { return make_float2(__uint_as_float(b.x), __uint_as_float(b.y)); }
+  static __device__ __forceinline__ uint2 from_f2(float2 f) { return make_uint2(__float_as_uint(f.x), __float_as_uint(f.y)); }
+};
+
+// An x-pair's storage word (lo = cell x0, hi = cell x0 + 1): two 16-bit
+// values in 32 bits (FP16, BF16) or two FP32 values in 64 bits; H holds one
+// value's bits.
+template <Store S> struct PairWord { using W = uint32_t; using H = uint16_t; };
+template <> struct PairWord<Store::F32> { using W = uint2; using H = uint32_t; };
+__device__ __forceinline__ uint32_t lo_of(uint32_t w) { return w & 0xffffu; }
+__device__ __forceinline__ uint32_t hi_of(uint32_t w) { return w >> 16; }
+__device__ __forceinline__ uint32_t lo_of(uint2 w) { return w.x; }
+__device__ __forceinline__ uint32_t hi_of(uint2 w) { return w.y; }
+template <class W> __device__ __forceinline__ W pair_make(uint32_t lo, uint32_t hi);
+template <> __device__ __forceinline__ uint32_t pair_make<uint32_t>(uint32_t lo, uint32_t hi) {
+  return (lo & 0xffffu) | (hi << 16);
+}
+template <> __device__ __forceinline__ uint2 pair_make<uint2>(uint32_t lo, uint32_t hi) { return make_uint2(lo, hi); }
+
 // pair (lo = cell x0, hi = cell x0 + 1) from two 16-bit halves
 __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { return (lo16 & 0xffffu) | (hi16 << 16); }
+
+// The pair kernels collide in stored units: one unit of the equilibrium
+// bracket (3 p~ + e (3 + 4.5 e) - 1.5 u.u) of a population of weight class
+// cls is eq_factor(cls) stored units -- unit for the 2-byte formats, which
+// store d unit / w, and w itself for FP32, which stores d.
+template <Store S>
+__host__ __device__ constexpr float eq_factor(int cls) {
+  return S == Store::F32 ? static_cast<float>(weight_of_class(cls)) : store_unit(S);
+}
 
 // Second half of a 2-byte x-pair update: decode the pulled pairs (boundary
 // values already in place), moments, case rules, collision and the paired
@@ -843,7 +879,8 @@ __device__ __forceinline__ uint32_t pair_of(uint32_t lo16, uint32_t hi16) { retu
 // side in three aligned stores, so that the next step's tile finds them in
 // one bulk copy instead of nine scattered rows.
 template <Store S, CaseRule RULE, bool REC = false, bool SR = false, class P>
-__device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, const uint32_t (&raw)[Q], const int x0,
+__device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl,
+                                                const typename PairWord<S>::W (&raw)[Q], const int x0,
                                                 const int j, const int k, const bool lid, const bool left_edge,
                                                 const bool live0, const bool live1, const bool store,
                                                 const uint32_t seed, const uint32_t links0 = 0,
@@ -856,13 +893,17 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   // the format's scales are compile-time values (store_scale; Encoding holds
   // the same numbers for the host and the other kernels)
   constexpr float UNIT = store_unit(S);
-  [[maybe_unused]] const float lid_g = static_cast<float>(6.0 * a.rho_w * a.lid_u) * UNIT;
+  static_assert(!REC || S != Store::F32, "wall records are for the 2-byte formats");
+  static_assert(RULE != CaseRule::SphereStd || S != Store::F32, "the FP32 sphere runs the one-cell kernels");
+  [[maybe_unused]] const float lid6 = static_cast<float>(6.0 * a.rho_w * a.lid_u);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
     float2 x = Pack2<S>::to_f2(raw[q]);
     if constexpr (RULE == CaseRule::CavityStd && ex != 0 && ez < 0) {
       // moving lid: + 6 rho_w w_q (c_q . u_w), in stored units
+      constexpr float FAC = eq_factor<S>(D3Q27::wclass[q]);
+      const float lid_g = lid6 * FAC;
       if (lid) x = add2rn(x, f2s(ex > 0 ? lid_g : -lid_g));
     }
     if constexpr (RULE == CaseRule::SphereStd && ex > 0) {
@@ -917,7 +958,6 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     a.mp[c0 + 1] = live1 ? static_cast<double>(p.y) + a.p_shift : a.p_shift;
   }
   const float om = static_cast<float>(a.omega);
-  const float om_u = om * UNIT;
   const float2 keep = f2s(1.0f - om);
   // -1.5 u.u, rounded as 1.5 u.u then negated
   const float2 uu = fma2rn(w, w, fma2rn(v, v, mul2rn(u, u)));
@@ -928,8 +968,18 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
   } else {
     mudu15 = mul2rn(f2s(-1.5f), uu);
   }
-  // omega unit (3 p~ - 1.5 u.u)
-  const float2 K = mul2rn(f2s(om_u), fma2rn(p, f2s(3.0f), mudu15));
+  // omega eq_factor(cls) and omega eq_factor(cls) (3 p~ - 1.5 u.u), per
+  // weight class (one value for the 2-byte formats, whose factor is the
+  // same for every class)
+  constexpr int NCLS = S == Store::F32 ? 4 : 1;
+  const float2 kb = fma2rn(p, f2s(3.0f), mudu15);
+  float om_c[NCLS];
+  float2 K_c[NCLS];
+#pragma unroll
+  for (int c = 0; c < NCLS; ++c) {
+    om_c[c] = om * eq_factor<S>(c);
+    K_c[c] = mul2rn(f2s(om_c[c]), kb);
+  }
   // Collision and stores; a pair whose two cells are both updated (every
   // pair but those beside a solid or past the lattice's end) takes a copy of
   // the loop without the per-population choice between a paired and two
@@ -951,6 +1001,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
     constexpr bool BOTH = decltype(both_c)::value;
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
+      constexpr int ci = NCLS == 1 ? 0 : D3Q27::wclass[q];
+      const float om_u = om_c[ci];
+      const float2 K = K_c[ci];
       float2 Kq = K;
       if constexpr (RULE == CaseRule::SphereStd) {
         // minus the reference flow's equilibrium, omega unit br_ref[q]
@@ -970,7 +1023,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
         const float2 h = mul2rn(e, f2s(en ? -om_u : om_u));
         gn = fma2rn(h, t, fma2rn(gq, keep, Kq));
       }
-      uint32_t word;
+      typename PairWord<S>::W word;
       if constexpr (SR)
         word = sr_pair<S>(gn, x * sr_mul(q));
       else
@@ -986,8 +1039,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
           }
         }
       } else {
-        if (live0) pl.store_half(q, b, static_cast<uint16_t>(word & 0xffffu));
-        if (live1) pl.store_half(q, b + 1, static_cast<uint16_t>(word >> 16));
+        using H = typename PairWord<S>::H;
+        if (live0) pl.store_half(q, b, static_cast<H>(lo_of(word)));
+        if (live1) pl.store_half(q, b + 1, static_cast<H>(hi_of(word)));
       }
     });
   };
@@ -999,11 +1053,12 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl, 
 
 template <Store S, Bc B, CaseRule RULE, bool SR = false, class P>
 __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, const int x0, const int j0, const int k) {
-  constexpr int RY = 2;
+  constexpr int RY = PairRows<S>::value;
+  using W = typename PairWord<S>::W;
   const bool xin = x0 < a.nx;  // nx even: both cells of the pair or neither
   const int xs = xin ? x0 : a.nx - 2;
   const bool left_edge = xs == 0, right_edge = xs + 2 >= a.nx;
-  uint32_t raw[RY][Q];
+  W raw[RY][Q];
   int32_t rowb[RY][3][3];  // [r][1 - ez][1 - ey]: index of x = xs in the source row
   bool act[RY];
   uint32_t row_out_bits[RY];  // cavity: bit (3 dz + dy) = source row outside the box
@@ -1075,18 +1130,18 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
       constexpr int ex = D3Q27::ex[q], ey = D3Q27::ey[q], ez = D3Q27::ez[q];
       [[maybe_unused]] constexpr int qb = D3Q27::bb[q];
       const int32_t srow = rowb[r][1 - ez][1 - ey];
-      const uint32_t pv = pl.load_pair(q, srow);
-      uint32_t v = pv;
+      const W pv = pl.load_pair(q, srow);
+      W v = pv;
       if constexpr (ex == 1) {
-        const uint32_t lv = pl.load_pair(q, srow + dleft);
-        v = pair_of(lv >> 16, pv);
+        const W lv = pl.load_pair(q, srow + dleft);
+        v = pair_make<W>(hi_of(lv), lo_of(pv));
       } else if constexpr (ex == -1) {
-        const uint32_t rv = pl.load_pair(q, srow + dright);
-        uint32_t rlo = rv & 0xffffu;
+        const W rv = pl.load_pair(q, srow + dright);
+        uint32_t rlo = lo_of(rv);
         if constexpr (RULE == CaseRule::SphereStd) {
-          if (right_edge) rlo = pv >> 16;  // zero-gradient outlet: the own column
+          if (right_edge) rlo = hi_of(pv);  // zero-gradient outlet: the own column
         }
-        v = pair_of(pv >> 16, rlo);
+        v = pair_make<W>(hi_of(pv), rlo);
       }
       if constexpr (RULE == CaseRule::CavityStd) {
         // halfway bounce-back: a link leaving the box returns the cell's own
@@ -1095,14 +1150,14 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
         const bool out0 = out_row || (ex == 1 && left_edge);
         const bool out1 = out_row || (ex == -1 && right_edge);
         if (out0 || out1) {
-          const uint32_t bbp = pl.load_pair(qb, b);
-          v = pair_of(out0 ? bbp : v, out1 ? (bbp >> 16) : (v >> 16));
+          const W bbp = pl.load_pair(qb, b);
+          v = pair_make<W>(out0 ? lo_of(bbp) : lo_of(v), out1 ? hi_of(bbp) : hi_of(v));
         }
       } else if constexpr (RULE == CaseRule::SphereStd) {
         const bool s0 = (links0 >> q) & 1u, s1 = (links1 >> q) & 1u;
         if (s0 || s1) {
-          const uint32_t bbp = pl.load_pair(qb, b);
-          v = pair_of(s0 ? bbp : v, s1 ? (bbp >> 16) : (v >> 16));
+          const W bbp = pl.load_pair(qb, b);
+          v = pair_make<W>(s0 ? lo_of(bbp) : lo_of(v), s1 ? hi_of(bbp) : hi_of(v));
         }
       }
       raw[r][q] = v;
