@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256, 2) step_kernel(const StepArgs a) {
 
 // 2-byte formats with nx even: each thread owns an x-pair in two rows
 // (step_cells_x2); blockDim.x threads along x cover 2 blockDim.x cells.
-// FP32 vortex with nx even: x-pairs of one row.
+// FP32 vortex and standard cavity with nx even: x-pairs of one row.
 template <Store S, Bc B, CaseRule RULE, bool SR>
 __global__ void __launch_bounds__(256, 2) step_kernel_x2(const StepArgs a) {
   pdl_release();
@@ -804,7 +804,8 @@ static cudaError_t step_pairs(const StepArgs& a, cudaStream_t s, bool* done) {
 
 template <Store S, Bc B, CaseRule R, bool EXACT>
 static cudaError_t step_impl(const StepArgs& a, cudaStream_t s) {
-  if constexpr (S == Store::F32 && R == CaseRule::None && B == Bc::Periodic) {
+  if constexpr (S == Store::F32 && (R == CaseRule::None || R == CaseRule::CavityStd) &&
+                (B == Bc::Standard || B == Bc::Periodic)) {
     if (a.nx % 2 == 0) {
       const dim3 block = step_block_x2(a.nx);
       const dim3 grid((a.nx + 2 * block.x - 1) / (2 * block.x), (a.ny + block.y - 1) / block.y, a.nz);

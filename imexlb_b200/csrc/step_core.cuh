@@ -971,6 +971,10 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl,
   // omega eq_factor(cls) and omega eq_factor(cls) (3 p~ - 1.5 u.u), per
   // weight class (one value for the 2-byte formats, whose factor is the
   // same for every class)
+  // FP32 relaxes its non-equilibrium part instead, g - omega (g - geq)
+  // with geq = w (3 p~ + e (3 + 4.5 e) - 1.5 u.u) (K_c = w (3 p~ - 1.5 u.u)):
+  // near tau = 1/2 (omega near 2) that form keeps FP32's rounding of g,
+  // where (1 - omega) g + omega geq doubles it.
   constexpr int NCLS = S == Store::F32 ? 4 : 1;
   const float2 kb = fma2rn(p, f2s(3.0f), mudu15);
   float om_c[NCLS];
@@ -978,7 +982,7 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl,
 #pragma unroll
   for (int c = 0; c < NCLS; ++c) {
     om_c[c] = om * eq_factor<S>(c);
-    K_c[c] = mul2rn(f2s(om_c[c]), kb);
+    K_c[c] = mul2rn(f2s(S == Store::F32 ? eq_factor<S>(c) : om_c[c]), kb);
   }
   // Collision and stores; a pair whose two cells are both updated (every
   // pair but those beside a solid or past the lattice's end) takes a copy of
@@ -1011,7 +1015,15 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl,
       }
       const float2 gq = g[q];
       float2 gn;
-      if constexpr (q == 0) {
+      if constexpr (S == Store::F32) {
+        constexpr float W = eq_factor<S>(D3Q27::wclass[q]);
+        float2 geq = K;
+        if constexpr (q != 0) {
+          const float2 e = edu2<q>(u, v, w);
+          geq = fma2rn(e, fma2rn(e, f2s(4.5f * W), f2s(3.0f * W)), K);
+        }
+        gn = fma2rn(f2s(-om), sub2rn(gq, geq), gq);
+      } else if constexpr (q == 0) {
         gn = fma2rn(gq, keep, Kq);
       } else {
         // with e negated, so are the factors 4.5 and omega unit: same values.
@@ -1149,10 +1161,10 @@ __device__ __forceinline__ void step_cells_x2(const StepArgs& a, const P& pl, co
         const bool out_row = (row_out_bits[r] >> (3 * (1 - ez) + (1 - ey))) & 1u;
         const bool out0 = out_row || (ex == 1 && left_edge);
         const bool out1 = out_row || (ex == -1 && right_edge);
-        if (out0 || out1) {
-          const W bbp = pl.load_pair(qb, b);
-          v = pair_make<W>(out0 ? lo_of(bbp) : lo_of(v), out1 ? hi_of(bbp) : hi_of(v));
-        }
+        // a predicated load, not a branch: the x-wall lanes of a warp load
+        // while the others do not, and no warp splits
+        const W bbp = (out0 || out1) ? pl.load_pair(qb, b) : v;
+        v = pair_make<W>(out0 ? lo_of(bbp) : lo_of(v), out1 ? hi_of(bbp) : hi_of(v));
       } else if constexpr (RULE == CaseRule::SphereStd) {
         const bool s0 = (links0 >> q) & 1u, s1 = (links1 >> q) & 1u;
         if (s0 || s1) {
