@@ -47,7 +47,7 @@ struct __align__(16) EngInst {
   int rule;      // CaseRule
   int bx_log2;   // tile width 2^bx_log2 threads along x (register-staged kernels)
   int parity0;   // engine step parity at admission
-  int x2;        // nx even, 2-byte format or FP32 vortex / cavity: threads own x-pairs (step_cells_x2)
+  int x2;        // nx even, 2-byte format or FP32 vortex: threads own x-pairs (step_cells_x2)
   int staged;    // 2-byte format, rows staged in shared memory (stage_core.cuh)
   int tw, th;    // cells of a tile along x and y
   stage::Geo geo;
@@ -766,13 +766,10 @@ cudaError_t launch_groups(const imexlb_engine* e, const EngArgs& ea) {
       }
     }
     if constexpr (S == Store::F32) {
-      // FP32 x-pairs (vortex and cavity)
-      if (mode == 1) {
+      // FP32 x-pairs (the vortex)
+      if (mode == 1 && rule == 0) {
         const int grid = std::min(e->grid, t1 - t0);
-        if (rule == 0)
-          engine_step_kernel<S, false, Bc::Periodic, CaseRule::None, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
-        else
-          engine_step_kernel<S, false, Bc::Standard, CaseRule::CavityStd, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
+        engine_step_kernel<S, false, Bc::Periodic, CaseRule::None, true><<<grid, 256, 0, e->stream>>>(ea, t0, t1);
         continue;
       }
     }
@@ -1065,9 +1062,10 @@ int imexlb_engine_add_as(imexlb_engine* e, const imexlb_instance_desc* d, imexlb
   sl.bx_log2 = bx_log2_for(d->nx, d->tile_bx);
   in.bx_log2 = sl.bx_log2;
   in.parity0 = static_cast<int>(e->gstep & 1);
-  // x-pairs: the 2-byte formats, and FP32 for the vortex and the cavity
+  // x-pairs: the 2-byte formats, and FP32 for the vortex (the FP32 cavity
+  // measured faster in the engine with two cells of a column a thread)
   in.x2 = d->nx % 2 == 0 && (storage == IMEXLB_F16 || storage == IMEXLB_BF16 ||
-                             (storage == IMEXLB_F32 && d->kase != IMEXLB_SPHERE));
+                             (storage == IMEXLB_F32 && d->kase == IMEXLB_TGV));
   // rows staged in shared memory where they fit a stage (and tile_bx asks
   // for no register-staged tile width)
   in.staged = instance_staged(storage, d, sl.L, &in.geo) ? 1 : 0;
