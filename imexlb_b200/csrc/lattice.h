@@ -76,13 +76,6 @@ struct Encoding {
   // units, float(feq_in[q] * scale[q]) (the inlet column's values)
   float inlet_g[Q] = {};
 };
-// Whether a lattice's 2-byte stores round stochastically (Encoding::sr):
-// yes for the cavity and the sphere channel, driven flows that settle into
-// a steady state, where round-to-nearest repeats the same error every step;
-// no for the Taylor-Green vortex, a decaying flow without a steady state,
-// whose error against FP64 is smaller with round-to-nearest (measured over
-// 2000-16000 steps of 64^3 and 96^3 vortices).  `kase` is an imexlb_case,
-// `storage` an imexlb_storage (2 = FP16, 3 = BF16).
 // The stochastic-rounding hash: the 32-bit "lowbias32" integer finaliser
 // (C. Wellons, hash-prospector, 2018).
 IMX_HDC uint32_t sr_hash(uint32_t x) {
@@ -93,6 +86,13 @@ IMX_HDC uint32_t sr_hash(uint32_t x) {
   x ^= x >> 16;
   return x;
 }
+// Whether a lattice's 2-byte stores round stochastically (Encoding::sr):
+// yes for the cavity and the sphere channel, driven flows that settle into
+// a steady state, where round-to-nearest repeats the same error every step;
+// no for the Taylor-Green vortex, a decaying flow without a steady state,
+// whose error against FP64 is smaller with round-to-nearest (measured over
+// 2000-16000 steps of 64^3 and 96^3 vortices).  `kase` is an imexlb_case,
+// `storage` an imexlb_storage (2 = FP16, 3 = BF16).
 inline uint32_t stochastic_rounding_for(int kase, int storage) {
   return (storage == 2 || storage == 3) && kase != 0 ? 1u : 0u;
 }
