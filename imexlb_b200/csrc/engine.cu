@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   constexpr bool WRAP = B == Bc::Periodic || RULE == CaseRule::SphereStd;
   constexpr bool REC = RULE == CaseRule::CavityStd;  // wall records staged with the rows
   constexpr int NS = MAX_STAGES;
-  constexpr int stage_elems = Q * (SLOT_UNITS / MAX_STAGES);
+  constexpr int stage_elems = Q * SLOT_CAP;
   extern __shared__ __align__(128) unsigned char smem[];
   T* stages = reinterpret_cast<T*>(smem);
   unsigned char* args = smem + static_cast<size_t>(Q) * SLOT_UNITS * sizeof(T);

@@ -174,8 +174,8 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   uint64_t* empty = full + MAX_STAGES;
   auto rec_stage = [&](int sn) { return reinterpret_cast<uint16_t*>(recs + sn * REC_STAGE_BYTES); };
   __shared__ int abort_flag;
-  const int NS = g.stages;
-  const int stage_elems = Q * g.cap;
+  constexpr int NS = MAX_STAGES;
+  constexpr int stage_elems = Q * SLOT_CAP;
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) {
       bar_init(&full[s], 1);

@@ -46,17 +46,18 @@ namespace stage {
 using namespace core;
 
 constexpr int THREADS = 256;
-constexpr int SLOT_UNITS = 2 * 1024;  // stages x elements per population slot
-constexpr uint64_t WAIT_NS = 1000000000ull;
 constexpr int MAX_STAGES = 2;
+constexpr int SLOT_CAP = 1024;                     // elements per population slot of a stage
+constexpr int SLOT_UNITS = MAX_STAGES * SLOT_CAP;  // stages x elements per population slot
+constexpr uint64_t WAIT_NS = 1000000000ull;
 
 // Tile geometry of one lattice.  A tile is R whole rows of a plane, or (flat
 // tiles) a run of C elements of a plane's rows taken as one line.
 struct Geo {
   int P;       // staged row length: the layout's pitch (whole rows)
   int R;       // rows per tile (whole-row tiles)
-  int cap;     // elements per population slot of a stage (R * P <= cap, or C + 2 FLAT_GUARD <= cap)
-  int stages;  // stages * cap == SLOT_UNITS
+  int cap;     // SLOT_CAP: R * P <= cap, or C + 2 FLAT_GUARD <= cap
+  int stages;  // MAX_STAGES: stages * cap == SLOT_UNITS
   int nty;     // tiles per plane
   int flat;    // flat tiles (sphere channel)
   int C;       // elements per flat tile
@@ -87,8 +88,8 @@ constexpr int REC_STAGE_BYTES = REC_ROWS * WallRecord::BYTES;
 inline bool make_geo(int ny, int64_t pitch, Geo* g, int max_rows = 1024) {
   if (pitch % 8 != 0 || pitch > 1024) return false;
   g->P = static_cast<int>(pitch);
-  g->cap = 1024;
-  g->stages = SLOT_UNITS / g->cap;
+  g->cap = SLOT_CAP;
+  g->stages = MAX_STAGES;
   g->R = g->cap / g->P;
   if (g->R > max_rows) g->R = max_rows;
   if (g->R > ny) g->R = ny;
@@ -100,13 +101,13 @@ inline bool make_geo(int ny, int64_t pitch, Geo* g, int max_rows = 1024) {
 // elements, when the plane is long enough that a tile's source run wraps
 // around y on one side at most.
 inline bool make_geo_flat(int ny, int64_t pitch, Geo* g) {
-  const int cap = 1024, C = cap - 2 * FLAT_GUARD;
+  const int cap = SLOT_CAP, C = cap - 2 * FLAT_GUARD;
   const int64_t np = static_cast<int64_t>(ny) * pitch;
   if (pitch % 8 != 0 || np < C + 2 * pitch + 2 * FLAT_GUARD || np > (int64_t(1) << 30)) return false;
   g->P = static_cast<int>(pitch);
   g->R = 1;
   g->cap = cap;
-  g->stages = SLOT_UNITS / cap;
+  g->stages = MAX_STAGES;
   g->flat = 1;
   g->C = C;
   g->nty = static_cast<int>((np + C - 1) / C);
@@ -267,7 +268,7 @@ __host__ __device__ __forceinline__ void tile_runs(const A& a, const Geo& g, int
   main.bytes = 0;
   wrap.bytes = 0;
   main.pop = wrap.pop = q;
-  const int32_t slot = q * g.cap;
+  const int32_t slot = q * SLOT_CAP;
   int kk = k - ez_of(q);
   if (kk < 0 || kk >= a.nz) {
     if (!WRAP_YZ) {
@@ -317,7 +318,7 @@ __host__ __device__ __forceinline__ void tile_runs_flat(const A& a, const Geo& g
   const int n = np - e0 < g.C ? np - e0 : g.C;
   const int32_t s0 = e0 - ey_of(q) * g.P - FLAT_GUARD;  // source element of slot element 0
   const int32_t s1 = s0 + n + 2 * FLAT_GUARD;            // one past the last
-  const int32_t slot = q * g.cap;
+  const int32_t slot = q * SLOT_CAP;
   if (s1 <= 0 || s0 >= np) {
     // the whole run lies across the y wrap (a short last tile of a plane)
     main.src = plane + (s1 <= 0 ? s0 + np : s0 - np);
@@ -425,7 +426,7 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
     lw = row + ((x == 0 ? a.nx - 2 : x - 2) >> 1);  // wrapped inside the row
     rw = row + ((x + 2 >= a.nx ? 0 : x + 2) >> 1);
   }
-  const int slotw = g.cap >> 1;
+  constexpr int slotw = SLOT_CAP / 2;  // a compile-time stride: every slot read is [base + immediate]
 
   uint32_t raw[Q];
   static_for<0, Q>([&](auto qc) {
@@ -520,6 +521,15 @@ __device__ __forceinline__ void pair_from_stage(const StepArgs& a, const P& pl, 
                                                             seed, links0, links1, rec_row);
 }
 
+// n / d for 0 <= n < 2048 and 8 <= 2 d <= 2048, without an integer division:
+// (n + 1/2) / d lies at least 1/(2 d) >= 2^-11 from an integer, and the two
+// round-to-nearest steps (the reciprocal and the product) move it by at most
+// (n / d) 2^-23 <= 2^-14, so the truncation is the quotient.  `inv` is
+// __frcp_rn(d).
+__device__ __forceinline__ int small_quotient(int n, float inv) {
+  return __float2int_rz((static_cast<float>(n) + 0.5f) * inv);
+}
+
 // The cells of tile (j0, k) from stage `st`, shared by the block's threads:
 // thread slot p is the pair at x = 2 (p mod P/2) of tile row p div P/2, so
 // a warp's pairs, and its stores, follow the rows' alignment in memory
@@ -535,12 +545,13 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
                                              const uint16_t* rec = nullptr, uint16_t* rec_out = nullptr) {
   const int rv = a.ny - j0 < g.R ? a.ny - j0 : g.R;
   const int half = g.P >> 1;
-  const int npairs = g.R * half;
+  const int npairs = g.R * half;  // at most SLOT_CAP / 2
+  const float inv_half = __frcp_rn(static_cast<float>(half));
   if constexpr (RULE == CaseRule::CavityStd) {
     const bool wall_plane = k == 0 || k == a.nz - 1;
     uint16_t* const rec_tile = rec_out + (static_cast<int64_t>(k) * a.ny + j0) * WallRecord::WORDS;
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
-      const int r = p / half, x = 2 * (p - r * half);
+      const int r = small_quotient(p, inv_half), x = 2 * (p - r * half);
       if (r >= rv || x >= a.nx) continue;
       const int j = j0 + r;
       uint16_t* const rec_row = rec_tile + r * WallRecord::WORDS;
@@ -556,22 +567,25 @@ __device__ __forceinline__ void consume_tile(const StepArgs& a, const P& pl, con
       const int e0 = j0;
       const int np = a.ny * g.P;
       const int n = np - e0 < g.C ? np - e0 : g.C;
+      // row of element e0 + 2p: jb + (x0 + 2p) / P, x0 + 2p < P + C
+      const int jb = e0 / g.P, x0 = e0 - jb * g.P;
+      const float inv_p = __frcp_rn(static_cast<float>(g.P));
       for (int p = threadIdx.x; 2 * p < n; p += THREADS) {
-        const int e = e0 + 2 * p;
-        const int j = e / g.P, x = e - j * g.P;
+        const int l = x0 + 2 * p, dj = small_quotient(l, inv_p);
+        const int j = jb + dj, x = l - dj * g.P;
         if (x < a.nx)
           pair_from_stage<S, B, RULE, true, true, SR>(a, pl, g, st, x, 0, 0, k, store, seed, nullptr, nullptr, j,
                                                   p + FLAT_GUARD / 2);
       }
     } else {
       for (int p = threadIdx.x; p < npairs; p += THREADS) {
-        const int r = p / half, x = 2 * (p - r * half);
+        const int r = small_quotient(p, inv_half), x = 2 * (p - r * half);
         if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true, false, SR>(a, pl, g, st, x, r, j0, k, store, seed);
       }
     }
   } else {
     for (int p = threadIdx.x; p < npairs; p += THREADS) {
-      const int r = p / half, x = 2 * (p - r * half);
+      const int r = small_quotient(p, inv_half), x = 2 * (p - r * half);
       if (r < rv && x < a.nx) pair_from_stage<S, B, RULE, true, false, SR>(a, pl, g, st, x, r, j0, k, store, seed);
     }
   }
