@@ -238,13 +238,10 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   const int grid = gridDim.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // Warp 0 issues the block's tiles in order t0 + blockIdx.x + n grid.  For
-  // the cavity and the sphere the descriptor of the next one is copied into
-  // shared memory one tile ahead (cp.async, lanes 0-7; tile n of the block
-  // uses descriptor slot n & 1), so the copies of a tile wait on no global
-  // load.  The vortex's kernel reads the tile list and instance directly:
-  // it measured 4 % faster so, with no spills against 20 bytes.
-  constexpr bool PREFETCH = RULE != CaseRule::None;
+  // Warp 0 issues the block's tiles in order t0 + blockIdx.x + n grid.  The
+  // descriptor of the next one is copied into shared memory one tile ahead
+  // (cp.async, lanes 0-7; tile n of the block uses descriptor slot n & 1),
+  // so the copies of a tile wait on no global load.
   auto fetch = [&](int t, int n) {
     if (t < t1 && lane < 8)
       cp_async16(reinterpret_cast<unsigned char*>(dslot + (n & 1)) + 16 * lane,
@@ -254,41 +251,25 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
   // copies of the block's tile number `issued` into stage sn (warp 0), then
   // fetch the descriptor of the next one, tile tf
   auto issue = [&](int sn, int tf) {
-    if constexpr (PREFETCH) {
-      cp_async_wait_all();
-      __syncwarp();
-      const StagedTile& d = dslot[issued & 1];
-      const int cur = (ea.parity ^ d.parity0) & 1;
-      const void* src_buf = d.buf[cur];
-      const int left = ea.left[d.slot];
-      if (lane == 0)
-        hdr[sn] = TileHdr{src_buf, const_cast<void*>(d.buf[1 - cur]), REC ? d.rec[1 - cur] : nullptr, d.geo, d.j0,
-                          d.k, left == 0, ea.store || left == 1, sr_hash(ea.seed[d.slot])};
-      if (left == 0)
-        issue_skip(&full[sn]);
-      else
-        issue_tile<T, WRAP>(d, d.geo, static_cast<const T*>(src_buf), d.j0, d.k, stages + sn * stage_elems,
-                            &full[sn], REC ? d.rec[cur] : nullptr, rec_stage(sn), args + sn * STAGED_ARGS_BYTES,
-                            d.args, static_cast<uint32_t>(STAGED_ARGS_BYTES));
-      __syncwarp();  // every lane has read the slot before the fetch after next refills it
-      fetch(tf, issued + 1);
-    } else {
-      const Tile tile = ea.tiles[tf - grid];
-      const EngInst* in = ea.inst + tile.slot;
-      const int cur = (ea.parity ^ in->parity0) & 1;
-      const int left = ea.left[tile.slot];
-      if (lane == 0)
-        hdr[sn] = TileHdr{in->buf[cur], in->buf[1 - cur], REC ? in->rec[1 - cur] : nullptr, in->geo, tile.j0, tile.k,
-                          left == 0, ea.store || left == 1, sr_hash(ea.seed[tile.slot])};
-      if (left == 0)
-        issue_skip(&full[sn]);
-      else
-        issue_tile<T, WRAP>(in->a, in->geo, static_cast<const T*>(in->buf[cur]), tile.j0, tile.k,
-                            stages + sn * stage_elems, &full[sn], REC ? in->rec[cur] : nullptr, rec_stage(sn),
-                            args + sn * STAGED_ARGS_BYTES, &in->a, static_cast<uint32_t>(STAGED_ARGS_BYTES));
-    }
+    cp_async_wait_all();
+    __syncwarp();
+    const StagedTile& d = dslot[issued & 1];
+    const int cur = (ea.parity ^ d.parity0) & 1;
+    const void* src_buf = d.buf[cur];
+    const int left = ea.left[d.slot];
+    if (lane == 0)
+      hdr[sn] = TileHdr{src_buf, const_cast<void*>(d.buf[1 - cur]), REC ? d.rec[1 - cur] : nullptr, d.geo, d.j0,
+                        d.k, left == 0, ea.store || left == 1, sr_hash(ea.seed[d.slot])};
+    if (left == 0)
+      issue_skip(&full[sn]);
+    else
+      issue_tile<T, WRAP>(d, d.geo, static_cast<const T*>(src_buf), d.j0, d.k, stages + sn * stage_elems, &full[sn],
+                          REC ? d.rec[cur] : nullptr, rec_stage(sn), args + sn * STAGED_ARGS_BYTES, d.args,
+                          static_cast<uint32_t>(STAGED_ARGS_BYTES));
+    __syncwarp();  // every lane has read the slot before the fetch after next refills it
+    fetch(tf, issued + 1);
   };
-  if (PREFETCH && warp == 0) fetch(t0 + blockIdx.x, 0);
+  if (warp == 0) fetch(t0 + blockIdx.x, 0);
   if (warp == 0) {
     for (; issued < NS - 1; ++issued) {
       const int t = t0 + blockIdx.x + issued * grid;
