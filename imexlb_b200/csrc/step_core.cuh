@@ -1006,9 +1006,9 @@ __device__ __forceinline__ void finish_pair_row(const StepArgs& a, const P& pl,
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       constexpr int ci = NCLS == 1 ? 0 : D3Q27::wclass[q];
-      const float om_u = om_c[ci];
+      [[maybe_unused]] const float om_u = om_c[ci];  // the 2-byte formats' collision
       const float2 K = K_c[ci];
-      float2 Kq = K;
+      [[maybe_unused]] float2 Kq = K;
       if constexpr (RULE == CaseRule::SphereStd) {
         // minus the reference flow's equilibrium, omega unit br_ref[q]
         Kq = add2rn(K, f2s(a.enc.kref[q]));
