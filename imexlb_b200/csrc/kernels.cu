@@ -374,21 +374,30 @@ __global__ void ghost_gather_kernel(typename StoreT<S>::T* __restrict__ dst, con
 }
 
 // The same gather over a packed plan: entry e is (target, source) as two
-// 32-bit indices (int2), one 8-byte load instead of two.
+// 32-bit indices (int2), one 8-byte load instead of two.  Launched with
+// programmatic dependent launch after the step kernel: the plan does not
+// depend on the step, so a thread loads its first entries while the step
+// kernel drains and only then waits for the step's values (pdl_wait).
 template <Store S>
 __global__ void ghost_gather_packed_kernel(typename StoreT<S>::T* __restrict__ dst,
                                            const typename StoreT<S>::T* __restrict__ prev,
                                            const int2* __restrict__ plan, int64_t n, int64_t sq, Encoding enc) {
   using T = typename StoreT<S>::T;
   constexpr int V = 4;
+  pdl_release();
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * V;
-  for (int64_t e0 = static_cast<int64_t>(blockIdx.x) * blockDim.x * V + threadIdx.x; e0 < n; e0 += stride) {
-    int2 p[V];
+  int64_t e0 = static_cast<int64_t>(blockIdx.x) * blockDim.x * V + threadIdx.x;
+  int2 p[V];
+  auto load_plan = [&]() {
 #pragma unroll
     for (int u = 0; u < V; ++u) {
       const int64_t e = e0 + static_cast<int64_t>(u) * blockDim.x;
       p[u] = e < n ? __ldg(plan + e) : make_int2(-1, -1);
     }
+  };
+  load_plan();
+  pdl_wait();  // the step kernel's values are complete and visible from here on
+  for (; e0 < n; e0 += stride) {
     T val[V];
 #pragma unroll
     for (int u = 0; u < V; ++u) {
@@ -403,6 +412,11 @@ __global__ void ghost_gather_packed_kernel(typename StoreT<S>::T* __restrict__ d
 #pragma unroll
     for (int u = 0; u < V; ++u)
       if (p[u].x >= 0) dst[p[u].x] = val[u];
+    if (e0 + stride < n) {
+      e0 += stride;
+      load_plan();
+      e0 -= stride;
+    }
   }
 }
 
@@ -876,12 +890,13 @@ cudaError_t launch_ghost_gather_packed(Store st, void* dst, const void* prev, co
   const int threads = 256;
   const int64_t want = (n + threads * 4 - 1) / (threads * 4);
   const int blocks = static_cast<int>(want < 148 * 8 ? want : 148 * 8);
+  cudaError_t err = cudaSuccess;
   switch (st) {
 #define IMX_GGP(S)                                                                                               \
   case S:                                                                                                        \
-    ghost_gather_packed_kernel<S><<<blocks, threads, 0, s>>>(static_cast<typename StoreT<S>::T*>(dst),           \
-                                                            static_cast<const typename StoreT<S>::T*>(prev), plan, \
-                                                            n, sq, enc);                                           \
+    err = launch_pdl(ghost_gather_packed_kernel<S>, dim3(blocks), dim3(threads), 0, s,                         \
+                     static_cast<typename StoreT<S>::T*>(dst), static_cast<const typename StoreT<S>::T*>(prev), \
+                     plan, n, sq, enc);                                                                        \
     break;
     IMX_GGP(Store::F64)
     IMX_GGP(Store::F32)
@@ -889,7 +904,7 @@ cudaError_t launch_ghost_gather_packed(Store st, void* dst, const void* prev, co
     IMX_GGP(Store::BF16)
 #undef IMX_GGP
   }
-  return cudaGetLastError();
+  return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_ghost_gather(Store st, void* dst, const void* prev, const int64_t* tgt, const int64_t* src,
