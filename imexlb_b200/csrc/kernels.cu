@@ -192,7 +192,14 @@ __global__ void __launch_bounds__(stage::THREADS, 2) staged_kernel(const StepArg
   const int grid = gridDim.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const T* src = static_cast<const T*>(a.src);
-  const Planes<T> pl{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
+  // the sphere's linked pairs also load from global memory; its kernels keep
+  // the per-population plane table (with strided planes they spill)
+  using PL = std::conditional_t<RULE == CaseRule::SphereStd, Planes<T>, StridedPlanes<T>>;
+  PL pl;
+  if constexpr (RULE == CaseRule::SphereStd)
+    pl = PL{reinterpret_cast<const T* const*>(a.srcq), reinterpret_cast<T* const*>(a.dstq)};
+  else
+    pl = PL{src, static_cast<T*>(a.dst), a.sq};
 
   // the block's first NS - 1 tiles
   int issued = 0;  // tiles of this block whose copies are issued (warp 0)

@@ -317,6 +317,34 @@ struct Planes {
   __device__ __forceinline__ void store_half(int q, int32_t idx, H v) const { *reinterpret_cast<H*>(dstq[q] + idx) = v; }
 };
 
+// Population planes at one stride: plane q starts q * sq elements into the
+// buffer.  A thread's per-cell index is one 64-bit address; each
+// population's offset q * sq is the same for every thread of the block (the
+// shared-memory staged kernels, whose reads come from the stage and whose
+// stores go here).
+template <class T>
+struct StridedPlanes {
+  const T* src;
+  T* dst;
+  int64_t sq;
+  using W = std::conditional_t<sizeof(T) == 4, uint2, uint32_t>;
+  using H = std::conditional_t<sizeof(T) == 4, uint32_t, uint16_t>;
+  __device__ __forceinline__ T load(int q, int32_t idx) const { return ldg_stream(src + idx + q * sq); }
+  __device__ __forceinline__ void store(int q, int32_t idx, T v) const { dst[idx + q * sq] = v; }
+  __device__ __forceinline__ W load_pair(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const W*>(src + idx + q * sq));
+  }
+  __device__ __forceinline__ uint32_t load_half(int q, int32_t idx) const {
+    return __ldg(reinterpret_cast<const unsigned short*>(src + idx + q * sq));
+  }
+  __device__ __forceinline__ void store_pair(int q, int32_t idx, W v) const {
+    *reinterpret_cast<W*>(dst + idx + q * sq) = v;
+  }
+  __device__ __forceinline__ void store_half(int q, int32_t idx, H v) const {
+    *reinterpret_cast<H*>(dst + idx + q * sq) = v;
+  }
+};
+
 template <Store S, Bc B, CaseRule RULE, bool EXACT, bool DRAG, class P>
 __device__ __forceinline__ void load_cell(const StepArgs& a, const P& pl, const int i, const int j, const int k,
                                           typename StoreT<S>::R (&f)[Q], double (&drag)[3]) {
