@@ -298,7 +298,12 @@ __global__ void __launch_bounds__(stage::THREADS, 2) engine_staged_kernel(const 
     const TileHdr& h = hdr[s];
     if (!h.skip) {
       const StepArgs& a = *reinterpret_cast<const StepArgs*>(args + s * STAGED_ARGS_BYTES);
-      const FlatPlanes<T> pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst), static_cast<int32_t>(a.sq)};
+      // the cavity and the vortex: one 64-bit plane base a pair and the
+      // block-uniform offset q * sq a population; the sphere's kernels keep
+      // 32-bit plane indices (they spill 56 bytes with the 64-bit base)
+      using PL = std::conditional_t<RULE == CaseRule::SphereStd, FlatPlanes<T>, StridedPlanes<T>>;
+      const PL pl{static_cast<const T*>(h.src), static_cast<T*>(h.dst),
+                  static_cast<decltype(PL::sq)>(a.sq)};
       const Geo g = h.geo;
       consume_tile<S, B, RULE, RULE == CaseRule::CavityStd || RULE == CaseRule::SphereStd>(
           a, pl, g, reinterpret_cast<const uint32_t*>(stages + s * stage_elems), h.j0, h.k, h.store != 0, h.seed,
